@@ -1,0 +1,180 @@
+/* perman_b200.h -- C ABI of the B200 matrix-permanent engine (libperman_b200.so).
+ *
+ * The library computes matrix permanents on an NVIDIA B200 (sm_100a) with
+ * hand-written CUDA kernels.  Every entry point is plain C: caller-owned host
+ * buffers, sizes as ints, an opaque context, int status codes.  There is no
+ * CPU fallback: without a usable B200 every compute call fails with
+ * PERM_ECUDA and a message.
+ *
+ * Reference interfaces replaced (berkyaglioglu/matrix-permanent-calculator):
+ *   gpu_perman64_xshared_coalescing_mshared<T>          gpu_exact_dense.cu:641
+ *   gpu_perman64_xshared_coalescing_mshared_multigpu<T> gpu_exact_dense.cu:702
+ *   gpu_perman64_xshared_coalescing_mshared_skipper<T>  gpu_exact_sparse.cu:1124
+ *   gpu_perman64_rasmussen<T>                           gpu_approximation_dense.cu:374
+ *   gpu_perman64_approximation<T>                       gpu_approximation_dense.cu:528
+ *   gpu_perman64_rasmussen_sparse                       gpu_approximation_sparse.cu:455
+ *   gpu_perman64_approximation_sparse                   gpu_approximation_sparse.cu:608
+ *   ReadMatrix / matrix2compressed[_sortOrder|_skipOrder] util.h:344, 523, 554, 622
+ * The reference's templates are C++ functions returning a bare double; the
+ * `gpu_perman64_*_{int,float,double}` entry points below keep those exact
+ * argument lists for callers that bind them directly, and the perm_* entry
+ * points are the status-returning form that new callers should use.
+ */
+#ifndef PERMAN_B200_H
+#define PERMAN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define PERM_OK 0
+#define PERM_EINVAL (-1)       /* bad argument (size, pointer, option)          */
+#define PERM_ECUDA (-2)        /* CUDA runtime error or no usable device        */
+#define PERM_ENOMEM (-3)       /* device or pinned host allocation failed       */
+#define PERM_EUNSUPPORTED (-4) /* valid request outside this build's limits     */
+#define PERM_ETIMEOUT (-5)     /* a bounded device wait gave up (error flag)    */
+#define PERM_EIO (-6)          /* matrix file could not be read or parsed       */
+
+/* ---- element types of caller matrices ------------------------------------ */
+#define PERM_F64 0
+#define PERM_F32 1
+#define PERM_I32 2
+
+/* ---- kernels (perm_result.kernel) ---------------------------------------- */
+#define PERM_KERNEL_DENSE 1   /* register-X Gray-code Ryser                 */
+#define PERM_KERNEL_SKIPPER 2 /* SkipPer on CRS/CCS                          */
+
+/* Limits of this build. */
+#define PERM_MAX_EXACT_N 64  /* Gray indices are 64-bit                 */
+#define PERM_MAX_MC_N 64     /* trial masks are 64-bit                  */
+
+typedef struct perm_ctx perm_ctx;       /* one device, one stream, scratch */
+typedef struct perm_matrix perm_matrix; /* device-resident dense matrix    */
+
+typedef struct {
+  double value;       /* permanent, hi + lo rounded to double               */
+  double hi, lo;      /* double-double result                               */
+  double steps;       /* Gray indices whose product was evaluated           */
+  double total_steps; /* 2^(n-1), the dense Gray range                      */
+  double kernel_ms;   /* device time of the compute kernel (CUDA events)    */
+  int kernel;         /* PERM_KERNEL_*                                      */
+  int n;
+} perm_result;
+
+typedef struct {
+  double mean;        /* estimate of the permanent of the 0/1 pattern       */
+  double std_error;   /* sample standard deviation / sqrt(trials)           */
+  double trials;
+  double zero_trials; /* trials that ended on an empty row / zero sum       */
+  double sum, sum_sq; /* raw accumulators                                   */
+  double kernel_ms;
+} perm_estimate;
+
+/* ---- context --------------------------------------------------------------- */
+int perm_version(void);                       /* 10000 * major + 100 * minor  */
+int perm_device_count(void);                  /* visible CUDA devices, or <0  */
+int perm_ctx_create(int device, perm_ctx** out);
+void perm_ctx_destroy(perm_ctx* ctx);
+const char* perm_ctx_last_error(const perm_ctx* ctx);
+const char* perm_status_string(int status);
+
+/* ---- exact permanents ------------------------------------------------------ */
+/* Dense Ryser of a row-major n x n matrix (dtype PERM_F64/F32/I32), 1 <= n <= 64.
+ * Replaces gpu_perman64_xshared_coalescing_mshared (gpu_exact_dense.cu:641). */
+int perm_exact_dense(perm_ctx* ctx, const void* mat, int n, int dtype, perm_result* out);
+
+/* Share `shard` of `nshards` of the same Gray walk; the permanent is the
+ * double-double sum of all shards' (hi, lo).  Ranks of a multi-GPU job call
+ * this with their rank and world size (replaces the per-device ranges of
+ * gpu_exact_dense.cu:729-752). */
+int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int shard, int nshards,
+                           perm_result* out);
+
+/* SkipPer on CRS (rptrs, cols, rvals) + CCS (cptrs, rows, cvals) of an n x n
+ * matrix, 1 <= n <= 64; only the stored entries are used (x0 from the CRS row
+ * sums and CCS column n-1, algo.h:751-760).  Replaces
+ * gpu_perman64_xshared_coalescing_mshared_skipper (gpu_exact_sparse.cu:1124). */
+int perm_exact_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols, const double* rvals,
+                      const int* cptrs, const int* rows, const double* cvals, perm_result* out);
+
+/* Device-resident dense matrices: upload once, run many times (no host copy
+ * inside perm_exact_dense_resident). */
+int perm_matrix_create_dense(perm_ctx* ctx, const void* mat, int n, int dtype, perm_matrix** out);
+void perm_matrix_destroy(perm_ctx* ctx, perm_matrix* m);
+int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, perm_result* out);
+
+/* ---- Monte-Carlo estimates of the permanent of the 0/1 pattern -------------- */
+/* trials >= 1 run exactly (the reference rounds up to a multiple of 1024);
+ * trial t uses Philox stream (seed, t) so results do not depend on the launch
+ * shape.  trial_values, if not NULL, receives the `trials` per-trial weights. */
+int perm_approx_rasmussen(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trials,
+                          uint64_t seed, double* trial_values, perm_estimate* out);
+int perm_approx_scaling(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trials,
+                        int scale_intervals, int scale_times, uint64_t seed, double* trial_values,
+                        perm_estimate* out);
+int perm_approx_rasmussen_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
+                                 int64_t trials, uint64_t seed, double* trial_values,
+                                 perm_estimate* out);
+int perm_approx_scaling_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
+                               const int* cptrs, const int* rows, int64_t trials,
+                               int scale_intervals, int scale_times, uint64_t seed,
+                               double* trial_values, perm_estimate* out);
+
+/* ---- matrix input (host only; no device needed) ------------------------------ */
+/* Reads the reference text format ("n nnz type" then "i j value" lines,
+ * util.h:344).  binary != 0 stores 1 for every entry (the -b flag).  `out`
+ * must hold cap_n * cap_n doubles; the matrix is written row-major with
+ * stride n.  type_out (>= 8 bytes) receives "int", "float" or "double". */
+int perm_read_matrix(const char* path, int binary, int cap_n, double* out, int* n_out,
+                     int* header_nnz, char* type_out);
+/* CRS/CCS of the positive entries; mode 0 plain (util.h:523), 1 sortOrder
+ * (util.h:554), 2 skipOrder (util.h:622; permutes mat in place).  Buffers:
+ * ptrs n+1, index/value arrays n*n.  Returns the stored count or <0. */
+int perm_compress(int mode, double* mat, int n, int* cptrs, int* rows, double* cvals, int* rptrs,
+                  int* cols, double* rvals);
+
+/* ---- measurement ------------------------------------------------------------- */
+/* FP64 pipe peak of this device: independent DFMA chains, lane-operations
+ * per second (DADD, DMUL and DFMA each count as one operation). */
+int perm_fp64_peak(perm_ctx* ctx, double* ops_per_second, double* kernel_ms);
+
+/* ---- reference-signature entry points ------------------------------------------
+ * Same arguments as the reference's templates; grid_dim/block_dim are accepted
+ * and ignored (launch shapes are chosen per device).  They run on the process
+ * default context (device from $PERM_DEVICE, else 0) and return NaN on error
+ * (message on stderr). */
+double gpu_perman64_xshared_coalescing_mshared_int(int* mat, int nov, int grid_dim, int block_dim);
+double gpu_perman64_xshared_coalescing_mshared_float(float* mat, int nov, int grid_dim, int block_dim);
+double gpu_perman64_xshared_coalescing_mshared_double(double* mat, int nov, int grid_dim,
+                                                      int block_dim);
+double gpu_perman64_xshared_coalescing_mshared_skipper_int(int* mat, int* rptrs, int* cols, int* cptrs,
+                                                           int* rows, int* cvals, int nov,
+                                                           int grid_dim, int block_dim);
+double gpu_perman64_xshared_coalescing_mshared_skipper_float(float* mat, int* rptrs, int* cols,
+                                                             int* cptrs, int* rows, float* cvals,
+                                                             int nov, int grid_dim, int block_dim);
+double gpu_perman64_xshared_coalescing_mshared_skipper_double(double* mat, int* rptrs, int* cols,
+                                                              int* cptrs, int* rows, double* cvals,
+                                                              int nov, int grid_dim, int block_dim);
+double gpu_perman64_rasmussen_int(int* mat, int nov, int number_of_times);
+double gpu_perman64_rasmussen_float(float* mat, int nov, int number_of_times);
+double gpu_perman64_rasmussen_double(double* mat, int nov, int number_of_times);
+double gpu_perman64_approximation_int(int* mat, int nov, int number_of_times, int scale_intervals,
+                                      int scale_times);
+double gpu_perman64_approximation_float(float* mat, int nov, int number_of_times, int scale_intervals,
+                                        int scale_times);
+double gpu_perman64_approximation_double(double* mat, int nov, int number_of_times,
+                                         int scale_intervals, int scale_times);
+double gpu_perman64_rasmussen_sparse(int* rptrs, int* cols, int nov, int nnz, int number_of_times,
+                                     int grid_graph);
+double gpu_perman64_approximation_sparse(int* cptrs, int* rows, int* rptrs, int* cols, int nov,
+                                         int nnz, int number_of_times, int scale_intervals,
+                                         int scale_times, int grid_graph);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PERMAN_B200_H */

@@ -1,0 +1,839 @@
+// engine.cu -- host side of the permanent engine: device contexts, launch
+// planning, the C ABI declared in include/perman_b200.h.
+//
+// Replaces the reference's host wrappers (gpu_exact_dense.cu:641-699,
+// gpu_exact_sparse.cu:1124-1190, gpu_approximation_dense.cu:374-409, 528-571,
+// gpu_approximation_sparse.cu:455-495, 608-661).  Differences by design:
+//  * a context owns the stream and all scratch, allocated once, so a call does
+//    no cudaMalloc/cudaFree (the reference allocates and frees per call and
+//    hard-codes cudaSetDevice(1));
+//  * every CUDA call is checked and reported through a status code and a
+//    per-context message (the reference checks none);
+//  * results come back as one double-double (16 bytes) reduced on the device
+//    instead of 524,288 partials summed on the host;
+//  * launch shapes are chosen from the device's SM count and the kernel's
+//    occupancy instead of a fixed <<<2048, 256>>>.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/perman_b200.h"
+#include "matrix_io.h"
+#include "mc.h"
+#include "perman_common.cuh"
+#include "ryser_dense.cuh"
+#include "skipper.h"
+
+namespace perm {
+const void* dense_kernel_0(int n);
+const void* dense_kernel_1(int n);
+const void* dense_kernel_2(int n);
+const void* dense_kernel_3(int n);
+const void* dense_kernel_4(int n);
+
+static const void* dense_kernel(int n) {
+  if (n >= 1 && n <= 20) return dense_kernel_0(n);
+  if (n <= 32) return dense_kernel_1(n);
+  if (n <= 42) return dense_kernel_2(n);
+  if (n <= 52) return dense_kernel_3(n);
+  if (n <= 64) return dense_kernel_4(n);
+  return nullptr;
+}
+
+__global__ void fp64_peak_kernel(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-3, x2 = x0 + 2e-3, x3 = x0 + 3e-3;
+  double x4 = x0 + 4e-3, x5 = x0 + 5e-3, x6 = x0 + 6e-3, x7 = x0 + 7e-3;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      x0 = fma(x0, a, b);
+      x1 = fma(x1, a, b);
+      x2 = fma(x2, a, b);
+      x3 = fma(x3, a, b);
+      x4 = fma(x4, a, b);
+      x5 = fma(x5, a, b);
+      x6 = fma(x6, a, b);
+      x7 = fma(x7, a, b);
+    }
+  }
+  double s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+}  // namespace perm
+
+using namespace perm;
+
+struct perm_matrix {
+  int n = 0;
+  double* d_col = nullptr;  // column-major, stride np
+};
+
+struct perm_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // scratch, allocated once
+  dd* partials = nullptr;  // kMaxBlocks dd
+  unsigned* ticket = nullptr;
+  double* d_out = nullptr;  // 8 doubles
+  int* d_err = nullptr;
+  unsigned long long* d_counters = nullptr;  // [0] queue head, [1] visited
+  double* h_out = nullptr;                   // pinned: 8 doubles + counters
+  // growable staging
+  unsigned char* d_stage = nullptr;
+  size_t d_stage_cap = 0;
+  unsigned char* h_stage = nullptr;
+  size_t h_stage_cap = 0;
+  double* d_trials = nullptr;
+  size_t d_trials_cap = 0;
+  int dense_occ[PERM_MAX_EXACT_N + 1] = {0};
+  std::string err;
+  std::mutex mu;
+};
+
+static const int kMaxBlocks = 8192;
+
+static int fail(perm_ctx* ctx, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  return code;
+}
+static int fail_cuda(perm_ctx* ctx, cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear sticky-free errors
+  return fail(ctx, e == cudaErrorMemoryAllocation ? PERM_ENOMEM : PERM_ECUDA, "%s: %s (%s)", what,
+              cudaGetErrorName(e), cudaGetErrorString(e));
+}
+#define CU(ctx, expr)                                     \
+  do {                                                    \
+    cudaError_t _e = (expr);                              \
+    if (_e != cudaSuccess) return fail_cuda(ctx, _e, #expr); \
+  } while (0)
+
+static int ensure_stage(perm_ctx* ctx, size_t bytes) {
+  bytes = (bytes + 255) & ~(size_t)255;
+  if (bytes > ctx->d_stage_cap) {
+    if (ctx->d_stage) cudaFree(ctx->d_stage);
+    ctx->d_stage = nullptr;
+    ctx->d_stage_cap = 0;
+    CU(ctx, cudaMalloc(&ctx->d_stage, bytes));
+    ctx->d_stage_cap = bytes;
+  }
+  if (bytes > ctx->h_stage_cap) {
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+    ctx->h_stage = nullptr;
+    ctx->h_stage_cap = 0;
+    CU(ctx, cudaMallocHost(&ctx->h_stage, bytes));
+    ctx->h_stage_cap = bytes;
+  }
+  return PERM_OK;
+}
+
+static double elem(const void* mat, int dtype, size_t idx) {
+  switch (dtype) {
+    case PERM_F32: return (double)static_cast<const float*>(mat)[idx];
+    case PERM_I32: return (double)static_cast<const int*>(mat)[idx];
+    default: return static_cast<const double*>(mat)[idx];
+  }
+}
+
+// Column-major, even-stride copy of a row-major host matrix.
+static void pack_columns(const void* mat, int n, int dtype, double* dst) {
+  const int np = (n + 1) & ~1;
+  for (int k = 0; k < n; k++) {
+    for (int j = 0; j < n; j++) dst[(size_t)k * np + j] = elem(mat, dtype, (size_t)j * n + k);
+    for (int j = n; j < np; j++) dst[(size_t)k * np + j] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+extern "C" int perm_version(void) { return 10000; }
+
+extern "C" int perm_device_count(void) {
+  int c = 0;
+  if (cudaGetDeviceCount(&c) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return c;
+}
+
+extern "C" const char* perm_status_string(int s) {
+  switch (s) {
+    case PERM_OK: return "ok";
+    case PERM_EINVAL: return "invalid argument";
+    case PERM_ECUDA: return "CUDA error";
+    case PERM_ENOMEM: return "out of memory";
+    case PERM_EUNSUPPORTED: return "unsupported";
+    case PERM_ETIMEOUT: return "device wait timed out";
+    case PERM_EIO: return "matrix input error";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char* perm_ctx_last_error(const perm_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+extern "C" void perm_ctx_destroy(perm_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->partials);
+  cudaFree(ctx->ticket);
+  cudaFree(ctx->d_out);
+  cudaFree(ctx->d_err);
+  cudaFree(ctx->d_counters);
+  cudaFree(ctx->d_stage);
+  cudaFree(ctx->d_trials);
+  if (ctx->h_out) cudaFreeHost(ctx->h_out);
+  if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+static int ctx_init(perm_ctx* ctx, int device) {
+  int count = 0;
+  CU(ctx, cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count)
+    return fail(ctx, PERM_EINVAL, "device %d not in [0, %d)", device, count);
+  ctx->device = device;
+  CU(ctx, cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CU(ctx, cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return fail(ctx, PERM_EUNSUPPORTED, "device %d is sm_%d%d; this build targets sm_100a (B200)", device,
+                prop.major, prop.minor);
+  ctx->num_sms = prop.multiProcessorCount;
+  CU(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  CU(ctx, cudaEventCreate(&ctx->ev0));
+  CU(ctx, cudaEventCreate(&ctx->ev1));
+  CU(ctx, cudaMalloc(&ctx->partials, sizeof(dd) * kMaxBlocks * 2));
+  CU(ctx, cudaMalloc(&ctx->ticket, sizeof(unsigned) * 4));
+  CU(ctx, cudaMalloc(&ctx->d_out, sizeof(double) * 8));
+  CU(ctx, cudaMalloc(&ctx->d_err, sizeof(int) * 4));
+  CU(ctx, cudaMalloc(&ctx->d_counters, sizeof(unsigned long long) * 4));
+  CU(ctx, cudaMemset(ctx->ticket, 0, sizeof(unsigned) * 4));
+  CU(ctx, cudaMemset(ctx->d_err, 0, sizeof(int) * 4));
+  CU(ctx, cudaMallocHost(&ctx->h_out, sizeof(double) * 16));
+  return PERM_OK;
+}
+
+extern "C" int perm_ctx_create(int device, perm_ctx** out) {
+  if (!out) return PERM_EINVAL;
+  *out = nullptr;
+  perm_ctx* ctx = new perm_ctx();
+  int rc = ctx_init(ctx, device);
+  if (rc != PERM_OK) {
+    // keep the message for the caller through a static copy
+    static thread_local std::string last;
+    last = ctx->err;
+    fprintf(stderr, "perm_ctx_create: %s\n", last.c_str());
+    perm_ctx_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return PERM_OK;
+}
+
+// Reads back out[0..7] and the error flag after the stream drains.
+static int finish_and_read(perm_ctx* ctx, int nout) {
+  CU(ctx, cudaMemcpyAsync(ctx->h_out, ctx->d_out, sizeof(double) * nout, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  CU(ctx, cudaMemcpyAsync(ctx->h_out + 8, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(ctx, cudaMemcpyAsync(ctx->h_out + 9, ctx->d_counters + 1, sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  CU(ctx, cudaStreamSynchronize(ctx->stream));
+  CU(ctx, cudaGetLastError());
+  int errflag = 0;
+  memcpy(&errflag, ctx->h_out + 8, sizeof(int));
+  if (errflag) {
+    cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return fail(ctx, PERM_ETIMEOUT, "shared-memory staging wait timed out on device %d", ctx->device);
+  }
+  return PERM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// dense exact
+// ---------------------------------------------------------------------------
+struct DensePlan {
+  int grid = 1, m = 3;
+  uint64_t block0 = 0, nblocks = 0;
+};
+
+static int dense_plan(perm_ctx* ctx, int n, int shard, int nshards, DensePlan* p) {
+  const void* fn = dense_kernel(n);
+  if (!fn) return fail(ctx, PERM_EUNSUPPORTED, "dense exact order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
+  size_t smem = dense_smem_bytes(n);
+  if (!ctx->dense_occ[n]) {
+    int occ = 0;
+    CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, smem));
+    ctx->dense_occ[n] = std::max(occ, 1);
+  }
+  const uint64_t total = n >= 1 ? (1ull << (n - 1)) : 1;
+  if (n < 4) {
+    p->grid = 1;
+    p->m = 0;
+    p->block0 = shard == 0 ? 0 : 1;
+    p->nblocks = 0;
+    return PERM_OK;
+  }
+  int grid = std::min(kMaxBlocks, ctx->num_sms * ctx->dense_occ[n]);
+  // Alignment m: each thread should own >= 64 aligned blocks when possible.
+  const uint64_t threads = (uint64_t)grid * 128 * (uint64_t)nshards;
+  int m = 3;
+  while (m < 20 && m < n - 1 && (total >> (m + 1)) >= threads * 64) m++;
+  const uint64_t all_blocks = total >> m;
+  const uint64_t b0 = all_blocks * (uint64_t)shard / (uint64_t)nshards;
+  const uint64_t b1 = all_blocks * (uint64_t)(shard + 1) / (uint64_t)nshards;
+  const uint64_t mine = b1 - b0;
+  if (mine < (uint64_t)grid * 128) grid = (int)std::max<uint64_t>(1, (mine + 127) / 128);
+  p->grid = grid;
+  p->m = m;
+  p->block0 = b0;
+  p->nblocks = mine;
+  return PERM_OK;
+}
+
+static int dense_launch(perm_ctx* ctx, const double* d_col, int n, const DensePlan& p) {
+  DenseArgs args;
+  args.colA = d_col;
+  args.np = (n + 1) & ~1;
+  args.m = p.m;
+  args.block0 = p.block0;
+  args.nblocks = p.nblocks;
+  args.partials = ctx->partials;
+  args.ticket = ctx->ticket;
+  args.out = ctx->d_out;
+  args.err = ctx->d_err;
+  void* kargs[] = {&args};
+  CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  CU(ctx, cudaLaunchKernel(dense_kernel(n), dim3(p.grid), dim3(128), kargs, dense_smem_bytes(n),
+                           ctx->stream));
+  CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  return PERM_OK;
+}
+
+static int dense_collect(perm_ctx* ctx, int n, const DensePlan& p, perm_result* out) {
+  int rc = finish_and_read(ctx, 2);
+  if (rc != PERM_OK) return rc;
+  float ms = 0;
+  CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  const double hi = ctx->h_out[0], lo = ctx->h_out[1];
+  out->hi = hi;
+  out->lo = lo;
+  out->value = hi + lo;
+  out->total_steps = std::ldexp(1.0, n - 1);
+  out->steps = n < 4 ? (p.block0 == 0 ? out->total_steps : 0.0) : std::ldexp((double)p.nblocks, p.m);
+  out->kernel_ms = ms;
+  out->kernel = PERM_KERNEL_DENSE;
+  out->n = n;
+  return PERM_OK;
+}
+
+static int check_dense_args(perm_ctx* ctx, const void* mat, int n, int dtype, const void* out) {
+  if (!ctx) return PERM_EINVAL;
+  if (!mat || !out) return fail(ctx, PERM_EINVAL, "null matrix or result pointer");
+  if (n < 1 || n > PERM_MAX_EXACT_N) return fail(ctx, PERM_EUNSUPPORTED, "order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
+  if (dtype != PERM_F64 && dtype != PERM_F32 && dtype != PERM_I32)
+    return fail(ctx, PERM_EINVAL, "unknown dtype %d", dtype);
+  return PERM_OK;
+}
+
+extern "C" int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int shard,
+                                      int nshards, perm_result* out) {
+  int rc = check_dense_args(ctx, mat, n, dtype, out);
+  if (rc) return rc;
+  if (nshards < 1 || shard < 0 || shard >= nshards)
+    return fail(ctx, PERM_EINVAL, "shard %d of %d", shard, nshards);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  const int np = (n + 1) & ~1;
+  const size_t bytes = sizeof(double) * (size_t)n * np;
+  if ((rc = ensure_stage(ctx, bytes))) return rc;
+  pack_columns(mat, n, dtype, reinterpret_cast<double*>(ctx->h_stage));
+  DensePlan p;
+  if ((rc = dense_plan(ctx, n, shard, nshards, &p))) return rc;
+  CU(ctx, cudaMemcpyAsync(ctx->d_stage, ctx->h_stage, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = dense_launch(ctx, reinterpret_cast<double*>(ctx->d_stage), n, p))) return rc;
+  return dense_collect(ctx, n, p, out);
+}
+
+extern "C" int perm_exact_dense(perm_ctx* ctx, const void* mat, int n, int dtype, perm_result* out) {
+  return perm_exact_dense_shard(ctx, mat, n, dtype, 0, 1, out);
+}
+
+extern "C" int perm_matrix_create_dense(perm_ctx* ctx, const void* mat, int n, int dtype, perm_matrix** out) {
+  int rc = check_dense_args(ctx, mat, n, dtype, out);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  const int np = (n + 1) & ~1;
+  const size_t bytes = sizeof(double) * (size_t)n * np;
+  std::vector<double> col((size_t)n * np);
+  pack_columns(mat, n, dtype, col.data());
+  perm_matrix* m = new perm_matrix();
+  m->n = n;
+  cudaError_t e = cudaMalloc(&m->d_col, bytes);
+  if (e != cudaSuccess) {
+    delete m;
+    return fail_cuda(ctx, e, "cudaMalloc(resident matrix)");
+  }
+  e = cudaMemcpy(m->d_col, col.data(), bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(m->d_col);
+    delete m;
+    return fail_cuda(ctx, e, "cudaMemcpy(resident matrix)");
+  }
+  *out = m;
+  return PERM_OK;
+}
+
+extern "C" void perm_matrix_destroy(perm_ctx* ctx, perm_matrix* m) {
+  if (!m) return;
+  if (ctx) cudaSetDevice(ctx->device);
+  cudaFree(m->d_col);
+  delete m;
+}
+
+extern "C" int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, perm_result* out) {
+  if (!ctx || !m || !out) return ctx ? fail(ctx, PERM_EINVAL, "null argument") : PERM_EINVAL;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  DensePlan p;
+  int rc = dense_plan(ctx, m->n, 0, 1, &p);
+  if (rc) return rc;
+  if ((rc = dense_launch(ctx, m->d_col, m->n, p))) return rc;
+  return dense_collect(ctx, m->n, p, out);
+}
+
+// ---------------------------------------------------------------------------
+// SkipPer
+// ---------------------------------------------------------------------------
+static inline uint32_t align16(uint32_t v) { return (v + 15u) & ~15u; }
+
+extern "C" int perm_exact_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
+                                 const double* rvals, const int* cptrs, const int* rows,
+                                 const double* cvals, perm_result* out) {
+  if (!ctx) return PERM_EINVAL;
+  if (!rptrs || !cols || !rvals || !cptrs || !rows || !cvals || !out)
+    return fail(ctx, PERM_EINVAL, "null CRS/CCS or result pointer");
+  if (n < 1 || n > PERM_MAX_EXACT_N) return fail(ctx, PERM_EUNSUPPORTED, "order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
+  const int nnz = rptrs[n];
+  if (nnz < 0 || nnz > n * n || cptrs[n] != nnz || rptrs[0] != 0 || cptrs[0] != 0)
+    return fail(ctx, PERM_EINVAL, "inconsistent CRS/CCS (rptrs[n]=%d, cptrs[n]=%d)", nnz, cptrs[n]);
+  for (int i = 0; i < n; i++)
+    if (rptrs[i + 1] < rptrs[i] || cptrs[i + 1] < cptrs[i])
+      return fail(ctx, PERM_EINVAL, "pointer arrays must be non-decreasing");
+  for (int p = 0; p < nnz; p++)
+    if (cols[p] < 0 || cols[p] >= n || rows[p] < 0 || rows[p] >= n)
+      return fail(ctx, PERM_EINVAL, "index out of range at entry %d", p);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  // x0 exactly as the reference SkipPer builds it (algo.h:751-760)
+  std::vector<double> x0(n);
+  for (int j = 0; j < n; j++) {
+    double rs = 0;
+    for (int p = rptrs[j]; p < rptrs[j + 1]; p++) rs += rvals[p];
+    x0[j] = -rs / 2.0;
+  }
+  for (int p = cptrs[n - 1]; p < cptrs[n]; p++) x0[rows[p]] += cvals[p];
+
+  SkipArgs a;
+  uint32_t off = align16(sizeof(double) * n);
+  a.off_cvals = off;
+  off = align16(off + sizeof(double) * nnz);
+  a.off_rptrs = off;
+  off = align16(off + sizeof(int) * (n + 1));
+  a.off_cptrs = off;
+  off = align16(off + sizeof(int) * (n + 1));
+  a.off_cols = off;
+  off = align16(off + sizeof(int) * nnz);
+  a.off_rows = off;
+  off = align16(off + sizeof(int) * nnz);
+  a.pack_bytes = off;
+  int rc = ensure_stage(ctx, off);
+  if (rc) return rc;
+  unsigned char* h = ctx->h_stage;
+  memset(h, 0, off);
+  memcpy(h, x0.data(), sizeof(double) * n);
+  memcpy(h + a.off_cvals, cvals, sizeof(double) * nnz);
+  memcpy(h + a.off_rptrs, rptrs, sizeof(int) * (n + 1));
+  memcpy(h + a.off_cptrs, cptrs, sizeof(int) * (n + 1));
+  memcpy(h + a.off_cols, cols, sizeof(int) * nnz);
+  memcpy(h + a.off_rows, rows, sizeof(int) * nnz);
+
+  const int block = 128;
+  const size_t smem = skipper_smem_bytes(a.pack_bytes, n, block);
+  if (smem > 227 * 1024) return fail(ctx, PERM_EUNSUPPORTED, "SkipPer operand needs %zu B of shared memory", smem);
+  CU(ctx, cudaFuncSetAttribute(skipper_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, skipper_kernel, block, smem));
+  occ = std::max(occ, 1);
+  const uint64_t total = 1ull << (n - 1);
+  int grid = std::min(kMaxBlocks, ctx->num_sms * occ);
+  const uint64_t threads = (uint64_t)grid * block;
+  uint64_t chunk = 256;
+  while (chunk < (1ull << 24) && total / (chunk * 2) >= threads * 32) chunk *= 2;
+  a.n = n;
+  a.total = total;
+  a.chunk = chunk;
+  a.nchunks = (total + chunk - 1) / chunk;
+  if (a.nchunks < threads) grid = (int)std::max<uint64_t>(1, (a.nchunks + block - 1) / block);
+  a.pack = ctx->d_stage;
+  a.next_chunk = ctx->d_counters;
+  a.visited = ctx->d_counters + 1;
+  a.partials = ctx->partials;
+  a.ticket = ctx->ticket;
+  a.out = ctx->d_out;
+  a.err = ctx->d_err;
+  CU(ctx, cudaMemcpyAsync(ctx->d_stage, h, off, cudaMemcpyHostToDevice, ctx->stream));
+  CU(ctx, cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * 2, ctx->stream));
+  void* kargs[] = {&a};
+  CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  CU(ctx, cudaLaunchKernel((const void*)skipper_kernel, dim3(grid), dim3(block), kargs, smem, ctx->stream));
+  CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  rc = finish_and_read(ctx, 2);
+  if (rc) return rc;
+  float ms = 0;
+  CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  unsigned long long vis = 0;
+  memcpy(&vis, ctx->h_out + 9, sizeof vis);
+  out->hi = ctx->h_out[0];
+  out->lo = ctx->h_out[1];
+  out->value = out->hi + out->lo;
+  out->steps = (double)vis;
+  out->total_steps = std::ldexp(1.0, n - 1);
+  out->kernel_ms = ms;
+  out->kernel = PERM_KERNEL_SKIPPER;
+  out->n = n;
+  return PERM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Monte Carlo
+// ---------------------------------------------------------------------------
+static int mc_run(perm_ctx* ctx, const std::vector<uint64_t>& rowmask, const std::vector<double>* dense,
+                  int n, bool scaling, int64_t trials, int y, int z, uint64_t seed, double* trial_values,
+                  perm_estimate* out) {
+  if (trials < 1) return fail(ctx, PERM_EINVAL, "trials must be >= 1 (got %lld)", (long long)trials);
+  if (scaling && (y < 1 || z < 0)) return fail(ctx, PERM_EINVAL, "scale interval must be >= 1 and scale times >= 0");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  const int np = (n + 1) & ~1;
+  McArgs a;
+  a.n = n;
+  a.np = np;
+  a.y = y;
+  a.z = z;
+  a.mask_bytes = sizeof(uint64_t) * np;
+  a.pack_bytes = a.mask_bytes + (scaling ? 2 * sizeof(double) * (size_t)n * np : 0);
+  int rc = ensure_stage(ctx, a.pack_bytes);
+  if (rc) return rc;
+  unsigned char* h = ctx->h_stage;
+  memset(h, 0, a.pack_bytes);
+  memcpy(h, rowmask.data(), sizeof(uint64_t) * n);
+  if (scaling) {
+    double* A = reinterpret_cast<double*>(h + a.mask_bytes);
+    double* AT = A + (size_t)n * np;
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) {
+        A[(size_t)i * np + j] = (*dense)[(size_t)i * n + j];
+        AT[(size_t)j * np + i] = (*dense)[(size_t)i * n + j];
+      }
+  }
+  const size_t smem = mc_smem_bytes(a.pack_bytes, scaling);
+  const void* fn = scaling ? (const void*)scaling_kernel : (const void*)rasmussen_kernel;
+  CU(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kMcBlock, smem));
+  occ = std::max(occ, 1);
+  const uint64_t warps_needed = (uint64_t)trials;
+  int grid = std::min<uint64_t>(std::min(kMaxBlocks, ctx->num_sms * occ), (warps_needed + 7) / 8);
+  grid = std::max(grid, 1);
+  if (trial_values && (size_t)trials > ctx->d_trials_cap) {
+    cudaFree(ctx->d_trials);
+    ctx->d_trials = nullptr;
+    ctx->d_trials_cap = 0;
+    CU(ctx, cudaMalloc(&ctx->d_trials, sizeof(double) * trials));
+    ctx->d_trials_cap = trials;
+  }
+  a.pack = ctx->d_stage;
+  a.trials = trials;
+  a.trial0 = 0;
+  a.seed = seed;
+  a.trial_out = trial_values ? ctx->d_trials : nullptr;
+  a.partials = reinterpret_cast<double*>(ctx->partials);
+  a.ticket = ctx->ticket;
+  a.out = ctx->d_out;
+  a.err = ctx->d_err;
+  CU(ctx, cudaMemcpyAsync(ctx->d_stage, h, a.pack_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  void* kargs[] = {&a};
+  CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  CU(ctx, cudaLaunchKernel(fn, dim3(grid), dim3(kMcBlock), kargs, smem, ctx->stream));
+  CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  if (trial_values)
+    CU(ctx, cudaMemcpyAsync(trial_values, ctx->d_trials, sizeof(double) * trials, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  rc = finish_and_read(ctx, 3);
+  if (rc) return rc;
+  float ms = 0;
+  CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  const double T = (double)trials, sum = ctx->h_out[0], sq = ctx->h_out[1];
+  out->trials = T;
+  out->sum = sum;
+  out->sum_sq = sq;
+  out->zero_trials = ctx->h_out[2];
+  out->mean = sum / T;
+  double var = T > 1 ? (sq - sum * out->mean) / (T - 1) : 0.0;
+  if (!(var > 0)) var = 0;
+  out->std_error = std::sqrt(var / T);
+  out->kernel_ms = ms;
+  return PERM_OK;
+}
+
+static int mc_dense(perm_ctx* ctx, const void* mat, int n, int dtype, bool scaling, int64_t trials, int y,
+                    int z, uint64_t seed, double* tv, perm_estimate* out) {
+  if (!ctx) return PERM_EINVAL;
+  if (!mat || !out) return fail(ctx, PERM_EINVAL, "null matrix or result pointer");
+  if (n < 1 || n > PERM_MAX_MC_N) return fail(ctx, PERM_EUNSUPPORTED, "order %d outside [1, %d]", n, PERM_MAX_MC_N);
+  if (dtype != PERM_F64 && dtype != PERM_F32 && dtype != PERM_I32) return fail(ctx, PERM_EINVAL, "unknown dtype %d", dtype);
+  std::vector<uint64_t> mask(n, 0);
+  std::vector<double> dense((size_t)n * n);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) {
+      double v = elem(mat, dtype, (size_t)i * n + j);
+      dense[(size_t)i * n + j] = v;
+      if (v != 0.0) mask[i] |= 1ull << j;
+    }
+  return mc_run(ctx, mask, &dense, n, scaling, trials, y, z, seed, tv, out);
+}
+
+static int mc_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols, bool scaling, int64_t trials,
+                     int y, int z, uint64_t seed, double* tv, perm_estimate* out) {
+  if (!ctx) return PERM_EINVAL;
+  if (!rptrs || !cols || !out) return fail(ctx, PERM_EINVAL, "null CRS or result pointer");
+  if (n < 1 || n > PERM_MAX_MC_N) return fail(ctx, PERM_EUNSUPPORTED, "order %d outside [1, %d]", n, PERM_MAX_MC_N);
+  std::vector<uint64_t> mask(n, 0);
+  std::vector<double> pattern((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) {
+    if (rptrs[i + 1] < rptrs[i]) return fail(ctx, PERM_EINVAL, "rptrs must be non-decreasing");
+    for (int p = rptrs[i]; p < rptrs[i + 1]; p++) {
+      if (cols[p] < 0 || cols[p] >= n) return fail(ctx, PERM_EINVAL, "column index out of range");
+      mask[i] |= 1ull << cols[p];
+      pattern[(size_t)i * n + cols[p]] = 1.0;  // the sparse estimators use the pattern only
+    }
+  }
+  return mc_run(ctx, mask, &pattern, n, scaling, trials, y, z, seed, tv, out);
+}
+
+extern "C" int perm_approx_rasmussen(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trials,
+                                     uint64_t seed, double* tv, perm_estimate* out) {
+  return mc_dense(ctx, mat, n, dtype, false, trials, 1, 0, seed, tv, out);
+}
+extern "C" int perm_approx_scaling(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trials, int y,
+                                   int z, uint64_t seed, double* tv, perm_estimate* out) {
+  return mc_dense(ctx, mat, n, dtype, true, trials, y, z, seed, tv, out);
+}
+extern "C" int perm_approx_rasmussen_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
+                                            int64_t trials, uint64_t seed, double* tv, perm_estimate* out) {
+  return mc_sparse(ctx, n, rptrs, cols, false, trials, 1, 0, seed, tv, out);
+}
+extern "C" int perm_approx_scaling_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
+                                          const int* cptrs, const int* rows, int64_t trials, int y, int z,
+                                          uint64_t seed, double* tv, perm_estimate* out) {
+  (void)cptrs;
+  (void)rows;
+  return mc_sparse(ctx, n, rptrs, cols, true, trials, y, z, seed, tv, out);
+}
+
+// ---------------------------------------------------------------------------
+// matrix input
+// ---------------------------------------------------------------------------
+extern "C" int perm_read_matrix(const char* path, int binary, int cap_n, double* out, int* n_out,
+                                int* header_nnz, char* type_out) {
+  if (!path || !out || !n_out) return PERM_EINVAL;
+  HostMatrix m;
+  std::string err = read_matrix_file(path, binary != 0, &m);
+  if (!err.empty()) {
+    fprintf(stderr, "perm_read_matrix: %s\n", err.c_str());
+    return PERM_EIO;
+  }
+  if (m.n > cap_n) return PERM_EUNSUPPORTED;
+  std::copy(m.a.begin(), m.a.end(), out);
+  *n_out = m.n;
+  if (header_nnz) *header_nnz = m.header_nnz;
+  if (type_out) snprintf(type_out, 8, "%s", m.type.c_str());
+  return PERM_OK;
+}
+
+extern "C" int perm_compress(int mode, double* mat, int n, int* cptrs, int* rows, double* cvals, int* rptrs,
+                             int* cols, double* rvals) {
+  if (!mat || n < 1 || !cptrs || !rows || !cvals || !rptrs || !cols || !rvals) return PERM_EINVAL;
+  if (mode < 0 || mode > 2) return PERM_EINVAL;
+  Compressed c;
+  compress_mode(mode, mat, n, &c);
+  std::copy(c.cptrs.begin(), c.cptrs.end(), cptrs);
+  std::copy(c.rptrs.begin(), c.rptrs.end(), rptrs);
+  std::copy(c.rows.begin(), c.rows.end(), rows);
+  std::copy(c.cols.begin(), c.cols.end(), cols);
+  std::copy(c.cvals.begin(), c.cvals.end(), cvals);
+  std::copy(c.rvals.begin(), c.rvals.end(), rvals);
+  return c.nnz();
+}
+
+// ---------------------------------------------------------------------------
+// measurement
+// ---------------------------------------------------------------------------
+extern "C" int perm_fp64_peak(perm_ctx* ctx, double* ops, double* kernel_ms) {
+  if (!ctx || !ops) return ctx ? fail(ctx, PERM_EINVAL, "null output") : PERM_EINVAL;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  const int block = 256, grid = ctx->num_sms * 8, iters = 4096;
+  fp64_peak_kernel<<<grid, block, 0, ctx->stream>>>(ctx->d_out, 64, 0.999999999, 1e-9);  // warm-up
+  CU(ctx, cudaGetLastError());
+  CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  fp64_peak_kernel<<<grid, block, 0, ctx->stream>>>(ctx->d_out, iters, 0.999999999, 1e-9);
+  CU(ctx, cudaGetLastError());
+  CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  CU(ctx, cudaEventSynchronize(ctx->ev1));
+  float ms = 0;
+  CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  const double lane_ops = (double)grid * block * iters * 16.0 * 8.0;
+  *ops = lane_ops / (ms * 1e-3);
+  if (kernel_ms) *kernel_ms = ms;
+  return PERM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// reference-signature entry points on a process default context
+// ---------------------------------------------------------------------------
+static perm_ctx* default_ctx() {
+  static std::once_flag once;
+  static perm_ctx* ctx = nullptr;
+  std::call_once(once, [] {
+    const char* d = getenv("PERM_DEVICE");
+    int dev = d ? atoi(d) : 0;
+    if (perm_ctx_create(dev, &ctx) != PERM_OK) ctx = nullptr;
+  });
+  return ctx;
+}
+
+static double shim_exact(const void* mat, int nov, int dtype) {
+  perm_ctx* ctx = default_ctx();
+  if (!ctx) return NAN;
+  perm_result r;
+  int rc = perm_exact_dense(ctx, mat, nov, dtype, &r);
+  if (rc != PERM_OK) {
+    fprintf(stderr, "perman_b200: %s\n", perm_ctx_last_error(ctx));
+    return NAN;
+  }
+  return r.value;
+}
+
+template <class T>
+static double shim_skipper(const T* mat, const int* rptrs, const int* cols, const int* cptrs, const int* rows,
+                           const T* cvals, int nov) {
+  perm_ctx* ctx = default_ctx();
+  if (!ctx) return NAN;
+  if (!mat || !rptrs || !cols || !cptrs || !rows || !cvals || nov < 1 || nov > PERM_MAX_EXACT_N) {
+    fprintf(stderr, "perman_b200: invalid SkipPer arguments\n");
+    return NAN;
+  }
+  const int nnz = rptrs[nov];
+  std::vector<double> rv(std::max(nnz, 1)), cv(std::max(nnz, 1));
+  for (int i = 0; i < nov; i++)
+    for (int p = rptrs[i]; p < rptrs[i + 1]; p++) rv[p] = (double)mat[(size_t)i * nov + cols[p]];
+  for (int p = 0; p < nnz; p++) cv[p] = (double)cvals[p];
+  perm_result r;
+  int rc = perm_exact_sparse(ctx, nov, rptrs, cols, rv.data(), cptrs, rows, cv.data(), &r);
+  if (rc != PERM_OK) {
+    fprintf(stderr, "perman_b200: %s\n", perm_ctx_last_error(ctx));
+    return NAN;
+  }
+  return r.value;
+}
+
+static uint64_t shim_seed() {
+  static std::atomic<uint64_t> calls{0};
+  return 0x5EED0000ull + calls.fetch_add(1);
+}
+
+static double shim_mc(const void* mat, int nov, int dtype, bool scaling, int times, int y, int z) {
+  perm_ctx* ctx = default_ctx();
+  if (!ctx) return NAN;
+  perm_estimate e;
+  int rc = scaling ? perm_approx_scaling(ctx, mat, nov, dtype, times, y, z, shim_seed(), nullptr, &e)
+                   : perm_approx_rasmussen(ctx, mat, nov, dtype, times, shim_seed(), nullptr, &e);
+  if (rc != PERM_OK) {
+    fprintf(stderr, "perman_b200: %s\n", perm_ctx_last_error(ctx));
+    return NAN;
+  }
+  return e.mean;
+}
+
+extern "C" {
+double gpu_perman64_xshared_coalescing_mshared_int(int* mat, int nov, int, int) { return shim_exact(mat, nov, PERM_I32); }
+double gpu_perman64_xshared_coalescing_mshared_float(float* mat, int nov, int, int) { return shim_exact(mat, nov, PERM_F32); }
+double gpu_perman64_xshared_coalescing_mshared_double(double* mat, int nov, int, int) { return shim_exact(mat, nov, PERM_F64); }
+double gpu_perman64_xshared_coalescing_mshared_skipper_int(int* mat, int* rptrs, int* cols, int* cptrs, int* rows,
+                                                           int* cvals, int nov, int, int) {
+  return shim_skipper(mat, rptrs, cols, cptrs, rows, cvals, nov);
+}
+double gpu_perman64_xshared_coalescing_mshared_skipper_float(float* mat, int* rptrs, int* cols, int* cptrs,
+                                                             int* rows, float* cvals, int nov, int, int) {
+  return shim_skipper(mat, rptrs, cols, cptrs, rows, cvals, nov);
+}
+double gpu_perman64_xshared_coalescing_mshared_skipper_double(double* mat, int* rptrs, int* cols, int* cptrs,
+                                                              int* rows, double* cvals, int nov, int, int) {
+  return shim_skipper(mat, rptrs, cols, cptrs, rows, cvals, nov);
+}
+double gpu_perman64_rasmussen_int(int* mat, int nov, int t) { return shim_mc(mat, nov, PERM_I32, false, t, 1, 0); }
+double gpu_perman64_rasmussen_float(float* mat, int nov, int t) { return shim_mc(mat, nov, PERM_F32, false, t, 1, 0); }
+double gpu_perman64_rasmussen_double(double* mat, int nov, int t) { return shim_mc(mat, nov, PERM_F64, false, t, 1, 0); }
+double gpu_perman64_approximation_int(int* mat, int nov, int t, int y, int z) { return shim_mc(mat, nov, PERM_I32, true, t, y, z); }
+double gpu_perman64_approximation_float(float* mat, int nov, int t, int y, int z) { return shim_mc(mat, nov, PERM_F32, true, t, y, z); }
+double gpu_perman64_approximation_double(double* mat, int nov, int t, int y, int z) { return shim_mc(mat, nov, PERM_F64, true, t, y, z); }
+double gpu_perman64_rasmussen_sparse(int* rptrs, int* cols, int nov, int nnz, int t, int grid_graph) {
+  (void)nnz;
+  (void)grid_graph;
+  perm_ctx* ctx = default_ctx();
+  if (!ctx) return NAN;
+  perm_estimate e;
+  if (perm_approx_rasmussen_sparse(ctx, nov, rptrs, cols, t, shim_seed(), nullptr, &e) != PERM_OK) {
+    fprintf(stderr, "perman_b200: %s\n", perm_ctx_last_error(ctx));
+    return NAN;
+  }
+  return e.mean;
+}
+double gpu_perman64_approximation_sparse(int* cptrs, int* rows, int* rptrs, int* cols, int nov, int nnz, int t,
+                                         int y, int z, int grid_graph) {
+  (void)nnz;
+  (void)grid_graph;
+  perm_ctx* ctx = default_ctx();
+  if (!ctx) return NAN;
+  perm_estimate e;
+  if (perm_approx_scaling_sparse(ctx, nov, rptrs, cols, cptrs, rows, t, y, z, shim_seed(), nullptr, &e) != PERM_OK) {
+    fprintf(stderr, "perman_b200: %s\n", perm_ctx_last_error(ctx));
+    return NAN;
+  }
+  return e.mean;
+}
+}  // extern "C"

@@ -1,0 +1,256 @@
+// mc.cu -- Monte-Carlo permanent estimators, one trial per warp.
+//
+// Rasmussen (replaces kernel_rasmussen, gpu_approximation_dense.cu:156-229, and
+// kernel_rasmussen_sparse, gpu_approximation_sparse.cu:198-290): per step take
+// the unextracted row with the fewest available nonzeros (lowest index on
+// ties), multiply the weight by that count and extract a uniformly chosen
+// available column.  An empty row ends the trial with weight 0.
+//
+// Scaling (replaces kernel_approximation, gpu_approximation_dense.cu:232-369, and
+// kernel_approximation_sparse, gpu_approximation_sparse.cu:292-452): same row
+// rule; every y steps run z Sinkhorn sweeps (columns then rows) over the
+// remaining submatrix in FP64; sample an available column with probability
+// proportional to d_r[row] * d_c[col]; weight *= 1 / p.  A zero column or row
+// sum ends the trial with weight 0.
+//
+// Both estimate the permanent of the 0/1 pattern of the matrix (the
+// reference's algorithms are documented for binary matrices only).
+//
+// B200 mapping: a warp runs one trial; lane l owns rows and columns l and
+// l + 32, so the minimum-degree row is one popc per lane plus a single
+// redux.sync minimum over (count << 8 | row), and each Sinkhorn sweep is a
+// column pass (lane = column, walking rows) and a row pass (lane = row, over
+// the transposed copy) with no bank conflicts.  Random numbers come from
+// Philox4x32-10 keyed by (seed) at counter (trial, step, tag), so trial t is
+// reproducible regardless of launch shape.  All FP64 operations use
+// explicitly rounded intrinsics in the same order as the CPU restatement, so
+// per-trial weights are bit-identical to it.  The trial weight is an FP32
+// significand with a separate exponent; trial values are accumulated in FP64.
+#include "mc.h"
+
+namespace perm {
+
+namespace {
+
+__device__ __forceinline__ int nth_set_bit(uint64_t m, int idx) {
+  for (int i = 0; i < idx; i++) m &= m - 1;
+  return __ffsll((long long)m) - 1;
+}
+
+// Row rule shared by both estimators: (count << 8 | row) minimum over the
+// unextracted rows; returns 0xffffffff if none is left.
+__device__ __forceinline__ unsigned min_row_key(const uint64_t* rowmask, int n, uint64_t colext,
+                                                uint64_t rowext, int lane) {
+  unsigned key = 0xffffffffu;
+  int r = lane;
+  if (r < n && !((rowext >> r) & 1))
+    key = ((unsigned)__popcll(rowmask[r] & ~colext) << 8) | (unsigned)r;
+  r = lane + 32;
+  if (r < n && !((rowext >> r) & 1)) {
+    unsigned k2 = ((unsigned)__popcll(rowmask[r] & ~colext) << 8) | (unsigned)r;
+    key = k2 < key ? k2 : key;
+  }
+  return __reduce_min_sync(0xffffffffu, key);
+}
+
+// Block + grid completion of the (sum, sum of squares, zeros) triple.
+__device__ __forceinline__ void finish3(double s, double s2, double z, double* slots, const McArgs& a) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    slots[warp * 3 + 0] = s;
+    slots[warp * 3 + 1] = s2;
+    slots[warp * 3 + 2] = z;
+  }
+  __syncthreads();
+  __shared__ bool is_last;
+  if (threadIdx.x == 0) {
+    double t0 = 0, t1 = 0, t2 = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      t0 += slots[w * 3 + 0];
+      t1 += slots[w * 3 + 1];
+      t2 += slots[w * 3 + 2];
+    }
+    a.partials[blockIdx.x * 3 + 0] = t0;
+    a.partials[blockIdx.x * 3 + 1] = t1;
+    a.partials[blockIdx.x * 3 + 2] = t2;
+    __threadfence();
+    unsigned prev = atomicAdd(a.ticket, 1u);
+    is_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last || threadIdx.x != 0) return;
+  __threadfence();
+  double t0 = 0, t1 = 0, t2 = 0;
+  for (unsigned b = 0; b < gridDim.x; b++) {
+    t0 += __ldcg(&a.partials[b * 3 + 0]);
+    t1 += __ldcg(&a.partials[b * 3 + 1]);
+    t2 += __ldcg(&a.partials[b * 3 + 2]);
+  }
+  a.out[0] = t0;
+  a.out[1] = t1;
+  a.out[2] = t2;
+  *a.ticket = 0u;
+  __threadfence();
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kMcBlock) rasmussen_kernel(McArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const uint64_t* rowmask = reinterpret_cast<const uint64_t*>(smem);
+  double* slots = reinterpret_cast<double*>(smem + a.pack_bytes);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(slots + (kMcBlock / 32) * 3);
+  const bool staged = stage_to_smem(smem, a.pack, a.mask_bytes, bar, a.err);
+
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int n = a.n;
+  double s = 0, s2 = 0, zeros = 0;
+  if (staged) {
+    for (uint64_t q = warp; q < a.trials; q += nwarps) {
+      const uint64_t t = a.trial0 + q;
+      uint64_t colext = 0, rowext = 0;
+      WExp w;
+      bool ok = true;
+      for (int step = 0; step < n; step++) {
+        const unsigned key = min_row_key(rowmask, n, colext, rowext, lane);
+        const int best = (int)(key >> 8), row = (int)(key & 0xffu);
+        if (best == 0) {
+          ok = false;
+          break;
+        }
+        w.mul((float)best);
+        const u32x4 rnd = philox_step(a.seed, t, (uint32_t)step, kTagRasmussen);
+        const int idx = (int)(((uint64_t)rnd.x * (uint64_t)best) >> 32);
+        const int col = nth_set_bit(rowmask[row] & ~colext, idx);
+        colext |= 1ull << col;
+        rowext |= 1ull << row;
+      }
+      const double v = ok ? w.value() : 0.0;
+      if (lane == 0) {
+        s += v;
+        s2 += v * v;
+        zeros += ok ? 0.0 : 1.0;
+        if (a.trial_out) a.trial_out[q] = v;
+      }
+    }
+  }
+  finish3(s, s2, zeros, slots, a);
+}
+
+__global__ void __launch_bounds__(kMcBlock) scaling_kernel(McArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int n = a.n, np = a.np;
+  const uint64_t* rowmask = reinterpret_cast<const uint64_t*>(smem);
+  const double* A = reinterpret_cast<const double*>(smem + a.mask_bytes);   // A[i * np + j]
+  const double* AT = A + (size_t)n * np;                                       // AT[j * np + i]
+  double* dwarp = reinterpret_cast<double*>(smem + a.pack_bytes);
+  double* slots = dwarp + (kMcBlock / 32) * 128;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(slots + (kMcBlock / 32) * 3);
+  const bool staged = stage_to_smem(smem, a.pack, a.pack_bytes, bar, a.err);
+
+  const int lane = threadIdx.x & 31;
+  double* dr = dwarp + (threadIdx.x >> 5) * 128;
+  double* dc = dr + 64;
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  double s = 0, s2 = 0, zeros = 0;
+  if (staged) {
+    for (uint64_t q = warp; q < a.trials; q += nwarps) {
+      const uint64_t t = a.trial0 + q;
+      dr[lane] = 1.0;
+      dr[lane + 32] = 1.0;
+      dc[lane] = 1.0;
+      dc[lane + 32] = 1.0;
+      __syncwarp();
+      uint64_t colext = 0, rowext = 0;
+      WExp w;
+      bool ok = true;
+      for (int it = 0; it < n && ok; it++) {
+        const unsigned key = min_row_key(rowmask, n, colext, rowext, lane);
+        const int row = (int)(key & 0xffu);
+        if (it % a.y == 0) {
+          for (int k = 0; k < a.z; k++) {
+            // column pass: lane owns columns lane, lane + 32
+            bool fail = false;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int j = lane + 32 * h;
+              if (j < n && !((colext >> j) & 1)) {
+                double cs = 0.0;
+                for (int i = 0; i < n; i++)
+                  if (!((rowext >> i) & 1)) cs = __dadd_rn(cs, __dmul_rn(dr[i], A[i * np + j]));
+                if (cs == 0.0)
+                  fail = true;
+                else
+                  dc[j] = __drcp_rn(cs);
+              }
+            }
+            if (__any_sync(0xffffffffu, fail)) {
+              ok = false;
+              break;
+            }
+            __syncwarp();
+            // row pass: lane owns rows lane, lane + 32 (reads the transposed copy)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int i = lane + 32 * h;
+              if (i < n && !((rowext >> i) & 1)) {
+                double rs = 0.0;
+                for (int j = 0; j < n; j++)
+                  if (!((colext >> j) & 1)) rs = __dadd_rn(rs, __dmul_rn(AT[j * np + i], dc[j]));
+                if (rs == 0.0)
+                  fail = true;
+                else
+                  dr[i] = __drcp_rn(rs);
+              }
+            }
+            if (__any_sync(0xffffffffu, fail)) {
+              ok = false;
+              break;
+            }
+            __syncwarp();
+          }
+          if (!ok) break;
+        }
+        const uint64_t avail = rowmask[row] & ~colext;
+        const double drow = dr[row];
+        double sum = 0.0;
+        for (uint64_t m = avail; m; m &= m - 1) sum = __dadd_rn(sum, __dmul_rn(drow, dc[__ffsll((long long)m) - 1]));
+        if (sum == 0.0) {
+          ok = false;
+          break;
+        }
+        const u32x4 rnd = philox_step(a.seed, t, (uint32_t)it, kTagScaling);
+        const double u = __dmul_rn(__dadd_rn(__dmul_rn((double)(rnd.x >> 5), 67108864.0), (double)(rnd.y >> 6)),
+                                   1.0 / 9007199254740992.0);
+        const double target = __dmul_rn(u, sum);
+        double run = 0.0, sp = 0.0;
+        int col = -1;
+        for (uint64_t m = avail; m; m &= m - 1) {
+          const int j = __ffsll((long long)m) - 1;
+          sp = __dmul_rn(drow, dc[j]);
+          run = __dadd_rn(run, sp);
+          col = j;
+          if (target < run) break;
+        }
+        w.mul(__double2float_rn(__ddiv_rn(sum, sp)));
+        colext |= 1ull << col;
+        rowext |= 1ull << row;
+        __syncwarp();
+      }
+      const double v = ok ? w.value() : 0.0;
+      if (lane == 0) {
+        s += v;
+        s2 += v * v;
+        zeros += ok ? 0.0 : 1.0;
+        if (a.trial_out) a.trial_out[q] = v;
+      }
+      __syncwarp();
+    }
+  }
+  finish3(s, s2, zeros, slots, a);
+}
+
+}  // namespace perm

@@ -1,0 +1,277 @@
+// perman_cli.cpp -- drop-in `perman` command line over libperman_b200.so.
+//
+// Mirrors the reference CLI (main.cu:315-590): the same flags and algorithm
+// ids, the same input format, the same "Result: <name> <value> in <seconds>"
+// line (printed with 17 significant digits instead of cout's 6).
+//   -m FILE | -f FILE   matrix file (the README documents -m, main.cu reads -f)
+//   -p ID               algorithm id (default 1)
+//   -s                  sparse algorithms        -b   binary (every entry 1)
+//   -a                  approximation            -x N trials (default 100000)
+//   -y N                scale interval (4)       -z N scale sweeps (5)
+//   -r N                preprocessing: 0 none, 1 sortOrder, 2 skipOrder
+//   -g                  GPU (the default)        -d N GPUs for multi-GPU ids (2)
+//   -t N                accepted, unused (host threads of the CPU algorithms)
+//   -c                  CPU algorithms: not part of this engine -> error
+//   --seed N            Monte-Carlo seed (default: time, like the reference)
+// The reference's grid-graph generator (-i, with -m/-n as grid sizes) is not
+// built; -n is accepted and ignored.
+#include <getopt.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "perman_b200.h"
+
+namespace {
+
+struct Options {
+  std::string file;
+  bool binary = false, sparse = false, approx = false, cpu = false, gpu = false, grid = false;
+  int algo = 1, threads = 16, gpu_num = 2, pre = 0;
+  int times = 100000, y = 4, z = 5;
+  long long seed = -1;
+};
+
+int usage(const char* msg) {
+  fprintf(stderr, "%s\n", msg);
+  return 1;
+}
+
+double now() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+void print_result(const char* name, double value, double seconds) {
+  printf("Result: %s %.17g in %.6f\n", name, value, seconds);
+  fflush(stdout);
+}
+
+int die(perm_ctx* ctx, int rc) {
+  fprintf(stderr, "perman: %s: %s\n", perm_status_string(rc), ctx ? perm_ctx_last_error(ctx) : "");
+  return 3;
+}
+
+// Multi-GPU exact dense: one host thread and context per device, shards of
+// the Gray range, double-double sum of the per-device results.
+int multi_gpu_dense(const std::vector<double>& a, int n, int gpus, perm_result* total) {
+  int avail = perm_device_count();
+  if (avail < 1) {
+    fprintf(stderr, "perman: no CUDA device\n");
+    return 3;
+  }
+  gpus = std::max(1, std::min(gpus, avail));
+  std::vector<perm_result> parts(gpus);
+  std::vector<int> rcs(gpus, 0);
+  std::vector<std::string> errs(gpus);
+  std::vector<std::thread> th;
+  for (int g = 0; g < gpus; g++) {
+    th.emplace_back([&, g] {
+      perm_ctx* ctx = nullptr;
+      rcs[g] = perm_ctx_create(g, &ctx);
+      if (rcs[g] == PERM_OK) {
+        rcs[g] = perm_exact_dense_shard(ctx, a.data(), n, PERM_F64, g, gpus, &parts[g]);
+        if (rcs[g] != PERM_OK) errs[g] = perm_ctx_last_error(ctx);
+      }
+      perm_ctx_destroy(ctx);
+    });
+  }
+  for (auto& t : th) t.join();
+  double hi = 0, lo = 0;
+  for (int g = 0; g < gpus; g++) {
+    if (rcs[g] != PERM_OK) {
+      fprintf(stderr, "perman: device %d: %s %s\n", g, perm_status_string(rcs[g]), errs[g].c_str());
+      return 3;
+    }
+    // double-double accumulate (TwoSum on the high parts)
+    double s = hi + parts[g].hi, bb = s - hi;
+    double e = (hi - (s - bb)) + (parts[g].hi - bb);
+    hi = s;
+    lo += e + parts[g].lo;
+  }
+  *total = parts[0];
+  total->hi = hi + lo;
+  total->lo = lo - (total->hi - hi);
+  total->value = total->hi;
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  Options o;
+  const char* short_opts = "bsr:t:f:gd:cap:x:y:z:im:n:";
+  const struct option long_opts[] = {
+      {"binary", 0, nullptr, 'b'},         {"sparse", 0, nullptr, 's'},
+      {"preprocessing", 1, nullptr, 'r'},  {"threads", 1, nullptr, 't'},
+      {"file", 1, nullptr, 'f'},           {"gpu", 0, nullptr, 'g'},
+      {"device", 1, nullptr, 'd'},         {"cpu", 0, nullptr, 'c'},
+      {"approximation", 0, nullptr, 'a'},  {"perman", 1, nullptr, 'p'},
+      {"numOfTimes", 1, nullptr, 'x'},     {"scaleIntervals", 1, nullptr, 'y'},
+      {"scaleTimes", 1, nullptr, 'z'},     {"grid", 0, nullptr, 'i'},
+      {"matrix", 1, nullptr, 'm'},         {"gridn", 1, nullptr, 'n'},
+      {"seed", 1, nullptr, 'S'},           {nullptr, 0, nullptr, 0}};
+  int c;
+  while ((c = getopt_long(argc, argv, short_opts, long_opts, nullptr)) != -1) {
+    if (optarg && optarg[0] == '-' && c != 'S') {
+      fprintf(stderr, "Option -%c requires an argument.\n", c);
+      return 1;
+    }
+    switch (c) {
+      case 'b': o.binary = true; break;
+      case 's': o.sparse = true; break;
+      case 'r': o.pre = atoi(optarg); break;
+      case 't': o.threads = atoi(optarg); break;
+      case 'f': o.file = optarg; break;
+      case 'm': o.file = optarg; break;
+      case 'g': o.gpu = true; break;
+      case 'd': o.gpu_num = atoi(optarg); break;
+      case 'c': o.cpu = true; break;
+      case 'a': o.approx = true; break;
+      case 'p': o.algo = atoi(optarg); break;
+      case 'x': o.times = atoi(optarg); break;
+      case 'y': o.y = atoi(optarg); break;
+      case 'z': o.z = atoi(optarg); break;
+      case 'i': o.grid = true; break;
+      case 'n': break;
+      case 'S': o.seed = atoll(optarg); break;
+      default: return 1;
+    }
+  }
+  for (int i = optind; i < argc; i++) printf("Non-option argument %s\n", argv[i]);
+  if (o.grid) return usage("perman: grid-graph mode (-i) is not part of the B200 engine");
+  if (o.file.empty()) return usage("Option -f (or -m) is a required argument.");
+  if (o.cpu && !o.gpu)
+    return usage("perman: the CPU algorithms (-c) are not part of the B200 engine; run with -g");
+  if (o.pre < 0 || o.pre > 2) return usage("perman: -r must be 0, 1 or 2");
+  if (o.seed < 0) o.seed = (long long)time(nullptr);
+
+  // read header first to size the buffer
+  FILE* fh = fopen(o.file.c_str(), "r");
+  if (!fh) {
+    fprintf(stderr, "perman: cannot open '%s'\n", o.file.c_str());
+    return 1;
+  }
+  int hn = 0;
+  if (fscanf(fh, "%d", &hn) != 1 || hn <= 0 || hn > 4096) {
+    fclose(fh);
+    fprintf(stderr, "perman: bad header in '%s'\n", o.file.c_str());
+    return 1;
+  }
+  fclose(fh);
+  std::vector<double> a((size_t)hn * hn);
+  int n = 0, hnnz = 0;
+  char type[8] = {0};
+  int rc = perm_read_matrix(o.file.c_str(), o.binary, hn, a.data(), &n, &hnnz, type);
+  if (rc != PERM_OK) return 1;
+  a.resize((size_t)n * n);
+  std::vector<int> cptrs(n + 1), rptrs(n + 1), rows((size_t)n * n), cols((size_t)n * n);
+  std::vector<double> cvals((size_t)n * n), rvals((size_t)n * n);
+  int nnz = perm_compress(o.pre, a.data(), n, cptrs.data(), rows.data(), cvals.data(), rptrs.data(), cols.data(),
+                          rvals.data());
+  if (nnz < 0) return usage("perman: compression failed");
+
+  perm_ctx* ctx = nullptr;
+  const double t0 = now();
+  rc = perm_ctx_create(0, &ctx);
+  if (rc != PERM_OK) {
+    fprintf(stderr, "perman: cannot use a B200: %s\n", perm_status_string(rc));
+    return 3;
+  }
+  int status = 0;
+  if (!o.approx) {
+    perm_result r;
+    const char* name = nullptr;
+    if (!o.sparse) {
+      static const char* names[] = {"gpu_perman64_xlocal", "gpu_perman64_xlocal", "gpu_perman64_xshared",
+                                    "gpu_perman64_xshared_coalescing",
+                                    "gpu_perman64_xshared_coalescing_mshared"};
+      if (o.algo >= 0 && o.algo <= 4) {
+        name = names[o.algo];
+        rc = perm_exact_dense(ctx, a.data(), n, PERM_F64, &r);
+      } else if (o.algo == 5 || o.algo == 6 || o.algo == 66) {
+        name = o.algo == 5   ? "gpu_perman64_xshared_coalescing_mshared_multigpu"
+               : o.algo == 6 ? "gpu_perman64_xshared_coalescing_mshared_multigpucpu_chunks"
+                             : "gpu_perman64_xshared_coalescing_mshared_multigpu_manual_distribution";
+        perm_ctx_destroy(ctx);
+        ctx = nullptr;
+        if (multi_gpu_dense(a, n, o.algo == 66 ? 4 : o.gpu_num, &r)) return 3;
+        rc = PERM_OK;
+      } else {
+        printf("Unknown Algorithm ID\n");
+        perm_ctx_destroy(ctx);
+        return 0;
+      }
+    } else {
+      static const char* snames[] = {nullptr,
+                                     "gpu_perman64_xlocal_sparse",
+                                     "gpu_perman64_xshared_sparse",
+                                     "gpu_perman64_xshared_coalescing_sparse",
+                                     "gpu_perman64_xshared_coalescing_mshared_sparse",
+                                     "gpu_perman64_xshared_coalescing_mshared_multigpu_sparse",
+                                     "gpu_perman64_xshared_coalescing_mshared_multigpucpu_chunks_sparse",
+                                     "gpu_perman64_xshared_coalescing_mshared_skipper",
+                                     "gpu_perman64_xshared_coalescing_mshared_multigpucpu_chunks_skipper"};
+      if ((o.algo >= 1 && o.algo <= 8) || o.algo == 66) {
+        name = o.algo == 66 ? "gpu_perman64_xshared_coalescing_mshared_multigpu_sparse_manual_distribution"
+                            : snames[o.algo];
+        rc = perm_exact_sparse(ctx, n, rptrs.data(), cols.data(), rvals.data(), cptrs.data(), rows.data(),
+                               cvals.data(), &r);
+      } else {
+        printf("Unknown Algorithm ID\n");
+        perm_ctx_destroy(ctx);
+        return 0;
+      }
+    }
+    if (rc != PERM_OK) {
+      status = die(ctx, rc);
+    } else {
+      printf("kernel in %.6f\n", r.kernel_ms * 1e-3);
+      print_result(name, r.value, now() - t0);
+    }
+  } else {
+    perm_estimate e;
+    const char* name = nullptr;
+    bool scaling = (o.algo == 2 || o.algo == 4);
+    if (o.algo < 1 || o.algo > 4) {
+      printf("Unknown Algorithm ID\n");
+      perm_ctx_destroy(ctx);
+      return 0;
+    }
+    if (!o.sparse) {
+      static const char* names[] = {nullptr, "gpu_perman64_rasmussen", "gpu_perman64_approximation",
+                                    "gpu_perman64_rasmussen_multigpucpu_chunks",
+                                    "gpu_perman64_approximation_multigpucpu_chunks"};
+      name = names[o.algo];
+      rc = scaling ? perm_approx_scaling(ctx, a.data(), n, PERM_F64, o.times, o.y, o.z, (uint64_t)o.seed, nullptr, &e)
+                   : perm_approx_rasmussen(ctx, a.data(), n, PERM_F64, o.times, (uint64_t)o.seed, nullptr, &e);
+    } else {
+      static const char* names[] = {nullptr, "gpu_perman64_rasmussen_sparse", "gpu_perman64_approximation_sparse",
+                                    "gpu_perman64_rasmussen_multigpucpu_chunks_sparse",
+                                    "gpu_perman64_approximation_multigpucpu_chunks_sparse"};
+      name = names[o.algo];
+      rc = scaling ? perm_approx_scaling_sparse(ctx, n, rptrs.data(), cols.data(), cptrs.data(), rows.data(), o.times,
+                                                o.y, o.z, (uint64_t)o.seed, nullptr, &e)
+                   : perm_approx_rasmussen_sparse(ctx, n, rptrs.data(), cols.data(), o.times, (uint64_t)o.seed,
+                                                  nullptr, &e);
+    }
+    if (rc != PERM_OK) {
+      status = die(ctx, rc);
+    } else {
+      printf("kernel in %.6f\n", e.kernel_ms * 1e-3);
+      printf("number of zeros: %.0f\n", e.zero_trials);
+      printf("std error: %.17g (%.0f trials, seed %lld)\n", e.std_error, e.trials, o.seed);
+      print_result(name, e.mean, now() - t0);
+    }
+  }
+  perm_ctx_destroy(ctx);
+  return status;
+}

@@ -1,0 +1,56 @@
+"""The C-ABI library loads and exports every symbol include/perman_b200.h declares
+(no compute calls: runs without a GPU)."""
+import ctypes
+import re
+import subprocess
+
+import pytest
+from conftest import ROOT
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "perman_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = set(re.findall(r"\b((?:perm|gpu_perman64)_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert "perm_exact_dense" in names and "perm_exact_sparse" in names
+    assert len(names) >= 30
+
+
+def test_library_exports_every_declared_symbol(pb):
+    lib = pb.load_library()
+    out = subprocess.run(["nm", "-D", "--defined-only", str(pb.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r"\bT\s+(\w+)", out))
+    missing = [n for n in declared_symbols() if n not in exported]
+    assert not missing, f"declared but not exported: {missing}"
+    for n in declared_symbols():
+        assert getattr(lib, n) is not None
+    assert set(pb.EXPORTED_SYMBOLS) <= exported
+
+
+def test_version_and_status_strings(pb):
+    lib = pb.load_library()
+    assert lib.perm_version() >= 10000
+    assert lib.perm_status_string(0) == b"ok"
+    assert b"invalid" in lib.perm_status_string(-1)
+
+
+def test_no_device_fails_loudly(pb):
+    lib = pb.load_library()
+    if lib.perm_device_count() > 0:
+        pytest.skip("a GPU is present")
+    h = ctypes.c_void_p()
+    rc = lib.perm_ctx_create(0, ctypes.byref(h))
+    assert rc != 0 and not h.value
+    with pytest.raises(pb.PermError):
+        pb.Engine(0)
+
+
+def test_missing_library_raises(pb, tmp_path):
+    with pytest.raises(pb.PermError):
+        pb.load_library(tmp_path / "nope.so")

@@ -1,0 +1,134 @@
+"""Dense exact Ryser kernel on the B200 against the oracle (tolerance 1e-10
+relative, the exact-algorithm bar; integer inputs that fit are compared exactly)."""
+import math
+
+import numpy as np
+import pytest
+from conftest import bernoulli, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+@pytest.mark.parametrize("n", list(range(1, 25)))
+def test_orders_1_to_24_vs_oracle(engine, orc, n):
+    rng = np.random.default_rng(1000 + n)
+    for kind in ("binary", "int", "real", "signed"):
+        if kind == "binary":
+            A = bernoulli(rng, n, 0.5) if n > 1 else np.ones((1, 1))
+        elif kind == "int":
+            A = rng.integers(0, 5, (n, n)).astype(float)
+        elif kind == "real":
+            A = 1.0 - rng.random((n, n))
+        else:
+            A = rng.standard_normal((n, n))
+        r = engine.exact_dense(A)
+        want = orc.perm_dd(A)
+        if kind in ("binary", "int"):
+            exact = orc.perm_exact_int(A)[0]
+            assert rel_err(r.value, exact) < 1e-13, (kind, r.value, exact)
+        else:
+            # signed matrices cancel heavily: compare against the oracle's scale
+            scale = max(abs(want[0]), 1e-300)
+            assert abs(r.value - want[0]) / scale < (TOL if kind == "real" else 1e-8), (kind, r.value, want)
+        assert r.total_steps == 2.0 ** (n - 1)
+
+
+def test_golden_vectors(engine, golden):
+    for name, c in golden.items():
+        r = engine.exact_dense(c["A"])
+        want = int(c["exact"]) if "exact" in c else c["dd"][0] + c["dd"][1]
+        assert rel_err(r.value, want) < TOL, (name, r.value, want)
+
+
+def test_dtypes_agree(engine):
+    rng = np.random.default_rng(3)
+    A = rng.integers(0, 5, (20, 20))
+    v64 = engine.exact_dense(A.astype(np.float64)).value
+    assert engine.exact_dense(A.astype(np.int32)).value == v64
+    assert engine.exact_dense(A.astype(np.float32)).value == v64
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 12, 18])
+def test_all_ones_factorial(engine, n):
+    assert engine.exact_dense(np.ones((n, n))).value == math.factorial(n)
+
+
+def test_identity_permutation_zero_row(engine):
+    rng = np.random.default_rng(4)
+    for n in (5, 17, 26):
+        P = np.eye(n)[rng.permutation(n)]
+        assert engine.exact_dense(P).value == 1.0
+        Z = rng.random((n, n))
+        Z[rng.integers(n)] = 0
+        assert engine.exact_dense(Z).value == 0.0
+
+
+@pytest.mark.parametrize("nshards", [2, 3, 7])
+def test_shards_sum_to_whole(engine, nshards):
+    rng = np.random.default_rng(5)
+    A = bernoulli(rng, 27, 0.5) * rng.integers(1, 5, (27, 27))
+    whole = engine.exact_dense(A)
+    hi = lo = 0.0
+    for s in range(nshards):
+        r = engine.exact_dense_shard(A, s, nshards)
+        hi, lo = hi + r.hi, lo + r.lo
+    assert rel_err(hi + lo, whole.value) < 1e-14
+
+
+def test_resident_matrix_matches_one_shot(engine):
+    rng = np.random.default_rng(6)
+    A = 1.0 - rng.random((25, 25))
+    m = engine.upload_dense(A)
+    try:
+        assert m.run().value == engine.exact_dense(A).value
+    finally:
+        m.free()
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("n", [36, 40])
+def test_full_size_invariances(engine, n):
+    """At the benchmark sizes the oracle is too slow; use size-independent
+    properties: row/column permutation and transpose invariance, and exact
+    scaling of a row by 2 on an integer matrix."""
+    rng = np.random.default_rng(n)
+    A = bernoulli(rng, n, 0.5) * rng.integers(1, 5, (n, n))
+    base = engine.exact_dense(A).value
+    Pm = A[rng.permutation(n)][:, rng.permutation(n)]
+    assert rel_err(engine.exact_dense(Pm).value, base) < TOL
+    assert rel_err(engine.exact_dense(A.T.copy()).value, base) < TOL
+    B = A.copy()
+    B[3] *= 2
+    assert rel_err(engine.exact_dense(B).value, 2 * base) < TOL
+
+
+def test_errors_are_reported(engine, pb):
+    with pytest.raises(pb.PermError) as e:
+        engine.exact_dense(np.ones((65, 65)))
+    assert e.value.status == pb.PERM_EUNSUPPORTED
+    with pytest.raises(pb.PermError):
+        engine.exact_dense(np.ones((3, 4)))
+    # the context stays usable after an error
+    assert engine.exact_dense(np.ones((5, 5))).value == 120.0
+
+
+def test_reference_signature_entry_points(pb):
+    rng = np.random.default_rng(8)
+    A = bernoulli(rng, 15, 0.5)
+    want = pb.default_engine().exact_dense(A).value
+    assert pb.gpu_perman64_xshared_coalescing_mshared(A, 15, 2048, 256) == want
+    lib = pb.load_library()
+    Ai = np.ascontiguousarray(A, dtype=np.int32)
+    assert lib.gpu_perman64_xshared_coalescing_mshared_int(Ai.ctypes.data_as(pb._P), 15, 2048, 256) == want
+
+
+def test_reference_gpu_kernel_same_inputs(engine, ref):
+    """The reference's own -p4 kernel (built for sm_100a) on the same binary
+    matrix; its FP32 X is exact for small integer inputs."""
+    rng = np.random.default_rng(9)
+    A = bernoulli(rng, 20, 0.5)
+    import ctypes
+    Ac = np.ascontiguousarray(A)
+    theirs = ref.lib.ref_gpu_dense_mshared_f64(Ac.ctypes.data_as(ctypes.c_void_p), 20, 2048, 128)
+    assert rel_err(engine.exact_dense(A).value, theirs) < 1e-12

@@ -1,0 +1,102 @@
+"""Monte-Carlo trial kernels on the B200: per-trial weights bit-identical to the
+oracle's CPU restatement (same Philox streams, same FP64 operation order), and
+estimates within the stated standard error of the exact permanent."""
+import math
+
+import numpy as np
+import pytest
+from conftest import bernoulli
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n", [1, 7, 20, 33, 64])
+def test_rasmussen_trials_bit_identical(engine, orc, n):
+    rng = np.random.default_rng(n)
+    A = bernoulli(rng, n, 0.5) if n > 1 else np.ones((1, 1))
+    e = engine.rasmussen(A, 3000, seed=42, keep_trials=True)
+    want = orc.rasmussen_trials(A, 42, 0, 3000)
+    np.testing.assert_array_equal(e.trial_values, want)
+
+
+@pytest.mark.parametrize("n,y,z", [(6, 1, 1), (20, 4, 5), (40, 4, 5), (64, 2, 3)])
+def test_scaling_trials_bit_identical(engine, orc, n, y, z):
+    rng = np.random.default_rng(100 + n)
+    A = bernoulli(rng, n, 0.5)
+    e = engine.scaling(A, 1000, y, z, seed=7, keep_trials=True)
+    want = orc.scaling_trials(A, y, z, 7, 0, 1000)
+    np.testing.assert_array_equal(e.trial_values, want)
+
+
+def test_estimates_within_standard_error(engine, orc):
+    rng = np.random.default_rng(5)
+    A = bernoulli(rng, 16, 0.5)
+    exact = orc.perm_exact_int(A)[0]
+    r = engine.rasmussen(A, 200000, seed=1)
+    s = engine.scaling(A, 200000, 4, 5, seed=2)
+    for est in (r, s):
+        assert est.std_error > 0
+        assert abs(est.mean - exact) < 5 * est.std_error
+    assert s.std_error < r.std_error  # scaling reduces the variance
+
+
+def test_mean_matches_trial_values(engine):
+    rng = np.random.default_rng(6)
+    A = bernoulli(rng, 30, 0.5)
+    e = engine.scaling(A, 5000, seed=3, keep_trials=True)
+    assert abs(e.mean - e.trial_values.mean()) <= 1e-12 * abs(e.mean)
+    assert e.zero_trials == float((e.trial_values == 0).sum())
+
+
+def test_streams_independent_of_trial_count(engine):
+    rng = np.random.default_rng(7)
+    A = bernoulli(rng, 25, 0.5)
+    a = engine.rasmussen(A, 1000, seed=9, keep_trials=True).trial_values
+    b = engine.rasmussen(A, 77777, seed=9, keep_trials=True).trial_values
+    np.testing.assert_array_equal(a, b[:1000])
+
+
+def test_sparse_equals_dense_pattern(engine, pb):
+    rng = np.random.default_rng(8)
+    A = bernoulli(rng, 24, 0.4)
+    c = pb.compress(0, A)
+    d = engine.rasmussen(A, 4000, seed=5, keep_trials=True).trial_values
+    s = engine.rasmussen_sparse(24, c["rptrs"], c["cols"], 4000, seed=5, keep_trials=True).trial_values
+    np.testing.assert_array_equal(d, s)
+    d = engine.scaling(A, 2000, 4, 5, seed=5, keep_trials=True).trial_values
+    s = engine.scaling_sparse(24, c["rptrs"], c["cols"], c["cptrs"], c["rows"], 2000, 4, 5, seed=5,
+                              keep_trials=True).trial_values
+    np.testing.assert_array_equal(d, s)
+
+
+def test_agrees_with_reference_estimator(engine, ref, orc):
+    """The reference's own CPU estimators (different RNG) and ours estimate the
+    same quantity: both within combined standard error of the exact value."""
+    rng = np.random.default_rng(9)
+    A = bernoulli(rng, 12, 0.5)
+    exact = orc.perm_exact_int(A)[0]
+    ours = engine.rasmussen(A, 100000, seed=11)
+    theirs = ref.rasmussen(A, 100000, 4)
+    assert abs(ours.mean - exact) < 5 * ours.std_error
+    assert abs(theirs - exact) < 5 * ours.std_error * 1.5
+    ours_s = engine.scaling(A, 50000, 4, 5, seed=12)
+    theirs_s = ref.approximation(A, 50000, 4, 5, 4)
+    assert abs(theirs_s - exact) < 6 * ours_s.std_error * 1.5
+
+
+def test_bad_arguments(engine, pb):
+    A = np.ones((5, 5))
+    with pytest.raises(pb.PermError):
+        engine.rasmussen(A, 0)
+    with pytest.raises(pb.PermError):
+        engine.scaling(A, 10, scale_intervals=0)
+    with pytest.raises(pb.PermError):
+        engine.rasmussen(np.ones((65, 65)), 10)
+
+
+def test_reference_signature_mc(pb):
+    A = np.ones((8, 8))
+    # every trial of J_n gives exactly n!
+    assert pb.gpu_perman64_rasmussen(A, 8, 1000) == math.factorial(8)
+    v = pb.gpu_perman64_approximation(A, 8, 1000, 4, 5)
+    assert abs(v - math.factorial(8)) < 1e-6 * math.factorial(8)

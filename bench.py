@@ -289,8 +289,19 @@ def main():
     }
     line["clocks"] = clk.summary()
 
+    line["config"]["kernel"] = {1: "FP64-X register kernel", 3: "int32-X register kernel"}.get(r.kernel, r.kernel)
     if rank == 0 and not args.no_secondary:
         line["secondary"] = secondary(pb, eng)
+        # the same n=40 matrix through the FP64-X kernel (the kernel used for real-valued inputs)
+        f64 = eng.upload_dense(A, variant=pb.PERM_KERNEL_DENSE)
+        f64.run()
+        fr = f64.run()
+        f64.free()
+        line["secondary"]["dense_n40_fp64x_same_matrix"] = {
+            "kernel_ms": fr.kernel_ms, "steps_per_s": total_steps / (fr.kernel_ms * 1e-3),
+            "fp64_frac_of_measured_peak": total_steps * ops_per_step / (fr.kernel_ms * 1e-3) / peak_ops,
+            "rel_diff_vs_headline": abs(fr.value - perm_value) / abs(perm_value)}
+        line["secondary"]["reference_gpu_p4_same_box"] = reference_gpu(A)
     if rank == 0 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1
@@ -307,6 +318,51 @@ def main():
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+class _Quiet:
+    """Silence fd 1 (the reference's functions print progress lines)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        os.close(devnull)
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def reference_gpu(A40):
+    """The reference's own -p4 kernel (built for sm_100a from its sources) on the
+    same box: the n=30 binary case and a 32-order slice of the headline matrix."""
+    try:
+        import ctypes
+
+        sys.path.insert(0, str(ROOT / "oracle"))
+        from oracle import Reference
+
+        ref = Reference()
+        out = {}
+        rng = np.random.default_rng(101)
+        while True:
+            m = (rng.random((30, 30)) < 0.5).astype(np.float64)
+            if m.any(0).all() and m.any(1).all():
+                break
+        for name, M in (("n30_binary", m), ("n32_int_slice_of_n40", np.ascontiguousarray(A40[:32, :32], dtype=np.float64))):
+            Mi = np.ascontiguousarray(M, dtype=np.int32)
+            with _Quiet():
+                ref.lib.ref_gpu_dense_mshared_i32(Mi.ctypes.data_as(ctypes.c_void_p), M.shape[0], 2048, 256)
+                t = time.perf_counter()
+                v = ref.lib.ref_gpu_dense_mshared_i32(Mi.ctypes.data_as(ctypes.c_void_p), M.shape[0], 2048, 256)
+                dt = time.perf_counter() - t
+            out[name] = {"seconds_incl_alloc_copy": dt, "steps_per_s": 2.0 ** (M.shape[0] - 1) / dt, "value": v}
+        return out
+    except Exception as e:  # reported, never fatal
+        return {"unavailable": str(e)}
 
 
 def secondary(pb, eng):
@@ -328,12 +384,25 @@ def secondary(pb, eng):
             break
     B = mk * (1.0 - rng.random((36, 36)))
     c = pb.compress(2, B)
-    s = eng.exact_sparse(c["n"], c["rptrs"], c["cols"], c["rvals"], c["cptrs"], c["rows"], c["cvals"])
-    d = eng.exact_dense(c["mat"])
-    out["skipper_n36_d020_real"] = {"kernel_ms": s.kernel_ms, "visited": s.steps, "dense_equivalent": s.total_steps,
-                                    "steps_per_s": s.total_steps / (s.kernel_ms * 1e-3), "permanent": s.value,
-                                    "dense_kernel_ms_same_matrix": d.kernel_ms,
-                                    "rel_diff_vs_dense_kernel": abs(s.value - d.value) / abs(d.value)}
+    s = eng.exact_sparse(c["n"], c["rptrs"], c["cols"], c["rvals"], c["cptrs"], c["rows"], c["cvals"],
+                         variant=pb.PERM_KERNEL_SKIPPER)
+    d = eng.exact_sparse(c["n"], c["rptrs"], c["cols"], c["rvals"], c["cptrs"], c["rows"], c["cvals"])
+    out["sparse_n36_d020_real"] = {"skipper_kernel_ms": s.kernel_ms, "skipper_visited": s.steps,
+                                   "dense_equivalent": s.total_steps,
+                                   "skipper_steps_per_s": s.total_steps / (s.kernel_ms * 1e-3),
+                                   "auto_kernel": d.kernel, "auto_kernel_ms": d.kernel_ms,
+                                   "auto_steps_per_s": d.total_steps / (d.kernel_ms * 1e-3), "permanent": d.value,
+                                   "rel_diff_skipper_vs_auto": abs(s.value - d.value) / abs(d.value)}
+    # a sparse binary case where SkipPer skips most of the walk
+    rng = np.random.default_rng(36)
+    P = ((np.eye(36) + np.eye(36)[rng.permutation(36)] + np.eye(36)[rng.permutation(36)]) > 0).astype(np.float64)
+    cp = pb.compress(2, P)
+    sp = eng.exact_sparse(cp["n"], cp["rptrs"], cp["cols"], cp["rvals"], cp["cptrs"], cp["rows"], cp["cvals"],
+                          variant=pb.PERM_KERNEL_SKIPPER)
+    dp = eng.exact_dense(cp["mat"])
+    out["sparse_n36_three_per_row_binary"] = {"skipper_kernel_ms": sp.kernel_ms, "skipper_visited": sp.steps,
+                                              "dense_equivalent": sp.total_steps, "dense_kernel_ms": dp.kernel_ms,
+                                              "permanent": sp.value}
     rng = np.random.default_rng(55)
     C = (rng.random((64, 64)) < 0.5).astype(np.float64)
     e = eng.rasmussen(C, 200000, seed=1)

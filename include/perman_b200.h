@@ -46,6 +46,7 @@ extern "C" {
 /* ---- kernels (perm_result.kernel) ---------------------------------------- */
 #define PERM_KERNEL_DENSE 1   /* register-X Gray-code Ryser                 */
 #define PERM_KERNEL_SKIPPER 2 /* SkipPer on CRS/CCS                          */
+#define PERM_KERNEL_DENSE_INT 3 /* int32-X Gray-code Ryser (integer matrices) */
 
 /* Limits of this build. */
 #define PERM_MAX_EXACT_N 64  /* Gray indices are 64-bit                 */
@@ -99,10 +100,26 @@ int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int
  * gpu_perman64_xshared_coalescing_mshared_skipper (gpu_exact_sparse.cu:1124). */
 int perm_exact_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols, const double* rvals,
                       const int* cptrs, const int* rows, const double* cvals, perm_result* out);
+/* As perm_exact_sparse with an explicit kernel.  variant 0 (what
+ * perm_exact_sparse uses) estimates the share of vanishing Gray terms from a
+ * fixed sample of 2048 indices and runs SkipPer when at least 75% vanish, the
+ * register kernels on the same (CRS) matrix otherwise; PERM_KERNEL_SKIPPER,
+ * PERM_KERNEL_DENSE and PERM_KERNEL_DENSE_INT force a kernel.  perm_result.kernel
+ * reports which ran. */
+int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, const int* cols, const double* rvals,
+                         const int* cptrs, const int* rows, const double* cvals, int variant, perm_result* out);
+
+/* Dense Ryser with an explicit kernel: variant 0 picks automatically (the
+ * int32-X kernel for integer matrices whose grouped row products provably fit
+ * in int32, the FP64-X kernel otherwise), PERM_KERNEL_DENSE forces FP64 X,
+ * PERM_KERNEL_DENSE_INT forces int32 X (PERM_EUNSUPPORTED if not exact). */
+int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard, int nshards,
+                        perm_result* out);
 
 /* Device-resident dense matrices: upload once, run many times (no host copy
  * inside perm_exact_dense_resident). */
 int perm_matrix_create_dense(perm_ctx* ctx, const void* mat, int n, int dtype, perm_matrix** out);
+int perm_matrix_create_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, perm_matrix** out);
 void perm_matrix_destroy(perm_ctx* ctx, perm_matrix* m);
 int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, perm_result* out);
 

@@ -29,15 +29,16 @@ CLI_PATH = PKG_DIR / "bin" / "perman"
 
 PERM_OK, PERM_EINVAL, PERM_ECUDA, PERM_ENOMEM, PERM_EUNSUPPORTED, PERM_ETIMEOUT, PERM_EIO = 0, -1, -2, -3, -4, -5, -6
 PERM_F64, PERM_F32, PERM_I32 = 0, 1, 2
-PERM_KERNEL_DENSE, PERM_KERNEL_SKIPPER = 1, 2
+PERM_KERNEL_DENSE, PERM_KERNEL_SKIPPER, PERM_KERNEL_DENSE_INT = 1, 2, 3
 MAX_EXACT_N = 64
 MAX_MC_N = 64
 
 # Every extern "C" symbol declared in include/perman_b200.h.
 EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
-    "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_exact_sparse",
-    "perm_matrix_create_dense", "perm_matrix_destroy", "perm_exact_dense_resident",
+    "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_exact_dense_ex",
+    "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
+    "perm_exact_dense_resident",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
     "perm_approx_scaling_sparse", "perm_read_matrix", "perm_compress", "perm_fp64_peak",
     "gpu_perman64_xshared_coalescing_mshared_int", "gpu_perman64_xshared_coalescing_mshared_float",
@@ -92,7 +93,10 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_ctx_last_error": (ctypes.c_char_p, [_P]), "perm_status_string": (ctypes.c_char_p, [i]),
         "perm_exact_dense": (i, [_P, _P, i, i, ctypes.POINTER(PermResult)]),
         "perm_exact_dense_shard": (i, [_P, _P, i, i, i, i, ctypes.POINTER(PermResult)]),
+        "perm_exact_dense_ex": (i, [_P, _P, i, i, i, i, i, ctypes.POINTER(PermResult)]),
+        "perm_matrix_create_dense_ex": (i, [_P, _P, i, i, i, ctypes.POINTER(_P)]),
         "perm_exact_sparse": (i, [_P, i, _P, _P, _P, _P, _P, _P, ctypes.POINTER(PermResult)]),
+        "perm_exact_sparse_ex": (i, [_P, i, _P, _P, _P, _P, _P, _P, i, ctypes.POINTER(PermResult)]),
         "perm_matrix_create_dense": (i, [_P, _P, i, i, ctypes.POINTER(_P)]),
         "perm_matrix_destroy": (None, [_P, _P]),
         "perm_exact_dense_resident": (i, [_P, _P, ctypes.POINTER(PermResult)]),
@@ -194,37 +198,45 @@ class Engine:
             raise PermError(rc, self.lib.perm_ctx_last_error(self.ctx).decode())
 
     # ---- exact ----
-    def exact_dense(self, mat) -> ExactResult:
+    def exact_dense(self, mat, variant: int = 0) -> ExactResult:
+        """Dense Ryser; variant 0 = automatic, PERM_KERNEL_DENSE = FP64 X, PERM_KERNEL_DENSE_INT = int32 X."""
         a, dt = _as_matrix(mat)
         r = PermResult()
-        self._check(self.lib.perm_exact_dense(self.ctx, _ptr(a), a.shape[0], dt, ctypes.byref(r)))
+        if variant:
+            self._check(self.lib.perm_exact_dense_ex(self.ctx, _ptr(a), a.shape[0], dt, variant, 0, 1,
+                                                     ctypes.byref(r)))
+        else:
+            self._check(self.lib.perm_exact_dense(self.ctx, _ptr(a), a.shape[0], dt, ctypes.byref(r)))
         return _exact(r)
 
-    def exact_dense_shard(self, mat, shard: int, nshards: int) -> ExactResult:
+    def exact_dense_shard(self, mat, shard: int, nshards: int, variant: int = 0) -> ExactResult:
         a, dt = _as_matrix(mat)
         r = PermResult()
-        self._check(self.lib.perm_exact_dense_shard(self.ctx, _ptr(a), a.shape[0], dt, shard, nshards,
-                                                    ctypes.byref(r)))
+        self._check(self.lib.perm_exact_dense_ex(self.ctx, _ptr(a), a.shape[0], dt, variant, shard, nshards,
+                                                 ctypes.byref(r)))
         return _exact(r)
 
-    def exact_sparse(self, n: int, rptrs, cols, rvals, cptrs, rows, cvals) -> ExactResult:
+    def exact_sparse(self, n: int, rptrs, cols, rvals, cptrs, rows, cvals, variant: int = 0) -> ExactResult:
+        """Sparse exact permanent; variant 0 = automatic, PERM_KERNEL_SKIPPER forces SkipPer."""
         ar = [np.ascontiguousarray(x, dtype=np.int32) for x in (rptrs, cols, cptrs, rows)]
         rv = np.ascontiguousarray(rvals, dtype=np.float64)
         cv = np.ascontiguousarray(cvals, dtype=np.float64)
         r = PermResult()
-        self._check(self.lib.perm_exact_sparse(self.ctx, n, _ptr(ar[0]), _ptr(ar[1]), _ptr(rv), _ptr(ar[2]),
-                                               _ptr(ar[3]), _ptr(cv), ctypes.byref(r)))
+        self._check(self.lib.perm_exact_sparse_ex(self.ctx, n, _ptr(ar[0]), _ptr(ar[1]), _ptr(rv), _ptr(ar[2]),
+                                                  _ptr(ar[3]), _ptr(cv), variant, ctypes.byref(r)))
         return _exact(r)
 
-    def exact_sparse_matrix(self, mat, order: int = 2) -> ExactResult:
-        """SkipPer of a dense matrix after the reference's -r <order> preprocessing."""
+    def exact_sparse_matrix(self, mat, order: int = 2, variant: int = 0) -> ExactResult:
+        """Sparse exact permanent of a dense matrix after the reference's -r <order> preprocessing."""
         c = compress(order, mat)
-        return self.exact_sparse(c["n"], c["rptrs"], c["cols"], c["rvals"], c["cptrs"], c["rows"], c["cvals"])
+        return self.exact_sparse(c["n"], c["rptrs"], c["cols"], c["rvals"], c["cptrs"], c["rows"], c["cvals"],
+                                 variant)
 
-    def upload_dense(self, mat) -> "ResidentMatrix":
+    def upload_dense(self, mat, variant: int = 0) -> "ResidentMatrix":
         a, dt = _as_matrix(mat)
         h = _P()
-        self._check(self.lib.perm_matrix_create_dense(self.ctx, _ptr(a), a.shape[0], dt, ctypes.byref(h)))
+        self._check(self.lib.perm_matrix_create_dense_ex(self.ctx, _ptr(a), a.shape[0], dt, variant,
+                                                         ctypes.byref(h)))
         return ResidentMatrix(self, h, a.shape[0])
 
     # ---- Monte Carlo ----

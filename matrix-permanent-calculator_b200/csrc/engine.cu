@@ -31,6 +31,7 @@
 #include "mc.h"
 #include "perman_common.cuh"
 #include "ryser_dense.cuh"
+#include "ryser_dense_int.cuh"
 #include "skipper.h"
 
 namespace perm {
@@ -39,6 +40,21 @@ const void* dense_kernel_1(int n);
 const void* dense_kernel_2(int n);
 const void* dense_kernel_3(int n);
 const void* dense_kernel_4(int n);
+
+const void* dense_int_kernel_g3(int n);
+const void* dense_int_kernel_g4(int n);
+const void* dense_int_kernel_g5(int n);
+const void* dense_int_kernel_g6(int n);
+
+static const void* dense_int_kernel(int n, int g) {
+  switch (g) {
+    case 3: return dense_int_kernel_g3(n);
+    case 4: return dense_int_kernel_g4(n);
+    case 5: return dense_int_kernel_g5(n);
+    case 6: return dense_int_kernel_g6(n);
+    default: return nullptr;
+  }
+}
 
 static const void* dense_kernel(int n) {
   if (n >= 1 && n <= 20) return dense_kernel_0(n);
@@ -72,10 +88,8 @@ __global__ void fp64_peak_kernel(double* out, int iters, double a, double b) {
 
 using namespace perm;
 
-struct perm_matrix {
-  int n = 0;
-  double* d_col = nullptr;  // column-major, stride np
-};
+struct DenseOperand;
+struct perm_matrix;
 
 struct perm_ctx {
   int device = 0;
@@ -96,7 +110,7 @@ struct perm_ctx {
   size_t h_stage_cap = 0;
   double* d_trials = nullptr;
   size_t d_trials_cap = 0;
-  int dense_occ[PERM_MAX_EXACT_N + 1] = {0};
+  int dense_occ[8][PERM_MAX_EXACT_N + 1] = {};  // [0]: FP64-X, [G]: int32-X groups of G
   std::string err;
   std::mutex mu;
 };
@@ -273,21 +287,101 @@ static int finish_and_read(perm_ctx* ctx, int nout) {
 // ---------------------------------------------------------------------------
 // dense exact
 // ---------------------------------------------------------------------------
+// A dense operand in its device image: FP64 columns (np = n rounded up to
+// even) for the FP64-X kernel, or doubled int32 columns plus y0 (np4 = n
+// rounded up to a multiple of 4) for the int32-X kernel.
+struct DenseOperand {
+  int n = 0, variant = PERM_KERNEL_DENSE, group = 0;
+  std::vector<unsigned char> image;
+};
+
+// Integer-valued with |a| < 2^24 and a product grouping that provably fits in
+// int32: returns the largest group size G in {6,5,4,3} such that every run of
+// G consecutive rows has prod(sum_k |a_jk|) < 2^31, or 0.
+static int int_group_size(const std::vector<double>& a, int n) {
+  if (n < 8) return 0;
+  std::vector<double> rowabs(n, 0.0);
+  for (int j = 0; j < n; j++)
+    for (int k = 0; k < n; k++) {
+      const double v = a[(size_t)j * n + k];
+      if (v != std::floor(v) || std::fabs(v) >= 16777216.0) return 0;
+      rowabs[j] += std::fabs(v);
+    }
+  for (int G = 6; G >= 3; G--) {
+    bool ok = true;
+    for (int j0 = 0; j0 < n && ok; j0 += G) {
+      double b = 1.0;
+      for (int t = 0; t < G && j0 + t < n; t++) b *= std::max(rowabs[j0 + t], 1.0);
+      ok = b < 2147483648.0;
+    }
+    if (ok) return G;
+  }
+  return 0;
+}
+
+static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, DenseOperand* op) {
+  std::vector<double> a((size_t)n * n);
+  for (size_t i = 0; i < a.size(); i++) a[i] = elem(mat, dtype, i);
+  op->n = n;
+  int G = (variant == PERM_KERNEL_DENSE) ? 0 : int_group_size(a, n);
+  if (variant == PERM_KERNEL_DENSE_INT && G == 0)
+    return fail(ctx, PERM_EUNSUPPORTED,
+                "int32-X kernel needs an integer matrix of order >= 8 whose row products fit in int32");
+  if (G) {
+    const int np4 = (n + 3) & ~3;
+    op->variant = PERM_KERNEL_DENSE_INT;
+    op->group = G;
+    op->image.assign(sizeof(int) * (size_t)(n + 1) * np4, 0);
+    int* img = reinterpret_cast<int*>(op->image.data());
+    for (int k = 0; k < n; k++)
+      for (int j = 0; j < n; j++) img[(size_t)k * np4 + j] = 2 * (int)a[(size_t)j * n + k];
+    int* y0 = img + (size_t)n * np4;
+    for (int j = 0; j < n; j++) {
+      long long rs = 0;
+      for (int k = 0; k < n; k++) rs += (long long)a[(size_t)j * n + k];
+      y0[j] = (int)(2 * (long long)a[(size_t)j * n + n - 1] - rs);
+    }
+  } else {
+    const int np = (n + 1) & ~1;
+    op->variant = PERM_KERNEL_DENSE;
+    op->group = 0;
+    op->image.assign(sizeof(double) * (size_t)n * np, 0);
+    double* img = reinterpret_cast<double*>(op->image.data());
+    for (int k = 0; k < n; k++)
+      for (int j = 0; j < n; j++) img[(size_t)k * np + j] = a[(size_t)j * n + k];
+  }
+  return PERM_OK;
+}
+
+struct perm_matrix {
+  DenseOperand op;
+  void* d_image = nullptr;
+};
+
+static const void* operand_kernel(const DenseOperand& op) {
+  if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_kernel(op.n, op.group);
+  return dense_kernel(op.n);
+}
+static size_t operand_smem(const DenseOperand& op) {
+  return op.variant == PERM_KERNEL_DENSE_INT ? dense_int_smem_bytes(op.n) : dense_smem_bytes(op.n);
+}
+
 struct DensePlan {
   int grid = 1, m = 3;
   uint64_t block0 = 0, nblocks = 0;
 };
 
-static int dense_plan(perm_ctx* ctx, int n, int shard, int nshards, DensePlan* p) {
-  const void* fn = dense_kernel(n);
+static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nshards, DensePlan* p) {
+  const int n = op.n;
+  const void* fn = operand_kernel(op);
   if (!fn) return fail(ctx, PERM_EUNSUPPORTED, "dense exact order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
-  size_t smem = dense_smem_bytes(n);
-  if (!ctx->dense_occ[n]) {
+  int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? op.group : 0][n];
+  if (!occ_slot) {
     int occ = 0;
-    CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, smem));
-    ctx->dense_occ[n] = std::max(occ, 1);
+    CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, operand_smem(op)));
+    occ_slot = std::max(occ, 1);
   }
-  const uint64_t total = n >= 1 ? (1ull << (n - 1)) : 1;
+  const uint64_t total = 1ull << (n - 1);
   if (n < 4) {
     p->grid = 1;
     p->m = 0;
@@ -295,7 +389,7 @@ static int dense_plan(perm_ctx* ctx, int n, int shard, int nshards, DensePlan* p
     p->nblocks = 0;
     return PERM_OK;
   }
-  int grid = std::min(kMaxBlocks, ctx->num_sms * ctx->dense_occ[n]);
+  int grid = std::min(kMaxBlocks, ctx->num_sms * occ_slot);
   // Alignment m: each thread should own >= 64 aligned blocks when possible.
   const uint64_t threads = (uint64_t)grid * 128 * (uint64_t)nshards;
   int m = 3;
@@ -312,30 +406,48 @@ static int dense_plan(perm_ctx* ctx, int n, int shard, int nshards, DensePlan* p
   return PERM_OK;
 }
 
-static int dense_launch(perm_ctx* ctx, const double* d_col, int n, const DensePlan& p) {
-  DenseArgs args;
-  args.colA = d_col;
-  args.np = (n + 1) & ~1;
-  args.m = p.m;
-  args.block0 = p.block0;
-  args.nblocks = p.nblocks;
-  args.partials = ctx->partials;
-  args.ticket = ctx->ticket;
-  args.out = ctx->d_out;
-  args.err = ctx->d_err;
-  void* kargs[] = {&args};
+static int dense_launch(perm_ctx* ctx, const DenseOperand& op, const void* d_image, const DensePlan& p) {
+  const int n = op.n;
   CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-  CU(ctx, cudaLaunchKernel(dense_kernel(n), dim3(p.grid), dim3(128), kargs, dense_smem_bytes(n),
-                           ctx->stream));
+  if (op.variant == PERM_KERNEL_DENSE_INT) {
+    DenseIntArgs args;
+    const int np4 = (n + 3) & ~3;
+    args.colI = static_cast<const int*>(d_image);
+    args.y0 = args.colI + (size_t)n * np4;
+    args.np4 = np4;
+    args.m = p.m;
+    args.block0 = p.block0;
+    args.nblocks = p.nblocks;
+    args.partials = ctx->partials;
+    args.ticket = ctx->ticket;
+    args.out = ctx->d_out;
+    args.err = ctx->d_err;
+    void* kargs[] = {&args};
+    CU(ctx, cudaLaunchKernel(operand_kernel(op), dim3(p.grid), dim3(128), kargs, operand_smem(op), ctx->stream));
+  } else {
+    DenseArgs args;
+    args.colA = static_cast<const double*>(d_image);
+    args.np = (n + 1) & ~1;
+    args.m = p.m;
+    args.block0 = p.block0;
+    args.nblocks = p.nblocks;
+    args.partials = ctx->partials;
+    args.ticket = ctx->ticket;
+    args.out = ctx->d_out;
+    args.err = ctx->d_err;
+    void* kargs[] = {&args};
+    CU(ctx, cudaLaunchKernel(operand_kernel(op), dim3(p.grid), dim3(128), kargs, operand_smem(op), ctx->stream));
+  }
   CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
   return PERM_OK;
 }
 
-static int dense_collect(perm_ctx* ctx, int n, const DensePlan& p, perm_result* out) {
+static int dense_collect(perm_ctx* ctx, const DenseOperand& op, const DensePlan& p, perm_result* out) {
   int rc = finish_and_read(ctx, 2);
   if (rc != PERM_OK) return rc;
   float ms = 0;
   CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  const int n = op.n;
   const double hi = ctx->h_out[0], lo = ctx->h_out[1];
   out->hi = hi;
   out->lo = lo;
@@ -343,7 +455,7 @@ static int dense_collect(perm_ctx* ctx, int n, const DensePlan& p, perm_result* 
   out->total_steps = std::ldexp(1.0, n - 1);
   out->steps = n < 4 ? (p.block0 == 0 ? out->total_steps : 0.0) : std::ldexp((double)p.nblocks, p.m);
   out->kernel_ms = ms;
-  out->kernel = PERM_KERNEL_DENSE;
+  out->kernel = op.variant;
   out->n = n;
   return PERM_OK;
 }
@@ -357,48 +469,61 @@ static int check_dense_args(perm_ctx* ctx, const void* mat, int n, int dtype, co
   return PERM_OK;
 }
 
-extern "C" int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int shard,
-                                      int nshards, perm_result* out) {
+static int check_variant(perm_ctx* ctx, int variant) {
+  if (variant != 0 && variant != PERM_KERNEL_DENSE && variant != PERM_KERNEL_DENSE_INT)
+    return fail(ctx, PERM_EINVAL, "unknown dense kernel variant %d", variant);
+  return PERM_OK;
+}
+
+extern "C" int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard,
+                                   int nshards, perm_result* out) {
   int rc = check_dense_args(ctx, mat, n, dtype, out);
   if (rc) return rc;
+  if ((rc = check_variant(ctx, variant))) return rc;
   if (nshards < 1 || shard < 0 || shard >= nshards)
     return fail(ctx, PERM_EINVAL, "shard %d of %d", shard, nshards);
+  DenseOperand op;
+  if ((rc = build_operand(ctx, mat, n, dtype, variant, &op))) return rc;
   std::lock_guard<std::mutex> lock(ctx->mu);
   CU(ctx, cudaSetDevice(ctx->device));
-  const int np = (n + 1) & ~1;
-  const size_t bytes = sizeof(double) * (size_t)n * np;
-  if ((rc = ensure_stage(ctx, bytes))) return rc;
-  pack_columns(mat, n, dtype, reinterpret_cast<double*>(ctx->h_stage));
+  if ((rc = ensure_stage(ctx, op.image.size()))) return rc;
+  memcpy(ctx->h_stage, op.image.data(), op.image.size());
   DensePlan p;
-  if ((rc = dense_plan(ctx, n, shard, nshards, &p))) return rc;
-  CU(ctx, cudaMemcpyAsync(ctx->d_stage, ctx->h_stage, bytes, cudaMemcpyHostToDevice, ctx->stream));
-  if ((rc = dense_launch(ctx, reinterpret_cast<double*>(ctx->d_stage), n, p))) return rc;
-  return dense_collect(ctx, n, p, out);
+  if ((rc = dense_plan(ctx, op, shard, nshards, &p))) return rc;
+  CU(ctx, cudaMemcpyAsync(ctx->d_stage, ctx->h_stage, op.image.size(), cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = dense_launch(ctx, op, ctx->d_stage, p))) return rc;
+  return dense_collect(ctx, op, p, out);
+}
+
+extern "C" int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int shard,
+                                      int nshards, perm_result* out) {
+  return perm_exact_dense_ex(ctx, mat, n, dtype, 0, shard, nshards, out);
 }
 
 extern "C" int perm_exact_dense(perm_ctx* ctx, const void* mat, int n, int dtype, perm_result* out) {
-  return perm_exact_dense_shard(ctx, mat, n, dtype, 0, 1, out);
+  return perm_exact_dense_ex(ctx, mat, n, dtype, 0, 0, 1, out);
 }
 
-extern "C" int perm_matrix_create_dense(perm_ctx* ctx, const void* mat, int n, int dtype, perm_matrix** out) {
+extern "C" int perm_matrix_create_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant,
+                                           perm_matrix** out) {
   int rc = check_dense_args(ctx, mat, n, dtype, out);
   if (rc) return rc;
+  if ((rc = check_variant(ctx, variant))) return rc;
+  perm_matrix* m = new perm_matrix();
+  if ((rc = build_operand(ctx, mat, n, dtype, variant, &m->op))) {
+    delete m;
+    return rc;
+  }
   std::lock_guard<std::mutex> lock(ctx->mu);
   CU(ctx, cudaSetDevice(ctx->device));
-  const int np = (n + 1) & ~1;
-  const size_t bytes = sizeof(double) * (size_t)n * np;
-  std::vector<double> col((size_t)n * np);
-  pack_columns(mat, n, dtype, col.data());
-  perm_matrix* m = new perm_matrix();
-  m->n = n;
-  cudaError_t e = cudaMalloc(&m->d_col, bytes);
+  cudaError_t e = cudaMalloc(&m->d_image, m->op.image.size());
   if (e != cudaSuccess) {
     delete m;
     return fail_cuda(ctx, e, "cudaMalloc(resident matrix)");
   }
-  e = cudaMemcpy(m->d_col, col.data(), bytes, cudaMemcpyHostToDevice);
+  e = cudaMemcpy(m->d_image, m->op.image.data(), m->op.image.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
-    cudaFree(m->d_col);
+    cudaFree(m->d_image);
     delete m;
     return fail_cuda(ctx, e, "cudaMemcpy(resident matrix)");
   }
@@ -406,10 +531,14 @@ extern "C" int perm_matrix_create_dense(perm_ctx* ctx, const void* mat, int n, i
   return PERM_OK;
 }
 
+extern "C" int perm_matrix_create_dense(perm_ctx* ctx, const void* mat, int n, int dtype, perm_matrix** out) {
+  return perm_matrix_create_dense_ex(ctx, mat, n, dtype, 0, out);
+}
+
 extern "C" void perm_matrix_destroy(perm_ctx* ctx, perm_matrix* m) {
   if (!m) return;
   if (ctx) cudaSetDevice(ctx->device);
-  cudaFree(m->d_col);
+  cudaFree(m->d_image);
   delete m;
 }
 
@@ -418,10 +547,10 @@ extern "C" int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, pe
   std::lock_guard<std::mutex> lock(ctx->mu);
   CU(ctx, cudaSetDevice(ctx->device));
   DensePlan p;
-  int rc = dense_plan(ctx, m->n, 0, 1, &p);
+  int rc = dense_plan(ctx, m->op, 0, 1, &p);
   if (rc) return rc;
-  if ((rc = dense_launch(ctx, m->d_col, m->n, p))) return rc;
-  return dense_collect(ctx, m->n, p, out);
+  if ((rc = dense_launch(ctx, m->op, m->d_image, p))) return rc;
+  return dense_collect(ctx, m->op, p, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -429,22 +558,9 @@ extern "C" int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, pe
 // ---------------------------------------------------------------------------
 static inline uint32_t align16(uint32_t v) { return (v + 15u) & ~15u; }
 
-extern "C" int perm_exact_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
-                                 const double* rvals, const int* cptrs, const int* rows,
-                                 const double* cvals, perm_result* out) {
-  if (!ctx) return PERM_EINVAL;
-  if (!rptrs || !cols || !rvals || !cptrs || !rows || !cvals || !out)
-    return fail(ctx, PERM_EINVAL, "null CRS/CCS or result pointer");
-  if (n < 1 || n > PERM_MAX_EXACT_N) return fail(ctx, PERM_EUNSUPPORTED, "order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
+static int run_skipper(perm_ctx* ctx, int n, const int* rptrs, const int* cols, const double* rvals,
+                       const int* cptrs, const int* rows, const double* cvals, perm_result* out) {
   const int nnz = rptrs[n];
-  if (nnz < 0 || nnz > n * n || cptrs[n] != nnz || rptrs[0] != 0 || cptrs[0] != 0)
-    return fail(ctx, PERM_EINVAL, "inconsistent CRS/CCS (rptrs[n]=%d, cptrs[n]=%d)", nnz, cptrs[n]);
-  for (int i = 0; i < n; i++)
-    if (rptrs[i + 1] < rptrs[i] || cptrs[i + 1] < cptrs[i])
-      return fail(ctx, PERM_EINVAL, "pointer arrays must be non-decreasing");
-  for (int p = 0; p < nnz; p++)
-    if (cols[p] < 0 || cols[p] >= n || rows[p] < 0 || rows[p] >= n)
-      return fail(ctx, PERM_EINVAL, "index out of range at entry %d", p);
   std::lock_guard<std::mutex> lock(ctx->mu);
   CU(ctx, cudaSetDevice(ctx->device));
   // x0 exactly as the reference SkipPer builds it (algo.h:751-760)
@@ -525,6 +641,76 @@ extern "C" int perm_exact_sparse(perm_ctx* ctx, int n, const int* rptrs, const i
   out->kernel = PERM_KERNEL_SKIPPER;
   out->n = n;
   return PERM_OK;
+}
+
+// Fraction of Gray indices whose x vector has a zero entry, estimated from a
+// fixed pseudo-random sample (deterministic).  SkipPer only pays off when
+// most terms vanish: a visited index costs it several times a dense-kernel
+// step, so below kSkipperZeroFraction the register kernel runs instead (same
+// matrix, same permanent).
+static const double kSkipperZeroFraction = 0.75;
+
+static double zero_term_fraction(int n, const int* rptrs, const double* rvals, const int* cptrs,
+                                 const int* rows, const double* cvals, int samples) {
+  std::vector<double> x0(n), x(n);
+  for (int j = 0; j < n; j++) {
+    double rs = 0;
+    for (int p = rptrs[j]; p < rptrs[j + 1]; p++) rs += rvals[p];
+    x0[j] = -rs / 2.0;
+  }
+  for (int p = cptrs[n - 1]; p < cptrs[n]; p++) x0[rows[p]] += cvals[p];
+  const uint64_t total = 1ull << (n - 1);
+  uint64_t state = 0x9E3779B97F4A7C15ull;
+  int zeros = 0;
+  for (int s = 0; s < samples; s++) {
+    state = state * 6364136223846793005ull + 1442695040888963407ull;
+    const uint64_t i = (state >> 1) % total;
+    const uint64_t g = i ^ (i >> 1);
+    x = x0;
+    for (int k = 0; k < n - 1; k++)
+      if ((g >> k) & 1)
+        for (int p = cptrs[k]; p < cptrs[k + 1]; p++) x[rows[p]] += cvals[p];
+    for (int j = 0; j < n; j++)
+      if (x[j] == 0.0) {
+        zeros++;
+        break;
+      }
+  }
+  return (double)zeros / samples;
+}
+
+extern "C" int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, const int* cols, const double* rvals,
+                                    const int* cptrs, const int* rows, const double* cvals, int variant,
+                                    perm_result* out) {
+  if (!ctx) return PERM_EINVAL;
+  if (!rptrs || !cols || !rvals || !cptrs || !rows || !cvals || !out)
+    return fail(ctx, PERM_EINVAL, "null CRS/CCS or result pointer");
+  if (n < 1 || n > PERM_MAX_EXACT_N) return fail(ctx, PERM_EUNSUPPORTED, "order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
+  const int nnz = rptrs[n];
+  if (nnz < 0 || nnz > n * n || cptrs[n] != nnz || rptrs[0] != 0 || cptrs[0] != 0)
+    return fail(ctx, PERM_EINVAL, "inconsistent CRS/CCS (rptrs[n]=%d, cptrs[n]=%d)", nnz, cptrs[n]);
+  for (int i = 0; i < n; i++)
+    if (rptrs[i + 1] < rptrs[i] || cptrs[i + 1] < cptrs[i])
+      return fail(ctx, PERM_EINVAL, "pointer arrays must be non-decreasing");
+  for (int p = 0; p < nnz; p++)
+    if (cols[p] < 0 || cols[p] >= n || rows[p] < 0 || rows[p] >= n)
+      return fail(ctx, PERM_EINVAL, "index out of range at entry %d", p);
+  if (variant != 0 && variant != PERM_KERNEL_SKIPPER && variant != PERM_KERNEL_DENSE &&
+      variant != PERM_KERNEL_DENSE_INT)
+    return fail(ctx, PERM_EINVAL, "unknown sparse kernel variant %d", variant);
+  bool skipper = variant == PERM_KERNEL_SKIPPER;
+  if (variant == 0) skipper = n < 8 || zero_term_fraction(n, rptrs, rvals, cptrs, rows, cvals, 2048) >= kSkipperZeroFraction;
+  if (skipper) return run_skipper(ctx, n, rptrs, cols, rvals, cptrs, rows, cvals, out);
+  // the matrix the CRS describes, for the register kernels
+  std::vector<double> a((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++)
+    for (int p = rptrs[i]; p < rptrs[i + 1]; p++) a[(size_t)i * n + cols[p]] = rvals[p];
+  return perm_exact_dense_ex(ctx, a.data(), n, PERM_F64, variant == PERM_KERNEL_SKIPPER ? 0 : variant, 0, 1, out);
+}
+
+extern "C" int perm_exact_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols, const double* rvals,
+                                 const int* cptrs, const int* rows, const double* cvals, perm_result* out) {
+  return perm_exact_sparse_ex(ctx, n, rptrs, cols, rvals, cptrs, rows, cvals, 0, out);
 }
 
 // ---------------------------------------------------------------------------

@@ -61,6 +61,8 @@ def ref():
 
 @pytest.fixture(scope="session")
 def golden():
+    if not GOLDEN.exists():
+        pytest.skip("tests/golden/golden.json not generated yet")
     with open(GOLDEN) as f:
         data = json.load(f)
     for c in data["cases"]:

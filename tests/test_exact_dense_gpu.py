@@ -49,9 +49,14 @@ def test_dtypes_agree(engine):
     assert engine.exact_dense(A.astype(np.float32)).value == v64
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 12, 18])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 12, 18, 22])
 def test_all_ones_factorial(engine, n):
-    assert engine.exact_dense(np.ones((n, n))).value == math.factorial(n)
+    # small orders are exact; beyond ~2^53 in the intermediate terms, 1e-13
+    for variant in (1, 3):
+        if variant == 3 and n < 8:
+            continue
+        v = engine.exact_dense(np.ones((n, n)), variant=variant).value
+        assert rel_err(v, math.factorial(n)) < (0 if n <= 12 else 1e-13)
 
 
 def test_identity_permutation_zero_row(engine):
@@ -95,6 +100,7 @@ def test_full_size_invariances(engine, n):
     rng = np.random.default_rng(n)
     A = bernoulli(rng, n, 0.5) * rng.integers(1, 5, (n, n))
     base = engine.exact_dense(A).value
+    assert rel_err(engine.exact_dense(A, variant=1).value, base) < TOL  # FP64-X and int32-X agree
     Pm = A[rng.permutation(n)][:, rng.permutation(n)]
     assert rel_err(engine.exact_dense(Pm).value, base) < TOL
     assert rel_err(engine.exact_dense(A.T.copy()).value, base) < TOL
@@ -132,3 +138,53 @@ def test_reference_gpu_kernel_same_inputs(engine, ref):
     Ac = np.ascontiguousarray(A)
     theirs = ref.lib.ref_gpu_dense_mshared_f64(Ac.ctypes.data_as(ctypes.c_void_p), 20, 2048, 128)
     assert rel_err(engine.exact_dense(A).value, theirs) < 1e-12
+
+
+# ---- int32-X kernel ---------------------------------------------------------------
+
+@pytest.mark.parametrize("n", [8, 9, 13, 17, 21, 24, 27])
+def test_int_kernel_exact_vs_oracle(engine, orc, pb, n):
+    rng = np.random.default_rng(500 + n)
+    for hi in (2, 5, 30):  # binary, small and larger integers -> different group sizes
+        A = bernoulli(rng, n, 0.5) * rng.integers(1, hi, (n, n))
+        exact = orc.perm_exact_int(A)[0]
+        r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
+        assert r.kernel == pb.PERM_KERNEL_DENSE_INT
+        assert rel_err(r.value, exact) < 1e-13, (hi, r.value, exact)
+        f = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE)
+        assert rel_err(f.value, r.value) < 1e-13
+
+
+def test_int_kernel_signed_entries(engine, orc, pb):
+    rng = np.random.default_rng(17)
+    A = rng.integers(-4, 5, (18, 18)).astype(float)
+    exact = orc.perm_exact_int(A)[0]
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
+    assert abs(r.value - exact) <= 1e-10 * max(abs(exact), 1.0) * 1e3
+
+
+def test_automatic_kernel_choice(engine, pb):
+    rng = np.random.default_rng(18)
+    A = bernoulli(rng, 20, 0.5)
+    assert engine.exact_dense(A).kernel == pb.PERM_KERNEL_DENSE_INT
+    assert engine.exact_dense(A * 0.5).kernel == pb.PERM_KERNEL_DENSE
+    big = A * 100000  # row products no longer fit int32 in groups of 3
+    assert engine.exact_dense(big).kernel == pb.PERM_KERNEL_DENSE
+    with pytest.raises(pb.PermError):
+        engine.exact_dense(A * 0.5, variant=pb.PERM_KERNEL_DENSE_INT)
+
+
+def test_int_kernel_golden(engine, golden, pb):
+    for name, c in golden.items():
+        if c["kind"] == "real" or c["n"] < 8 or "exact" not in c:
+            continue
+        r = engine.exact_dense(c["A"], variant=pb.PERM_KERNEL_DENSE_INT)
+        assert rel_err(r.value, int(c["exact"])) < TOL, name
+
+
+def test_int_kernel_shards(engine, pb):
+    rng = np.random.default_rng(19)
+    A = bernoulli(rng, 26, 0.5) * rng.integers(1, 5, (26, 26))
+    whole = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT).value
+    parts = [engine.exact_dense_shard(A, s, 5, variant=pb.PERM_KERNEL_DENSE_INT) for s in range(5)]
+    assert rel_err(sum(p.hi + p.lo for p in parts), whole) < 1e-14

@@ -112,7 +112,10 @@ def test_golden_reference_values_match_oracle(golden):
             continue
         if c.get("ref_perman64") is not None:
             assert rel_err(c["ref_perman64"], want) < 1e-9, name
-        if c.get("ref_skip_balanced_skiporder") is not None:
+        # the reference's CRS/CCS keep positive entries only (util.h:537), so its
+        # SkipPer computes the permanent of the positive part: compare on
+        # non-negative matrices
+        if c.get("ref_skip_balanced_skiporder") is not None and (c["A"] >= 0).all():
             assert rel_err(c["ref_skip_balanced_skiporder"], want) < 1e-9, name
         if c["kind"] in ("binary", "int") and c["n"] <= 24:
             assert rel_err(c["ref_parallel_perman64"], want) < 1e-9, name

@@ -111,7 +111,8 @@ def test_golden_reference_values_match_oracle(golden):
         if want == 0:
             continue
         if c.get("ref_perman64") is not None:
-            assert rel_err(c["ref_perman64"], want) < 1e-9, name
+            # serial double-X walk with an uncompensated sum: ~1e-9 on n=30 reals
+            assert rel_err(c["ref_perman64"], want) < (1e-8 if c["kind"] == "real" else 1e-9), name
         # the reference's CRS/CCS keep positive entries only (util.h:537), so its
         # SkipPer computes the permanent of the positive part: compare on
         # non-negative matrices

@@ -184,6 +184,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--order", type=int, default=N_ORDER, help="matrix order (profiling runs use a smaller one)")
+    ap.add_argument("--variant", choices=["auto", "fp64", "int"], default="auto",
+                    help="dense kernel: automatic, FP64-X or int32-X")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -203,15 +206,16 @@ def main():
     torch.cuda.set_device(device)
     pb = load_pkg()
     eng = pb.Engine(device)
-    A = make_matrix(rank)
+    A = make_matrix(rank, args.order)
     n = A.shape[0]
+    variant = {"auto": 0, "fp64": pb.PERM_KERNEL_DENSE, "int": pb.PERM_KERNEL_DENSE_INT}[args.variant]
     total_steps = 2.0 ** (n - 1)
     ops_per_step = 2.0 * n  # n X-updates + n multiplies per Gray step (algorithmic)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")  # 256 MB > L2
 
     peak_ops, _ = eng.fp64_peak()
     peak_ops = max(peak_ops, eng.fp64_peak()[0])
-    res = eng.upload_dense(A)
+    res = eng.upload_dense(A, variant=variant)
 
     def barrier():
         if dist is not None:
@@ -243,11 +247,11 @@ def main():
     # end to end through the C ABI with a host matrix
     e2e_ms = []
     for _ in range(2):
-        eng.exact_dense(A)
+        eng.exact_dense(A, variant=variant)
     barrier()
     for _ in range(args.steps):
         t = time.perf_counter()
-        r2 = eng.exact_dense(A)
+        r2 = eng.exact_dense(A, variant=variant)
         e2e_ms.append((time.perf_counter() - t) * 1e3)
     e2e_s = sum(e2e_ms) * 1e-3
     if dist is not None:
@@ -270,7 +274,8 @@ def main():
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, resident in HBM)",
-        "config": {"workload": WORKLOAD, "n": n, "density": DENSITY, "values": "U{1,2,3,4}",
+        "config": {"workload": WORKLOAD.replace("n=40", f"n={n}"), "n": n, "density": DENSITY,
+                   "values": "U{1,2,3,4}",
                    "gray_steps_per_permanent": total_steps, "parallelism": f"{world} rank(s), one matrix each",
                    "l2": "256 MB buffer written between steps (operand is 12.8 KB; compute-bound)",
                    "timing": "CUDA events around each kernel on the engine stream; max over ranks"},

@@ -307,6 +307,9 @@ def main():
             "fp64_frac_of_measured_peak": total_steps * ops_per_step / (fr.kernel_ms * 1e-3) / peak_ops,
             "rel_diff_vs_headline": abs(fr.value - perm_value) / abs(perm_value)}
         line["secondary"]["reference_gpu_p4_same_box"] = reference_gpu(A)
+        line["secondary"]["batched_8192_n12_28"] = batched_secondary(pb, eng)
+        line["secondary"]["serving_poisson_2000_per_s"] = serving_secondary(pb)
+        line["secondary"]["serving_poisson_40_per_s"] = serving_secondary(pb, requests=120, rate=40.0)
     if rank == 0 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1
@@ -368,6 +371,103 @@ def reference_gpu(A40):
         return out
     except Exception as e:  # reported, never fatal
         return {"unavailable": str(e)}
+
+
+def batched_secondary(pb, eng, count=8192):
+    """8192 matrices, n ~ U[12,28], density ~ U[0.2,0.9], half binary and half
+    U(0,1], half marked sparse (the batch kernel takes them dense): one
+    persistent launch per captured graph, lane ranges from the autotuner; the
+    comparison point is one launch per matrix of the plain kernel."""
+    rng = np.random.default_rng(4444)
+    mats = []
+    for i in range(count):
+        n = int(rng.integers(12, 29))
+        d = rng.uniform(0.2, 0.9)
+        while True:
+            m = (rng.random((n, n)) < d).astype(np.float64)
+            if m.any(0).all() and m.any(1).all():
+                break
+        if i % 2:
+            m *= 1.0 - rng.random((n, n))
+        mats.append(m)
+    t = time.perf_counter()
+    table = eng.batch_autotune(12, 28)
+    tune_s = time.perf_counter() - t
+    b = eng.batch(mats)
+    b.run()
+    times = []
+    for _ in range(3):
+        vals, ms = b.run()
+        times.append(ms)
+    b.free()
+    batch_ms = min(times)
+    # one launch per matrix (plain kernel, FP64 X, host loop through the C ABI)
+    for m in mats[:64]:
+        eng.exact_dense(m, variant=pb.PERM_KERNEL_DENSE)
+    t = time.perf_counter()
+    ref_vals = [eng.exact_dense(m, variant=pb.PERM_KERNEL_DENSE).value for m in mats]
+    per_ms = (time.perf_counter() - t) * 1e3
+    # binary matrices without a perfect matching have permanent 0: both kernels
+    # return rounding noise there, so relative differences use |perm| >= 1e-3
+    err = max(abs(a - b) / abs(b) for a, b in zip(vals, ref_vals) if abs(b) >= 1e-3)
+    noise = max((abs(a - b) for a, b in zip(vals, ref_vals) if abs(b) < 1e-3), default=0.0)
+    steps = sum(2.0 ** (m.shape[0] - 1) for m in mats)
+    return {"matrices": count, "batch_ms": batch_ms, "batch_perms_per_s": count / (batch_ms * 1e-3),
+            "batch_steps_per_s": steps / (batch_ms * 1e-3),
+            "one_launch_per_matrix_ms": per_ms, "one_launch_per_matrix_perms_per_s": count / (per_ms * 1e-3),
+            "speedup_vs_one_launch_per_matrix": per_ms / batch_ms, "max_rel_diff_vs_single": err, "max_abs_diff_where_perm_below_1e-3": noise,
+            "autotune_s": tune_s, "autotuned_lane_log2": table,
+            "timing": "CUDA events around the graph launch (queue reset + kernel + 128 KB readback)"}
+
+
+def serving_secondary(pb, requests=400, rate=2000.0, slots=4, seed=5555):
+    """Poisson arrivals mixing exact (n ~ U[16,34], U(0,1], d=0.5) and
+    approximate (binary n ~ U[40,64], d=0.5, Rasmussen or scaling y=4 z=5,
+    2e5 trials) requests through the request loop."""
+    import threading
+
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(requests):
+        if rng.random() < 0.5:
+            n = int(rng.integers(16, 35))
+            A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+            reqs.append((pb.PERM_REQ_EXACT_DENSE, A, {}))
+        else:
+            n = int(rng.integers(40, 65))
+            A = (rng.random((n, n)) < 0.5).astype(np.float64)
+            kind = pb.PERM_REQ_RASMUSSEN if rng.random() < 0.5 else pb.PERM_REQ_SCALING
+            reqs.append((kind, A, {"trials": 200000, "scale_intervals": 4, "scale_times": 5, "seed": i}))
+    gaps = rng.exponential(1.0 / rate, requests)
+    with pb.Server(0, slots=slots) as srv:
+        tickets = [None] * requests
+
+        def feeder():
+            t0 = time.perf_counter()
+            due = 0.0
+            for i, (k, A, kw) in enumerate(reqs):
+                due += gaps[i]
+                while time.perf_counter() - t0 < due:
+                    time.sleep(min(0.0005, max(0.0, due - (time.perf_counter() - t0))))
+                tickets[i] = srv.submit(k, A, **kw)
+
+        th = threading.Thread(target=feeder)
+        t0 = time.perf_counter()
+        th.start()
+        th.join()
+        resps = [srv.wait(t) for t in tickets]
+        wall = time.perf_counter() - t0
+    lat = np.array([r["t_done_ms"] - r["t_submit_ms"] for r in resps])
+    ok = sum(r["status"] == 0 for r in resps)
+    errors = sorted({f'{r["status"]}: {r["message"]}' for r in resps if r["status"] != 0})[:5]
+    first = min(r["t_submit_ms"] for r in resps)
+    last = max(r["t_done_ms"] for r in resps)
+    dev = sum(r["device_ms"] for r in resps)
+    return {"requests": requests, "offered_rate_per_s": rate, "slots": slots, "ok": ok,
+            "perms_per_s": requests / ((last - first) * 1e-3), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_device_ms_per_request": dev / requests,
+            "errors": errors,
+            "wall_s": wall}
 
 
 def secondary(pb, eng):

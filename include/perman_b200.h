@@ -23,6 +23,7 @@
 #ifndef PERMAN_B200_H
 #define PERMAN_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -93,6 +94,10 @@ int perm_exact_dense(perm_ctx* ctx, const void* mat, int n, int dtype, perm_resu
  * gpu_exact_dense.cu:729-752). */
 int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int shard, int nshards,
                            perm_result* out);
+/* The Gray-index range [*first, *last) that shard `shard` of `nshards`
+ * covers for order n.  Host only (no device): depends on (n, shard, nshards)
+ * alone, so ranks on different devices always partition [0, 2^(n-1)). */
+int perm_shard_range(int n, int shard, int nshards, uint64_t* first, uint64_t* last);
 
 /* SkipPer on CRS (rptrs, cols, rvals) + CCS (cptrs, rows, cvals) of an n x n
  * matrix, 1 <= n <= 64; only the stored entries are used (x0 from the CRS row
@@ -122,6 +127,62 @@ int perm_matrix_create_dense(perm_ctx* ctx, const void* mat, int n, int dtype, p
 int perm_matrix_create_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, perm_matrix** out);
 void perm_matrix_destroy(perm_ctx* ctx, perm_matrix* m);
 int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, perm_result* out);
+
+/* ---- batches: many exact permanents in one persistent launch -------------------- */
+/* A batch holds `count` row-major matrices concatenated in `values` (matrix i
+ * has order orders[i], 1 <= order <= 40, and occupies orders[i]^2 doubles).
+ * perm_batch_create uploads them and captures the run (queue reset, one
+ * persistent kernel, result readback) as a CUDA graph; perm_batch_run replays
+ * it and writes (hi, lo) per matrix into results[2 * count] in caller order.
+ * No counterpart in the reference, which computes one matrix per call
+ * (gpu_exact_dense.cu:641); each result equals perm_exact_dense's to rounding. */
+typedef struct perm_batch perm_batch;
+int perm_batch_create(perm_ctx* ctx, int count, const int* orders, const double* values, perm_batch** out);
+int perm_batch_run(perm_ctx* ctx, perm_batch* b, double* results, double* kernel_ms);
+void perm_batch_destroy(perm_ctx* ctx, perm_batch* b);
+int perm_batch_exact(perm_ctx* ctx, int count, const int* orders, const double* values, double* results,
+                     double* kernel_ms);
+/* Measures, for each order in [n_lo, n_hi], the batch kernel with every
+ * candidate lane-range length and keeps the fastest in the context (used by
+ * later perm_batch_create calls).  m_out receives n_hi - n_lo + 1 exponents. */
+int perm_batch_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* m_out);
+
+/* ---- request loop: continuous batching on one GPU ------------------------------
+ * No counterpart in the reference.  `slots` worker contexts run requests
+ * concurrently (each with its own stream and resident scratch); a request is
+ * admitted when a slot is idle and its device-memory need fits the budget
+ * (0 = half the free device memory).  Exact requests longer than
+ * `slice_steps` Gray indices (0 = 2^31) run as several shard launches so small
+ * requests interleave.  The request's matrix is copied at submit. */
+#define PERM_REQ_EXACT_DENSE 0
+#define PERM_REQ_EXACT_SPARSE 1
+#define PERM_REQ_RASMUSSEN 2
+#define PERM_REQ_SCALING 3
+typedef struct {
+  int kind;            /* PERM_REQ_*                                      */
+  int n;
+  const double* mat;   /* row-major n x n                                */
+  int64_t trials;      /* Monte-Carlo kinds                              */
+  int scale_intervals; /* PERM_REQ_SCALING                               */
+  int scale_times;
+  uint64_t seed;
+} perm_request;
+typedef struct {
+  int status;          /* PERM_OK or the failing call's status           */
+  int kernel;          /* PERM_KERNEL_* for exact kinds                  */
+  double value, hi, lo, std_error;
+  double t_submit_ms, t_admit_ms, t_done_ms; /* since server creation      */
+  double device_ms;    /* sum of the request's kernel times              */
+  char message[160];
+} perm_response;
+typedef struct perm_server perm_server;
+int perm_server_create(int device, int slots, size_t memory_budget, uint64_t slice_steps, perm_server** out);
+int perm_server_submit(perm_server* s, const perm_request* req, uint64_t* ticket);
+/* Waits up to timeout_ms (< 0: forever) and hands the response over once. */
+int perm_server_wait(perm_server* s, uint64_t ticket, int timeout_ms, perm_response* out);
+/* out5 = submitted, completed, in flight, queued, device bytes in use. */
+int perm_server_stats(perm_server* s, double* out5);
+void perm_server_destroy(perm_server* s);
 
 /* ---- Monte-Carlo estimates of the permanent of the 0/1 pattern -------------- */
 /* trials >= 1 run exactly (the reference rounds up to a multiple of 1024);

@@ -36,9 +36,11 @@ MAX_MC_N = 64
 # Every extern "C" symbol declared in include/perman_b200.h.
 EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
-    "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_exact_dense_ex",
+    "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
     "perm_exact_dense_resident",
+    "perm_batch_create", "perm_batch_run", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune",
+    "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
     "perm_approx_scaling_sparse", "perm_read_matrix", "perm_compress", "perm_fp64_peak",
     "gpu_perman64_xshared_coalescing_mshared_int", "gpu_perman64_xshared_coalescing_mshared_float",
@@ -65,6 +67,21 @@ class PermResult(ctypes.Structure):
     _fields_ = [("value", ctypes.c_double), ("hi", ctypes.c_double), ("lo", ctypes.c_double),
                 ("steps", ctypes.c_double), ("total_steps", ctypes.c_double),
                 ("kernel_ms", ctypes.c_double), ("kernel", ctypes.c_int), ("n", ctypes.c_int)]
+
+
+class PermRequest(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("n", ctypes.c_int), ("mat", ctypes.c_void_p), ("trials", ctypes.c_int64),
+                ("scale_intervals", ctypes.c_int), ("scale_times", ctypes.c_int), ("seed", ctypes.c_uint64)]
+
+
+class PermResponse(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("kernel", ctypes.c_int), ("value", ctypes.c_double),
+                ("hi", ctypes.c_double), ("lo", ctypes.c_double), ("std_error", ctypes.c_double),
+                ("t_submit_ms", ctypes.c_double), ("t_admit_ms", ctypes.c_double), ("t_done_ms", ctypes.c_double),
+                ("device_ms", ctypes.c_double), ("message", ctypes.c_char * 160)]
+
+
+PERM_REQ_EXACT_DENSE, PERM_REQ_EXACT_SPARSE, PERM_REQ_RASMUSSEN, PERM_REQ_SCALING = 0, 1, 2, 3
 
 
 class PermEstimate(ctypes.Structure):
@@ -94,6 +111,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_exact_dense": (i, [_P, _P, i, i, ctypes.POINTER(PermResult)]),
         "perm_exact_dense_shard": (i, [_P, _P, i, i, i, i, ctypes.POINTER(PermResult)]),
         "perm_exact_dense_ex": (i, [_P, _P, i, i, i, i, i, ctypes.POINTER(PermResult)]),
+        "perm_shard_range": (i, [i, i, i, ctypes.POINTER(u64), ctypes.POINTER(u64)]),
         "perm_matrix_create_dense_ex": (i, [_P, _P, i, i, i, ctypes.POINTER(_P)]),
         "perm_exact_sparse": (i, [_P, i, _P, _P, _P, _P, _P, _P, ctypes.POINTER(PermResult)]),
         "perm_exact_sparse_ex": (i, [_P, i, _P, _P, _P, _P, _P, _P, i, ctypes.POINTER(PermResult)]),
@@ -109,6 +127,16 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
                                  ctypes.c_char_p]),
         "perm_compress": (i, [i, _P, i, _P, _P, _P, _P, _P, _P]),
         "perm_fp64_peak": (i, [_P, ctypes.POINTER(d), ctypes.POINTER(d)]),
+        "perm_batch_create": (i, [_P, i, _P, _P, ctypes.POINTER(_P)]),
+        "perm_batch_run": (i, [_P, _P, _P, ctypes.POINTER(d)]),
+        "perm_batch_destroy": (None, [_P, _P]),
+        "perm_batch_exact": (i, [_P, i, _P, _P, _P, ctypes.POINTER(d)]),
+        "perm_batch_autotune": (i, [_P, i, i, _P]),
+        "perm_server_create": (i, [i, i, ctypes.c_size_t, u64, ctypes.POINTER(_P)]),
+        "perm_server_submit": (i, [_P, ctypes.POINTER(PermRequest), ctypes.POINTER(u64)]),
+        "perm_server_wait": (i, [_P, u64, i, ctypes.POINTER(PermResponse)]),
+        "perm_server_stats": (i, [_P, _P]),
+        "perm_server_destroy": (None, [_P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -278,10 +306,50 @@ class Engine:
                                                         scale_times, seed, _ptr(tv), ctypes.byref(e)))
         return self._estimate(e, tv)
 
+    # ---- batches ----
+    def batch(self, mats) -> "Batch":
+        """Upload a list of square matrices (orders 1..40) as one resident batch."""
+        orders = np.array([np.asarray(m).shape[0] for m in mats], dtype=np.int32)
+        vals = np.ascontiguousarray(np.concatenate([np.asarray(m, dtype=np.float64).ravel() for m in mats]))
+        h = _P()
+        self._check(self.lib.perm_batch_create(self.ctx, len(mats), _ptr(orders), _ptr(vals), ctypes.byref(h)))
+        return Batch(self, h, len(mats))
+
+    def batch_exact(self, mats) -> tuple[np.ndarray, float]:
+        b = self.batch(mats)
+        try:
+            return b.run()
+        finally:
+            b.free()
+
+    def batch_autotune(self, n_lo: int, n_hi: int) -> dict:
+        out = np.zeros(n_hi - n_lo + 1, dtype=np.int32)
+        self._check(self.lib.perm_batch_autotune(self.ctx, n_lo, n_hi, _ptr(out)))
+        return {n_lo + i: int(m) for i, m in enumerate(out)}
+
     def fp64_peak(self) -> tuple[float, float]:
         ops, ms = ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.perm_fp64_peak(self.ctx, ctypes.byref(ops), ctypes.byref(ms)))
         return ops.value, ms.value
+
+
+class Batch:
+    """A resident batch; run() replays its captured CUDA graph."""
+
+    def __init__(self, engine: Engine, handle, count: int):
+        self.engine, self.handle, self.count = engine, handle, count
+
+    def run(self) -> tuple[np.ndarray, float]:
+        """Returns (values, device ms); values[i] = hi + lo of matrix i."""
+        res = np.zeros(2 * self.count, dtype=np.float64)
+        ms = ctypes.c_double()
+        self.engine._check(self.engine.lib.perm_batch_run(self.engine.ctx, self.handle, _ptr(res), ctypes.byref(ms)))
+        return res[0::2] + res[1::2], ms.value
+
+    def free(self):
+        if self.handle:
+            self.engine.lib.perm_batch_destroy(self.engine.ctx, self.handle)
+            self.handle = None
 
 
 class ResidentMatrix:
@@ -300,6 +368,53 @@ class ResidentMatrix:
         if self.handle:
             self.engine.lib.perm_matrix_destroy(self.engine.ctx, self.handle)
             self.handle = None
+
+
+class Server:
+    """Request loop on one GPU (continuous batching over `slots` contexts)."""
+
+    def __init__(self, device: int = 0, slots: int = 4, memory_budget: int = 0, slice_steps: int = 0, lib_path=None):
+        self.lib = load_library(lib_path)
+        h = _P()
+        rc = self.lib.perm_server_create(device, slots, memory_budget, slice_steps, ctypes.byref(h))
+        if rc != PERM_OK:
+            raise PermError(rc, f"cannot create a server on device {device}")
+        self.handle = h
+
+    def submit(self, kind: int, mat, trials: int = 0, scale_intervals: int = 4, scale_times: int = 5,
+               seed: int = 1) -> int:
+        a = np.ascontiguousarray(mat, dtype=np.float64)
+        req = PermRequest(kind, a.shape[0], a.ctypes.data, trials, scale_intervals, scale_times, seed)
+        t = ctypes.c_uint64()
+        rc = self.lib.perm_server_submit(self.handle, ctypes.byref(req), ctypes.byref(t))
+        if rc != PERM_OK:
+            raise PermError(rc, "submit failed")
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> dict:
+        r = PermResponse()
+        rc = self.lib.perm_server_wait(self.handle, ticket, timeout_ms, ctypes.byref(r))
+        if rc != PERM_OK:
+            raise PermError(rc, f"wait for ticket {ticket} failed")
+        return {"status": r.status, "kernel": r.kernel, "value": r.value, "hi": r.hi, "lo": r.lo,
+                "std_error": r.std_error, "t_submit_ms": r.t_submit_ms, "t_admit_ms": r.t_admit_ms,
+                "t_done_ms": r.t_done_ms, "device_ms": r.device_ms, "message": r.message.decode(errors="replace")}
+
+    def stats(self) -> dict:
+        out = np.zeros(5)
+        self.lib.perm_server_stats(self.handle, _ptr(out))
+        return dict(zip(("submitted", "completed", "in_flight", "queued", "bytes_in_use"), out.tolist()))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.perm_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 # ---- host-only helpers (no device needed) -------------------------------------
@@ -341,6 +456,54 @@ def compress(mode: int, mat) -> dict:
         raise PermError(nnz, "perm_compress failed")
     return {"n": n, "nnz": nnz, "mat": a, "cptrs": cptrs, "rows": rows[:nnz], "cvals": cvals[:nnz],
             "rptrs": rptrs, "cols": cols[:nnz], "rvals": rvals[:nnz]}
+
+
+def shard_range(n: int, shard: int, nshards: int) -> tuple[int, int]:
+    """Gray-index range [first, last) of one shard (host only, device independent)."""
+    lib = load_library()
+    a, b = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib.perm_shard_range(n, shard, nshards, ctypes.byref(a), ctypes.byref(b))
+    if rc != PERM_OK:
+        raise PermError(rc, f"bad shard request n={n} shard={shard}/{nshards}")
+    return a.value, b.value
+
+
+def dd_sum(pairs) -> tuple[float, float]:
+    """Double-double sum of (hi, lo) pairs in the given order."""
+    hi = lo = 0.0
+    for h, l in pairs:
+        s = hi + h
+        bb = s - hi
+        lo += ((hi - (s - bb)) + (h - bb)) + l
+        hi = s
+    s = hi + lo
+    return s, lo - (s - hi)
+
+
+def distributed_exact_dense(mat, group=None, engine: Engine | None = None, shard_fn=None) -> tuple[float, float]:
+    """Exact permanent of one matrix over all ranks of a torch.distributed group.
+
+    Rank r computes shard r of world (perm_exact_dense_shard on its own GPU),
+    the 16-byte (hi, lo) partials are all-gathered -- the only collective --
+    and every rank adds them in rank order (double-double, deterministic).
+    `shard_fn(mat, rank, world) -> (hi, lo)` replaces the device call; it
+    exists so that the host logic can be exercised without a GPU."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    if shard_fn is None:
+        eng = engine or default_engine()
+        r = eng.exact_dense_shard(mat, rank, world)
+        part = (r.hi, r.lo)
+    else:
+        part = shard_fn(mat, rank, world)
+    backend = dist.get_backend(group)
+    dev = f"cuda:{torch.cuda.current_device()}" if backend == "nccl" else "cpu"
+    t = torch.tensor([part[0], part[1]], dtype=torch.float64, device=dev)
+    gathered = [torch.zeros_like(t) for _ in range(world)]
+    dist.all_gather(gathered, t, group=group)
+    return dd_sum((float(g[0]), float(g[1])) for g in gathered)
 
 
 # ---- reference-named entry points (argument meaning as in the reference) ------

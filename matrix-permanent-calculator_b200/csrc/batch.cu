@@ -1,0 +1,190 @@
+// batch.cu -- many exact permanents of mixed order in one persistent launch.
+//
+// The reference computes one matrix per call (gpu_exact_dense.cu:641-699); a
+// batch of thousands of small matrices would be thousands of launches, each
+// too small to fill the GPU.  Here the Gray ranges of all matrices are cut
+// into tiles -- one warp-sized piece: 32 lanes x 2^m aligned Gray indices -- and
+// a persistent grid of warps drains a global tile queue, largest matrices
+// first.  A warp stages its tile's matrix into its own shared-memory slot
+// (kept when the next tile is from the same matrix), walks the lanes' ranges
+// with the same register-X step as ryser_dense.cuh, reduces the tile to one
+// double-double and stores it; the warp that completes a matrix's last tile
+// (per-matrix atomic ticket) sums that matrix's tile partials in tile order --
+// deterministic -- and writes (hi, lo).  Orders 1..kBatchMaxOrder; per-order
+// lane-range lengths 2^m come from the autotuner (or a default).
+#include <cuda_runtime.h>
+
+#include "batch.h"
+#include "ryser_dense.cuh"
+
+namespace perm {
+
+namespace {
+
+// Walk lane range [s, e) (aligned, multiple of 8, e > s) of an order-N matrix
+// whose columns are at col (stride np) and x0 at x0s.
+template <int N>
+__device__ __noinline__ void walk_range(const double* col, int np, const double* x0s, uint64_t s, uint64_t e,
+                                           Acc& acc) {
+  double x[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) x[j] = x0s[j];
+  const uint64_t g = s ^ (s >> 1);
+#pragma unroll 1
+  for (int k = 0; k < N - 1; k++) {
+    if ((g >> k) & 1) {
+#pragma unroll
+      for (int j = 0; j < N; j++) x[j] += col[k * np + j];
+    }
+  }
+  acc.add(prod_only<N>(x));
+  const double* c0 = col;
+  const double* c1 = col + np;
+  const double* c2 = col + 2 * np;
+  const uint64_t groups = (e - s) >> 3;
+  uint64_t base = s;
+#pragma unroll 1
+  for (uint64_t gi = 0; gi + 1 < groups; gi++, base += 8) {
+    const double s4 = ((base >> 3) & 1) ? -1.0 : 1.0;
+    const uint64_t i8 = base + 8;
+    const int k8 = __ffsll((long long)i8) - 1;
+    const double s8 = ((i8 >> (k8 + 1)) & 1) ? -1.0 : 1.0;
+    double t1 = step<N, +1>(x, c0, 0.0);
+    double t2 = step<N, +1>(x, c1, 0.0);
+    double t3 = step<N, -1>(x, c0, 0.0);
+    double t4 = step<N, 0>(x, c2, s4);
+    double t5 = step<N, +1>(x, c0, 0.0);
+    double t6 = step<N, -1>(x, c1, 0.0);
+    double t7 = step<N, -1>(x, c0, 0.0);
+    double t8 = step<N, 0>(x, col + k8 * np, s8);
+    acc.add(((t2 - t1) + (t4 - t3)) + ((t6 - t5) + (t8 - t7)));
+  }
+  const double s4 = ((base >> 3) & 1) ? -1.0 : 1.0;
+  double t1 = step<N, +1>(x, c0, 0.0);
+  double t2 = step<N, +1>(x, c1, 0.0);
+  double t3 = step<N, -1>(x, c0, 0.0);
+  double t4 = step<N, 0>(x, c2, s4);
+  double t5 = step<N, +1>(x, c0, 0.0);
+  double t6 = step<N, -1>(x, c1, 0.0);
+  double t7 = step<N, -1>(x, c0, 0.0);
+  acc.add(((t2 - t1) + (t4 - t3)) + ((t6 - t5) - t7));
+}
+
+// Orders below 9 have fewer than 256 Gray indices: lane 0 walks them all.
+__device__ void walk_small(const double* col, int np, const double* x0s, int n, Acc& acc) {
+  double x[8];
+  for (int j = 0; j < n; j++) x[j] = x0s[j];
+  const uint64_t total = 1ull << (n - 1);
+  for (uint64_t i = 0; i < total; i++) {
+    if (i) {
+      const int k = __ffsll((long long)i) - 1;
+      const double s = ((i >> (k + 1)) & 1) ? -1.0 : 1.0;
+      for (int j = 0; j < n; j++) x[j] = fma(s, col[k * np + j], x[j]);
+    }
+    double p = x[0];
+    for (int j = 1; j < n; j++) p *= x[j];
+    acc.add((i & 1) ? -p : p);
+  }
+}
+
+__device__ __forceinline__ void walk_dispatch(int n, const double* col, int np, const double* x0s, uint64_t s,
+                                              uint64_t e, Acc& acc) {
+  switch (n) {
+#define PERM_BATCH_CASE(N) \
+  case N: walk_range<N>(col, np, x0s, s, e, acc); break;
+    PERM_BATCH_CASE(9) PERM_BATCH_CASE(10) PERM_BATCH_CASE(11) PERM_BATCH_CASE(12) PERM_BATCH_CASE(13)
+    PERM_BATCH_CASE(14) PERM_BATCH_CASE(15) PERM_BATCH_CASE(16) PERM_BATCH_CASE(17) PERM_BATCH_CASE(18)
+    PERM_BATCH_CASE(19) PERM_BATCH_CASE(20) PERM_BATCH_CASE(21) PERM_BATCH_CASE(22) PERM_BATCH_CASE(23)
+    PERM_BATCH_CASE(24) PERM_BATCH_CASE(25) PERM_BATCH_CASE(26) PERM_BATCH_CASE(27) PERM_BATCH_CASE(28)
+    PERM_BATCH_CASE(29) PERM_BATCH_CASE(30) PERM_BATCH_CASE(31) PERM_BATCH_CASE(32) PERM_BATCH_CASE(33)
+    PERM_BATCH_CASE(34) PERM_BATCH_CASE(35) PERM_BATCH_CASE(36) PERM_BATCH_CASE(37) PERM_BATCH_CASE(38)
+    PERM_BATCH_CASE(39) PERM_BATCH_CASE(40)
+#undef PERM_BATCH_CASE
+    default: break;
+  }
+}
+
+__device__ __forceinline__ int find_matrix(const BatchMatrix* mats, int count, uint64_t tile) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {  // last matrix with first_tile <= tile
+    const int mid = (lo + hi + 1) >> 1;
+    if (mats[mid].first_tile <= tile)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kBatchBlock) batch_kernel(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* slot = reinterpret_cast<double*>(smem) + (size_t)wib * kBatchSlotDoubles;  // [n][np] + x0[np]
+  int cached = -1;
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(a.next_tile, 1ull);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= a.total_tiles) break;
+    const int mi = find_matrix(a.mats, a.count, t);
+    const BatchMatrix M = a.mats[mi];
+    const int n = M.n, np = (n + 1) & ~1;
+    if (mi != cached) {
+      __syncwarp();
+      const double* src = a.operands + M.offset;
+      for (int idx = lane; idx < n * np; idx += 32) slot[idx] = src[idx];
+      __syncwarp();
+      double* x0 = slot + n * np;
+      for (int j = lane; j < n; j += 32) {
+        double rs = 0.0;
+        for (int k = 0; k < n; k++) rs += slot[k * np + j];
+        x0[j] = slot[(n - 1) * np + j] - rs * 0.5;
+      }
+      __syncwarp();
+      cached = mi;
+    }
+    const double* x0 = slot + n * np;
+    Acc acc;
+    if (n < 9) {
+      if (lane == 0) walk_small(slot, np, x0, n, acc);
+    } else {
+      const uint64_t q = t - M.first_tile;
+      const uint64_t L = 1ull << M.m;
+      const uint64_t s = (q * 32 + lane) * L;
+      walk_dispatch(n, slot, np, x0, s, s + L, acc);
+    }
+    dd v = acc.value();
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) v = dd_add(v, dd_shfl_down(v, d));
+    bool last = false;
+    if (lane == 0) {
+      a.tile_partials[t] = v;
+      __threadfence();
+      const unsigned prev = atomicAdd(&a.mat_done[mi], 1u);
+      last = (prev == M.ntiles - 1);
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
+      __threadfence();
+      dd s = {0.0, 0.0};
+      for (uint64_t k = lane; k < M.ntiles; k += 32) {
+        dd p;
+        p.hi = __ldcg(&a.tile_partials[M.first_tile + k].hi);
+        p.lo = __ldcg(&a.tile_partials[M.first_tile + k].lo);
+        s = dd_add(s, p);
+      }
+#pragma unroll
+      for (int d = 16; d >= 1; d >>= 1) s = dd_add(s, dd_shfl_down(s, d));
+      if (lane == 0) {
+        const double f = (n & 1) ? 2.0 : -2.0;
+        a.results[2 * M.index] = s.hi * f;
+        a.results[2 * M.index + 1] = s.lo * f;
+        a.mat_done[mi] = 0u;
+      }
+    }
+  }
+}
+
+}  // namespace perm

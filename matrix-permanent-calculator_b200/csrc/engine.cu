@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/perman_b200.h"
+#include "batch.h"
 #include "matrix_io.h"
 #include "mc.h"
 #include "perman_common.cuh"
@@ -111,6 +112,8 @@ struct perm_ctx {
   double* d_trials = nullptr;
   size_t d_trials_cap = 0;
   int dense_occ[8][PERM_MAX_EXACT_N + 1] = {};  // [0]: FP64-X, [G]: int32-X groups of G
+  int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
+  int batch_occ = 0;
   std::string err;
   std::mutex mu;
 };
@@ -371,6 +374,32 @@ struct DensePlan {
   uint64_t block0 = 0, nblocks = 0;
 };
 
+// Shard boundaries depend on (n, shard, nshards) only -- never on the device
+// -- so ranks with different grids still partition [0, 2^(n-1)) exactly:
+// shards are cut at multiples of 2^ms, ms = max(3, n - 21) (at most 2^20
+// shard units), and the kernel's range alignment m never exceeds ms.
+static void shard_bounds(int n, int shard, int nshards, uint64_t* first, uint64_t* last, int* ms_out) {
+  const uint64_t total = 1ull << (n - 1);
+  if (n < 4) {
+    *first = shard == 0 ? 0 : total;
+    *last = total;
+    if (ms_out) *ms_out = 0;
+    return;
+  }
+  const int ms = std::max(3, n - 21);
+  const uint64_t units = total >> ms;
+  *first = (units * (uint64_t)shard / (uint64_t)nshards) << ms;
+  *last = (units * (uint64_t)(shard + 1) / (uint64_t)nshards) << ms;
+  if (ms_out) *ms_out = ms;
+}
+
+extern "C" int perm_shard_range(int n, int shard, int nshards, uint64_t* first, uint64_t* last) {
+  if (n < 1 || n > PERM_MAX_EXACT_N || nshards < 1 || shard < 0 || shard >= nshards || !first || !last)
+    return PERM_EINVAL;
+  shard_bounds(n, shard, nshards, first, last, nullptr);
+  return PERM_OK;
+}
+
 static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nshards, DensePlan* p) {
   const int n = op.n;
   const void* fn = operand_kernel(op);
@@ -381,7 +410,9 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
     CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, operand_smem(op)));
     occ_slot = std::max(occ, 1);
   }
-  const uint64_t total = 1ull << (n - 1);
+  uint64_t first = 0, last = 0;
+  int ms = 0;
+  shard_bounds(n, shard, nshards, &first, &last, &ms);
   if (n < 4) {
     p->grid = 1;
     p->m = 0;
@@ -390,18 +421,16 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
     return PERM_OK;
   }
   int grid = std::min(kMaxBlocks, ctx->num_sms * occ_slot);
-  // Alignment m: each thread should own >= 64 aligned blocks when possible.
-  const uint64_t threads = (uint64_t)grid * 128 * (uint64_t)nshards;
+  // Alignment m <= ms: each thread should own >= 64 aligned blocks when possible.
+  const uint64_t len = last - first;
+  const uint64_t threads = (uint64_t)grid * 128;
   int m = 3;
-  while (m < 20 && m < n - 1 && (total >> (m + 1)) >= threads * 64) m++;
-  const uint64_t all_blocks = total >> m;
-  const uint64_t b0 = all_blocks * (uint64_t)shard / (uint64_t)nshards;
-  const uint64_t b1 = all_blocks * (uint64_t)(shard + 1) / (uint64_t)nshards;
-  const uint64_t mine = b1 - b0;
+  while (m < 20 && m < ms && (len >> (m + 1)) >= threads * 64) m++;
+  const uint64_t mine = len >> m;
   if (mine < (uint64_t)grid * 128) grid = (int)std::max<uint64_t>(1, (mine + 127) / 128);
   p->grid = grid;
   p->m = m;
-  p->block0 = b0;
+  p->block0 = first >> m;
   p->nblocks = mine;
   return PERM_OK;
 }
@@ -848,6 +877,227 @@ extern "C" int perm_approx_scaling_sparse(perm_ctx* ctx, int n, const int* rptrs
   (void)cptrs;
   (void)rows;
   return mc_sparse(ctx, n, rptrs, cols, true, trials, y, z, seed, tv, out);
+}
+
+// ---------------------------------------------------------------------------
+// batched exact permanents (one persistent launch, captured in a CUDA graph)
+// ---------------------------------------------------------------------------
+struct perm_batch {
+  int count = 0;
+  uint64_t total_tiles = 0;
+  int grid = 1;
+  double* d_operands = nullptr;
+  BatchMatrix* d_mats = nullptr;
+  dd* d_tile_partials = nullptr;
+  unsigned* d_mat_done = nullptr;
+  unsigned long long* d_next = nullptr;
+  double* d_results = nullptr;
+  double* h_results = nullptr;  // pinned
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static void batch_free(perm_batch* b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  cudaFree(b->d_operands);
+  cudaFree(b->d_mats);
+  cudaFree(b->d_tile_partials);
+  cudaFree(b->d_mat_done);
+  cudaFree(b->d_next);
+  cudaFree(b->d_results);
+  if (b->h_results) cudaFreeHost(b->h_results);
+  delete b;
+}
+
+static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, const double* values,
+                               const int* m_override, perm_batch** out) {
+  if (count < 1 || !orders || !values || !out) return fail(ctx, PERM_EINVAL, "empty batch or null pointer");
+  std::vector<BatchMatrix> mats(count);
+  std::vector<uint64_t> src_off(count);
+  uint64_t off = 0, img = 0;
+  for (int i = 0; i < count; i++) {
+    const int n = orders[i];
+    if (n < 1 || n > kBatchMaxOrder)
+      return fail(ctx, PERM_EUNSUPPORTED, "batch order %d (matrix %d) outside [1, %d]", n, i, kBatchMaxOrder);
+    src_off[i] = off;
+    off += (uint64_t)n * n;
+    BatchMatrix& M = mats[i];
+    M.n = n;
+    M.index = i;
+    M.m = m_override ? m_override[n] : (ctx->batch_m[n] ? ctx->batch_m[n] : batch_default_m(n));
+    if (n >= 9 && (M.m < 3 || M.m > n - 6)) M.m = batch_default_m(n);
+    M.ntiles = n < 9 ? 1u : (uint32_t)((1ull << (n - 1)) >> (M.m + 5));
+    const int np = (n + 1) & ~1;
+    M.offset = img;
+    img += (uint64_t)n * np;
+  }
+  // queue order: most Gray work first (longest-processing-time scheduling)
+  std::vector<int> order(count);
+  for (int i = 0; i < count; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return mats[x].n > mats[y].n; });
+  std::vector<BatchMatrix> q(count);
+  uint64_t tiles = 0;
+  for (int r = 0; r < count; r++) {
+    q[r] = mats[order[r]];
+    q[r].first_tile = tiles;
+    tiles += q[r].ntiles;
+  }
+  std::vector<double> image(img);
+  for (int i = 0; i < count; i++) {
+    const int n = mats[i].n, np = (n + 1) & ~1;
+    const double* a = values + src_off[i];
+    double* dst = image.data() + mats[i].offset;
+    for (int k = 0; k < n; k++)
+      for (int j = 0; j < np; j++) dst[(size_t)k * np + j] = j < n ? a[(size_t)j * n + k] : 0.0;
+  }
+  perm_batch* b = new perm_batch();
+  b->count = count;
+  b->total_tiles = tiles;
+  cudaError_t e;
+#define BT(expr)                                    \
+  do {                                              \
+    e = (expr);                                     \
+    if (e != cudaSuccess) {                         \
+      batch_free(b);                                \
+      return fail_cuda(ctx, e, #expr);              \
+    }                                               \
+  } while (0)
+  BT(cudaMalloc(&b->d_operands, sizeof(double) * std::max<uint64_t>(img, 1)));
+  BT(cudaMalloc(&b->d_mats, sizeof(BatchMatrix) * count));
+  BT(cudaMalloc(&b->d_tile_partials, sizeof(dd) * tiles));
+  BT(cudaMalloc(&b->d_mat_done, sizeof(unsigned) * count));
+  BT(cudaMalloc(&b->d_next, sizeof(unsigned long long)));
+  BT(cudaMalloc(&b->d_results, sizeof(double) * 2 * count));
+  BT(cudaMallocHost(&b->h_results, sizeof(double) * 2 * count));
+  BT(cudaMemcpy(b->d_operands, image.data(), sizeof(double) * img, cudaMemcpyHostToDevice));
+  BT(cudaMemcpy(b->d_mats, q.data(), sizeof(BatchMatrix) * count, cudaMemcpyHostToDevice));
+  BT(cudaMemset(b->d_mat_done, 0, sizeof(unsigned) * count));
+  if (!ctx->batch_occ) {
+    BT(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem_bytes()));
+    int occ = 0;
+    BT(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, kBatchBlock, batch_smem_bytes()));
+    ctx->batch_occ = std::max(occ, 1);
+  }
+  const uint64_t warps = (uint64_t)ctx->num_sms * ctx->batch_occ * (kBatchBlock / 32);
+  const uint64_t want = std::min<uint64_t>(warps, tiles);
+  b->grid = (int)std::max<uint64_t>(1, (want + (kBatchBlock / 32) - 1) / (kBatchBlock / 32));
+  // capture: reset the queue head, run, read the results back
+  BatchArgs args;
+  args.operands = b->d_operands;
+  args.mats = b->d_mats;
+  args.count = count;
+  args.total_tiles = tiles;
+  args.next_tile = b->d_next;
+  args.tile_partials = b->d_tile_partials;
+  args.mat_done = b->d_mat_done;
+  args.results = b->d_results;
+  void* kargs[] = {&args};
+  BT(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), ctx->stream);
+  cudaLaunchKernel((const void*)batch_kernel, dim3(b->grid), dim3(kBatchBlock), kargs, batch_smem_bytes(), ctx->stream);
+  cudaMemcpyAsync(b->h_results, b->d_results, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, ctx->stream);
+  BT(cudaStreamEndCapture(ctx->stream, &b->graph));
+  BT(cudaGraphInstantiate(&b->exec, b->graph, 0));
+#undef BT
+  *out = b;
+  return PERM_OK;
+}
+
+extern "C" int perm_batch_create(perm_ctx* ctx, int count, const int* orders, const double* values,
+                                 perm_batch** out) {
+  if (!ctx) return PERM_EINVAL;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  return batch_create_locked(ctx, count, orders, values, nullptr, out);
+}
+
+static int batch_run_locked(perm_ctx* ctx, perm_batch* b, double* results, double* kernel_ms) {
+  CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  CU(ctx, cudaGraphLaunch(b->exec, ctx->stream));
+  CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  CU(ctx, cudaStreamSynchronize(ctx->stream));
+  CU(ctx, cudaGetLastError());
+  float ms = 0;
+  CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  if (kernel_ms) *kernel_ms = ms;
+  if (results) memcpy(results, b->h_results, sizeof(double) * 2 * b->count);
+  return PERM_OK;
+}
+
+extern "C" int perm_batch_run(perm_ctx* ctx, perm_batch* b, double* results, double* kernel_ms) {
+  if (!ctx || !b) return ctx ? fail(ctx, PERM_EINVAL, "null batch") : PERM_EINVAL;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  return batch_run_locked(ctx, b, results, kernel_ms);
+}
+
+extern "C" void perm_batch_destroy(perm_ctx* ctx, perm_batch* b) {
+  if (ctx) cudaSetDevice(ctx->device);
+  batch_free(b);
+}
+
+extern "C" int perm_batch_exact(perm_ctx* ctx, int count, const int* orders, const double* values, double* results,
+                                double* kernel_ms) {
+  perm_batch* b = nullptr;
+  int rc = perm_batch_create(ctx, count, orders, values, &b);
+  if (rc) return rc;
+  rc = perm_batch_run(ctx, b, results, kernel_ms);
+  perm_batch_destroy(ctx, b);
+  return rc;
+}
+
+// Autotuner: for each order in [n_lo, n_hi] time a synthetic batch of that
+// order (~2^26 Gray steps in total) with each candidate lane-range exponent
+// and keep the fastest in the context; m_out (n_hi - n_lo + 1 ints) receives
+// the choices.
+extern "C" int perm_batch_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* m_out) {
+  if (!ctx) return PERM_EINVAL;
+  if (n_lo < 1 || n_hi > kBatchMaxOrder || n_lo > n_hi) return fail(ctx, PERM_EINVAL, "orders [%d, %d]", n_lo, n_hi);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  uint64_t state = 0x243F6A8885A308D3ull;
+  for (int n = n_lo; n <= n_hi; n++) {
+    if (n < 9) {
+      ctx->batch_m[n] = 0;
+      if (m_out) m_out[n - n_lo] = 0;
+      continue;
+    }
+    const int count = (int)std::max<uint64_t>(1, (1ull << 26) >> (n - 1));
+    std::vector<int> orders(count, n);
+    std::vector<double> vals((size_t)count * n * n);
+    for (double& v : vals) {
+      state = state * 6364136223846793005ull + 1442695040888963407ull;
+      v = 1.0 - (double)(state >> 11) * (1.0 / 9007199254740992.0);
+    }
+    int best_m = batch_default_m(n);
+    double best_ms = 1e30;
+    for (int m = 3; m <= std::min(16, n - 6); m++) {
+      int mo[kBatchMaxOrder + 1] = {};
+      mo[n] = m;
+      perm_batch* b = nullptr;
+      int rc = batch_create_locked(ctx, count, orders.data(), vals.data(), mo, &b);
+      if (rc) return rc;
+      double ms = 1e30, t = 0;
+      for (int rep = 0; rep < 3; rep++) {
+        rc = batch_run_locked(ctx, b, nullptr, &t);
+        if (rc) {
+          batch_free(b);
+          return rc;
+        }
+        if (rep) ms = std::min(ms, t);
+      }
+      batch_free(b);
+      if (ms < best_ms * 0.98) {
+        best_ms = ms;
+        best_m = m;
+      }
+    }
+    ctx->batch_m[n] = best_m;
+    if (m_out) m_out[n - n_lo] = best_m;
+  }
+  return PERM_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,72 @@
+"""Batched persistent kernel: every matrix of a mixed-order batch equals the
+single-matrix kernel's result and the oracle within 1e-10 relative (the two
+kernels cut the Gray walk differently, so real-valued matrices with heavy
+cancellation differ in the last ~12 digits)."""
+import numpy as np
+import pytest
+from conftest import bernoulli, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_batch(rng, count, lo, hi):
+    mats = []
+    for i in range(count):
+        n = int(rng.integers(lo, hi + 1))
+        d = rng.uniform(0.2, 0.9)
+        m = bernoulli(rng, n, d) if n > 1 else np.ones((1, 1))
+        if i % 2:
+            m = m * (1.0 - rng.random((n, n)))
+        mats.append(m)
+    return mats
+
+
+def test_batch_matches_single_matrix_kernel(engine, pb):
+    rng = np.random.default_rng(404)
+    mats = mixed_batch(rng, 300, 1, 26) + [np.ones((n, n)) for n in (1, 2, 3, 8, 9)]
+    vals, ms = engine.batch_exact(mats)
+    assert ms > 0
+    for m, v in zip(mats, vals):
+        want = engine.exact_dense(m, variant=pb.PERM_KERNEL_DENSE).value
+        assert rel_err(v, want) < 1e-10, (m.shape, v, want)
+
+
+def test_batch_vs_oracle_and_golden(engine, orc, golden):
+    cases = [c for c in golden.values() if c["n"] <= 40]
+    vals, _ = engine.batch_exact([c["A"] for c in cases])
+    for c, v in zip(cases, vals):
+        want = int(c["exact"]) if "exact" in c else c["dd"][0] + c["dd"][1]
+        assert rel_err(v, want) < 1e-10, c["name"]
+    rng = np.random.default_rng(5)
+    mats = [rng.standard_normal((n, n)) for n in (10, 13, 17)]
+    vals, _ = engine.batch_exact(mats)
+    for m, v in zip(mats, vals):
+        hi, lo = orc.perm_dd(m)
+        assert abs(v - (hi + lo)) <= 1e-9 * max(abs(hi), 1e-300)
+
+
+def test_batch_is_deterministic_and_replayable(engine):
+    rng = np.random.default_rng(9)
+    b = engine.batch(mixed_batch(rng, 200, 9, 24))
+    try:
+        v1, _ = b.run()
+        v2, _ = b.run()
+        np.testing.assert_array_equal(v1, v2)
+    finally:
+        b.free()
+
+
+def test_autotune_keeps_results(engine, pb):
+    rng = np.random.default_rng(10)
+    mats = mixed_batch(rng, 64, 12, 22)
+    before, _ = engine.batch_exact(mats)
+    table = engine.batch_autotune(12, 22)
+    assert all(3 <= m <= n - 6 for n, m in table.items())
+    after, _ = engine.batch_exact(mats)
+    for a, b in zip(before, after):
+        assert rel_err(a, b) < 1e-12
+
+
+def test_batch_rejects_large_order(engine, pb):
+    with pytest.raises(pb.PermError):
+        engine.batch_exact([np.ones((41, 41))])

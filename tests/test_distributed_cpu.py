@@ -1,0 +1,79 @@
+"""Multi-GPU host logic on CPU: shard ranges partition the Gray walk exactly
+for any (n, world), and world_size-2 gloo ranks that each sum their shard
+(with the oracle standing in for the device) recombine to the permanent."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 9, 17, 30, 40, 64])
+@pytest.mark.parametrize("world", [1, 2, 3, 8, 13])
+def test_shard_ranges_partition(pb, n, world):
+    total = 1 << (n - 1)
+    prev = 0
+    for s in range(world):
+        a, b = pb.shard_range(n, s, world)
+        assert a == prev and b >= a
+        if n >= 4:
+            ms = max(3, n - 21)
+            assert a % (1 << ms) == 0 and b % (1 << ms) == 0
+        prev = b
+    assert prev == total
+
+
+def test_dd_sum_is_exactish(pb):
+    parts = [(1e16, 1.0), (-1e16, 0.5), (3.0, 1e-17)]
+    hi, lo = pb.dd_sum(parts)
+    assert hi + lo == 4.5
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, A, out_path):
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    sys.path.insert(0, str(root / "tests"))
+    sys.path.insert(0, str(root / "oracle"))
+    import torch.distributed as dist
+    from conftest import load_package
+    from oracle import Oracle
+
+    pb = load_package()
+    orc = Oracle()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    n = A.shape[0]
+    factor = 2.0 if n & 1 else -2.0
+
+    def shard_fn(mat, r, w):  # CPU stand-in for perm_exact_dense_shard
+        a, b = pb.shard_range(n, r, w)
+        hi, lo = orc.ryser_dd_range(mat, a, b, threads=1)
+        return hi * factor, lo * factor
+
+    hi, lo = pb.distributed_exact_dense(A, shard_fn=shard_fn)
+    dist.barrier()
+    dist.destroy_process_group()
+    np.save(f"{out_path}.{rank}.npy", np.array([hi, lo]))
+
+
+@pytest.mark.parametrize("n", [11, 16])
+def test_gloo_two_ranks_recombine(pb, orc, tmp_path, n):
+    rng = np.random.default_rng(n)
+    A = rng.random((n, n))
+    port = _free_port()
+    out = str(tmp_path / "res")
+    mp.start_processes(_rank_main, args=(2, port, A, out), nprocs=2, join=True, start_method="spawn")
+    want = sum(orc.perm_dd(A))
+    for r in range(2):
+        hi, lo = np.load(f"{out}.{r}.npy")
+        assert abs((hi + lo) - want) <= 1e-14 * abs(want)

@@ -1,0 +1,78 @@
+"""Request loop: every result is the same alone and in the mix (exact: 1e-12
+relative -- large requests run as shards, which changes the rounding only;
+Monte Carlo: bit-identical, same Philox streams), work of different slots
+overlaps on the device, and a bad request fails alone."""
+import numpy as np
+import pytest
+from conftest import bernoulli, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def make_requests(pb, rng, count):
+    reqs = []
+    for i in range(count):
+        kind = i % 4
+        if kind in (0, 1):
+            n = int(rng.integers(12, 27))
+            A = bernoulli(rng, n, 0.5) * (1.0 - rng.random((n, n)))
+            reqs.append((pb.PERM_REQ_EXACT_DENSE if kind == 0 else pb.PERM_REQ_EXACT_SPARSE, A, {}))
+        else:
+            n = int(rng.integers(20, 41))
+            A = bernoulli(rng, n, 0.5)
+            reqs.append((pb.PERM_REQ_RASMUSSEN if kind == 2 else pb.PERM_REQ_SCALING, A,
+                         {"trials": 20000, "seed": 100 + i}))
+    return reqs
+
+
+def alone(engine, pb, kind, A, kw):
+    if kind == pb.PERM_REQ_EXACT_DENSE:
+        return engine.exact_dense(A).value
+    if kind == pb.PERM_REQ_EXACT_SPARSE:
+        return engine.exact_sparse_matrix(A, order=0).value
+    if kind == pb.PERM_REQ_RASMUSSEN:
+        return engine.rasmussen(A, kw["trials"], seed=kw["seed"]).mean
+    return engine.scaling(A, kw["trials"], 4, 5, seed=kw["seed"]).mean
+
+
+def test_results_same_alone_and_in_the_mix(engine, pb):
+    rng = np.random.default_rng(77)
+    reqs = make_requests(pb, rng, 48)
+    with pb.Server(0, slots=4, slice_steps=1 << 20) as srv:
+        tickets = [srv.submit(k, A, **kw) for k, A, kw in reqs]
+        resps = [srv.wait(t) for t in tickets]
+    overlap = 0
+    for (k, A, kw), r in zip(reqs, resps):
+        assert r["status"] == pb.PERM_OK, r["message"]
+        want = alone(engine, pb, k, A, kw)
+        if k in (pb.PERM_REQ_RASMUSSEN, pb.PERM_REQ_SCALING):
+            assert r["value"] == want
+        else:
+            assert rel_err(r["value"], want) < 1e-12
+    spans = sorted((r["t_admit_ms"], r["t_done_ms"]) for r in resps)
+    for (a0, d0), (a1, d1) in zip(spans, spans[1:]):
+        overlap += a1 < d0
+    assert overlap > 0, "no two requests were ever in flight together"
+
+
+def test_bad_request_fails_alone(pb):
+    rng = np.random.default_rng(3)
+    with pb.Server(0, slots=2) as srv:
+        good = srv.submit(pb.PERM_REQ_EXACT_DENSE, bernoulli(rng, 14, 0.5))
+        bad = srv.submit(pb.PERM_REQ_EXACT_DENSE, np.ones((70, 70)))
+        mc_bad = srv.submit(pb.PERM_REQ_SCALING, np.ones((10, 10)), trials=0)
+        assert srv.wait(good)["status"] == pb.PERM_OK
+        assert srv.wait(bad)["status"] == pb.PERM_EUNSUPPORTED
+        assert srv.wait(mc_bad)["status"] == pb.PERM_EINVAL
+
+
+def test_memory_budget_admission(pb):
+    """A budget smaller than two requests forces one-at-a-time admission."""
+    rng = np.random.default_rng(4)
+    mats = [bernoulli(rng, 20, 0.5) for _ in range(6)]
+    with pb.Server(0, slots=4, memory_budget=6000) as srv:
+        ts = [srv.submit(pb.PERM_REQ_EXACT_DENSE, m) for m in mats]
+        rs = [srv.wait(t) for t in ts]
+    spans = sorted((r["t_admit_ms"], r["t_done_ms"]) for r in rs)
+    for (a0, d0), (a1, d1) in zip(spans, spans[1:]):
+        assert a1 >= d0 - 1e-6

@@ -128,6 +128,27 @@ int perm_matrix_create_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype
 void perm_matrix_destroy(perm_ctx* ctx, perm_matrix* m);
 int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, perm_result* out);
 
+/* ---- allocation-free dense exact permanent ------------------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory themselves or have it allocated behind their back: code running
+ * inside another framework's memory pool, plugins in a host process that owns
+ * every device allocation, work issued while allocation is forbidden.  The
+ * caller passes a device-resident row-major n x n matrix `d_mat` and a device
+ * buffer `d_out` of two doubles that receives (hi, lo); everything else lives
+ * in one static device array (~96 KB per GPU that loads this library, held
+ * until the process exits).  No cudaMalloc or cudaFree is called.
+ *  - orders 1..64; larger orders return PERM_EUNSUPPORTED (the array holds one
+ *    64 x 64 operand and partials for 4096 CTAs), null pointers PERM_EINVAL;
+ *  - runs asynchronously on `stream` (a cudaStream_t, NULL = default stream);
+ *    a staging timeout turns d_out into NaN;
+ *  - the first call on a device does that device's one-time set-up (the
+ *    array's device address and the kernel's occupancy): make it before any
+ *    stream capture;
+ *  - all calls on a device share the array and it keeps the last call's
+ *    contents: calls that overlap on the GPU race, so order them on one stream
+ *    or synchronise between them. */
+int perm_exact_dense_noalloc(const double* d_mat, int n, double* d_out, void* stream);
+
 /* ---- batches: many exact permanents in one persistent launch -------------------- */
 /* A batch holds `count` row-major matrices concatenated in `values` (matrix i
  * has order orders[i], 1 <= order <= 40, and occupies orders[i]^2 doubles).

@@ -38,7 +38,7 @@ EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
-    "perm_exact_dense_resident",
+    "perm_exact_dense_resident", "perm_exact_dense_noalloc",
     "perm_batch_create", "perm_batch_run", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",

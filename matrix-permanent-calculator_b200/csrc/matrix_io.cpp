@@ -131,6 +131,44 @@ void compress_skip_order(double* a, int n, Compressed* out) {
   compress(a, n, out);
 }
 
+std::string grid_graph(int m, int n, HostMatrix* out) {
+  if (m < 1 || n < 1) return "grid sides must be positive";
+  if ((m & 1) && (n & 1)) return "one of the grid sides must be even";
+  // iterate over `rows` x `cols` cells with `cols` even
+  const int rows = (m % 2 == 0) ? n : m;
+  const int cols = (m % 2 == 0) ? m : n;
+  const int nov = m * n / 2;
+  if (nov > 4096) return "grid too large";
+  out->n = nov;
+  out->header_nnz = 0;
+  out->type = "int";
+  out->a.assign((size_t)nov * nov, 0.0);
+  const int half = cols / 2;
+  for (int i = 0; i < rows; i++) {
+    for (int j = 0; j < cols; j++) {
+      const int x = i * half + j / 2;
+      int nb[4], k = 0;
+      if (x - half >= 0) nb[k++] = x - half;  // cell above
+      if (x + half < nov) nb[k++] = x + half;  // cell below
+      if (j % 2 == 0) {  // horizontal neighbours share index x or x-1
+        if (j != 0) nb[k++] = x - 1;
+        nb[k++] = x;
+      } else {
+        nb[k++] = x;
+        if (j != cols - 1) nb[k++] = x + 1;
+      }
+      const bool black = ((i + j) & 1) == 0;  // black cells are rows, white cells columns
+      for (int t = 0; t < k; t++) {
+        if (black)
+          out->a[(size_t)x * nov + nb[t]] = 1.0;
+        else
+          out->a[(size_t)nb[t] * nov + x] = 1.0;
+      }
+    }
+  }
+  return "";
+}
+
 void compress_mode(int mode, double* a, int n, Compressed* out) {
   if (mode == 1)
     compress_sort_order(a, n, out);

@@ -51,4 +51,11 @@ void compress_skip_order(double* a, int n, Compressed* out);
 // Dispatch on the reference's -r value: 0 plain, 1 sortOrder, 2 skipOrder.
 void compress_mode(int mode, double* a, int n, Compressed* out);
 
+// Grid-graph input mode (util.h:403-520): the 0/1 bipartite adjacency
+// between the two colour classes of an m x n board, order nov = m*n/2, whose
+// permanent counts the board's domino tilings.  Cells are numbered
+// row-by-row, half a row per index along the even side.  Returns "" or an
+// error (both sides odd).
+std::string grid_graph(int m, int n, HostMatrix* out);
+
 }  // namespace perm

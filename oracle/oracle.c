@@ -725,3 +725,191 @@ void orc_scaling_trials(const double* a, int n, int y, int z, uint64_t seed, int
     out[q] = ok ? w_value(w) : 0.0;
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Sparse estimators for any order (CRS + CCS of the 0/1 pattern), restating */
+/* rasmussen_sparse (algo.h:172-268) and approximation_perman64_sparse       */
+/* (algo.h:366-470) / the GPU sparse kernels (gpu_approximation_sparse.cu:    */
+/* 198-452) with the device kernels' streams and FP64 order.  For n <= 64    */
+/* they equal orc_rasmussen_trials / orc_scaling_trials on the pattern.      */
+/* ------------------------------------------------------------------------ */
+static int bit_get(const uint64_t* b, int i) { return (int)((b[i >> 6] >> (i & 63)) & 1); }
+static void bit_set(uint64_t* b, int i) { b[i >> 6] |= 1ULL << (i & 63); }
+
+void orc_rasmussen_sparse_trials(const int* rptrs, const int* cols, const int* cptrs, const int* rows, int n,
+                                 uint64_t seed, int64_t t0, int64_t count, double* out) {
+#pragma omp parallel
+  {
+    int* cnt = (int*)malloc(sizeof(int) * (size_t)n);
+    uint64_t* colext = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)((n + 63) / 64));
+    uint64_t* rowext = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)((n + 63) / 64));
+#pragma omp for schedule(static)
+    for (int64_t q = 0; q < count; q++) {
+      const int64_t t = t0 + q;
+      memset(colext, 0, sizeof(uint64_t) * (size_t)((n + 63) / 64));
+      memset(rowext, 0, sizeof(uint64_t) * (size_t)((n + 63) / 64));
+      for (int r = 0; r < n; r++) cnt[r] = rptrs[r + 1] - rptrs[r];
+      wexp_t w = {0.5f, 1};
+      int ok = 1;
+      for (int step = 0; step < n; step++) {
+        int best = n + 1, row = -1;
+        for (int r = 0; r < n; r++)
+          if (!bit_get(rowext, r) && cnt[r] < best) {
+            best = cnt[r];
+            row = r;
+          }
+        if (best == 0) {
+          ok = 0;
+          break;
+        }
+        w_mul(&w, (float)best);
+        uint32_t rnd[4];
+        philox_step(seed, t, step, TAG_RASMUSSEN, rnd);
+        int idx = (int)(((uint64_t)rnd[0] * (uint64_t)best) >> 32);
+        int col = -1;
+        for (int p = rptrs[row]; p < rptrs[row + 1]; p++) {
+          int c = cols[p];
+          if (bit_get(colext, c)) continue;
+          if (idx == 0) {
+            col = c;
+            break;
+          }
+          idx--;
+        }
+        bit_set(colext, col);
+        bit_set(rowext, row);
+        for (int p = cptrs[col]; p < cptrs[col + 1]; p++) cnt[rows[p]]--;
+      }
+      out[q] = ok ? w_value(w) : 0.0;
+    }
+    free(cnt);
+    free(colext);
+    free(rowext);
+  }
+}
+
+void orc_scaling_sparse_trials(const int* rptrs, const int* cols, const int* cptrs, const int* rows, int n, int y,
+                               int z, uint64_t seed, int64_t t0, int64_t count, double* out) {
+#pragma omp parallel
+  {
+    int* cnt = (int*)malloc(sizeof(int) * (size_t)n);
+    double* dr = (double*)malloc(sizeof(double) * (size_t)n);
+    double* dc = (double*)malloc(sizeof(double) * (size_t)n);
+    const int W = (n + 63) / 64;
+    uint64_t* colext = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)W);
+    uint64_t* rowext = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)W);
+#pragma omp for schedule(static)
+    for (int64_t q = 0; q < count; q++) {
+      const int64_t t = t0 + q;
+      memset(colext, 0, sizeof(uint64_t) * (size_t)W);
+      memset(rowext, 0, sizeof(uint64_t) * (size_t)W);
+      for (int r = 0; r < n; r++) {
+        cnt[r] = rptrs[r + 1] - rptrs[r];
+        dr[r] = dc[r] = 1.0;
+      }
+      wexp_t w = {0.5f, 1};
+      int ok = 1;
+      for (int it = 0; it < n && ok; it++) {
+        int best = n + 1, row = -1;
+        for (int r = 0; r < n; r++)
+          if (!bit_get(rowext, r) && cnt[r] < best) {
+            best = cnt[r];
+            row = r;
+          }
+        if (it % y == 0) {
+          for (int k = 0; k < z && ok; k++) {
+            for (int j = 0; j < n && ok; j++) {
+              if (bit_get(colext, j)) continue;
+              double cs = 0;
+              for (int p = cptrs[j]; p < cptrs[j + 1]; p++)
+                if (!bit_get(rowext, rows[p])) cs = cs + dr[rows[p]];
+              if (cs == 0) ok = 0;
+              else dc[j] = 1.0 / cs;
+            }
+            for (int i = 0; i < n && ok; i++) {
+              if (bit_get(rowext, i)) continue;
+              double rs = 0;
+              for (int p = rptrs[i]; p < rptrs[i + 1]; p++)
+                if (!bit_get(colext, cols[p])) rs = rs + dc[cols[p]];
+              if (rs == 0) ok = 0;
+              else dr[i] = 1.0 / rs;
+            }
+          }
+          if (!ok) break;
+        }
+        double sum = 0;
+        for (int p = rptrs[row]; p < rptrs[row + 1]; p++)
+          if (!bit_get(colext, cols[p])) sum = sum + dr[row] * dc[cols[p]];
+        if (sum == 0) {
+          ok = 0;
+          break;
+        }
+        uint32_t rnd[4];
+        philox_step(seed, t, it, TAG_SCALING, rnd);
+        double u = ((double)(rnd[0] >> 5) * 67108864.0 + (double)(rnd[1] >> 6)) * (1.0 / 9007199254740992.0);
+        double target = u * sum, run = 0, sp = 0;
+        int col = -1;
+        for (int p = rptrs[row]; p < rptrs[row + 1]; p++) {
+          int c = cols[p];
+          if (bit_get(colext, c)) continue;
+          sp = dr[row] * dc[c];
+          run = run + sp;
+          col = c;
+          if (target < run) break;
+        }
+        w_mul(&w, (float)(sum / sp));
+        bit_set(colext, col);
+        bit_set(rowext, row);
+        for (int p = cptrs[col]; p < cptrs[col + 1]; p++) cnt[rows[p]]--;
+      }
+      out[q] = ok ? w_value(w) : 0.0;
+    }
+    free(cnt);
+    free(dr);
+    free(dc);
+    free(colext);
+    free(rowext);
+  }
+}
+
+/* Grid graph of an m x n board (util.h:403-520 restated): the bipartite
+ * adjacency of its two colour classes, whose permanent counts the board's
+ * domino tilings.  Writes the dense nov x nov 0/1 matrix (nov = m*n/2);
+ * returns nov, or -1 when both sides are odd. */
+int orc_grid_graph(int m, int n, double* mat, int cap) {
+  if ((m & 1) && (n & 1)) return -1;
+  int row, col;
+  if (m % 2 == 0) {
+    row = n;
+    col = m;
+  } else {
+    row = m;
+    col = n;
+  }
+  const int nov = m * n / 2;
+  if (nov > cap) return -2;
+  memset(mat, 0, sizeof(double) * (size_t)nov * nov);
+  for (int i = 0; i < row; i++)
+    for (int j = 0; j < col; j++) {
+      const int x = i * (col / 2) + j / 2;
+      const int black = ((i + j) & 1) == 0;
+      /* neighbours of cell (i, j) in the other colour class, indexed the same way */
+      int nb[4], k = 0;
+      if (x - col / 2 >= 0) nb[k++] = x - col / 2;
+      if (x + col / 2 < nov) nb[k++] = x + col / 2;
+      if (j % 2 == 0) {
+        if (j != 0) nb[k++] = x - 1;
+        nb[k++] = x;
+      } else {
+        nb[k++] = x;
+        if (j != col - 1) nb[k++] = x + 1;
+      }
+      for (int t = 0; t < k; t++) {
+        if (black)
+          mat[(size_t)x * nov + nb[t]] = 1.0;
+        else
+          mat[(size_t)nb[t] * nov + x] = 1.0;
+      }
+    }
+  return nov;
+}

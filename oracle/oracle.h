@@ -61,6 +61,14 @@ void orc_rasmussen_trials(const double* a, int n, uint64_t seed, int64_t t0, int
 void orc_scaling_trials(const double* a, int n, int y, int z, uint64_t seed, int64_t t0,
                         int64_t count, double* out);
 
+/* Sparse estimators for any order on CRS + CCS of the 0/1 pattern. */
+void orc_rasmussen_sparse_trials(const int* rptrs, const int* cols, const int* cptrs, const int* rows, int n,
+                                 uint64_t seed, int64_t t0, int64_t count, double* out);
+void orc_scaling_sparse_trials(const int* rptrs, const int* cols, const int* cptrs, const int* rows, int n, int y,
+                               int z, uint64_t seed, int64_t t0, int64_t count, double* out);
+/* Dense 0/1 grid-graph matrix of an m x n board (util.h:403-520). */
+int orc_grid_graph(int m, int n, double* mat, int cap);
+
 #ifdef __cplusplus
 }
 #endif

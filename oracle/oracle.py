@@ -57,6 +57,9 @@ class Oracle:
         L.orc_philox4x32_10.argtypes = [_P, _P, _P]
         L.orc_rasmussen_trials.argtypes = [_P, i, u64, i64, i64, _P]
         L.orc_scaling_trials.argtypes = [_P, i, i, i, u64, i64, i64, _P]
+        L.orc_rasmussen_sparse_trials.argtypes = [_P, _P, _P, _P, i, u64, i64, i64, _P]
+        L.orc_scaling_sparse_trials.argtypes = [_P, _P, _P, _P, i, i, i, u64, i64, i64, _P]
+        L.orc_grid_graph.argtypes = [i, i, _P, i]
 
     @staticmethod
     def _mat(a):
@@ -124,6 +127,41 @@ class Oracle:
         return out
 
 
+def _crs_ccs(a):
+    a = np.asarray(a) != 0
+    n = a.shape[0]
+    rptrs = np.concatenate([[0], np.cumsum(a.sum(1))]).astype(np.int32)
+    cols = np.nonzero(a)[1].astype(np.int32)
+    cptrs = np.concatenate([[0], np.cumsum(a.sum(0))]).astype(np.int32)
+    rows = np.nonzero(a.T)[1].astype(np.int32)
+    return n, rptrs, cols, cptrs, rows
+
+
+def _oracle_sparse(self, a, seed, t0, count, y=None, z=None):
+    n, rp, cl, cp, rw = _crs_ccs(a)
+    out = np.zeros(count)
+    if y is None:
+        self.lib.orc_rasmussen_sparse_trials(_ptr(rp), _ptr(cl), _ptr(cp), _ptr(rw), n, seed, t0, count, _ptr(out))
+    else:
+        self.lib.orc_scaling_sparse_trials(_ptr(rp), _ptr(cl), _ptr(cp), _ptr(rw), n, y, z, seed, t0, count,
+                                           _ptr(out))
+    return out
+
+
+def _grid_graph(self, m, n):
+    cap = max(1, m * n // 2)
+    out = np.zeros(cap * cap)
+    k = self.lib.orc_grid_graph(m, n, _ptr(out), cap)
+    if k < 0:
+        raise ValueError("both sides odd")
+    return out[: k * k].reshape(k, k).copy()
+
+
+Oracle.rasmussen_sparse_trials = lambda self, a, seed, t0, count: _oracle_sparse(self, a, seed, t0, count)
+Oracle.scaling_sparse_trials = lambda self, a, y, z, seed, t0, count: _oracle_sparse(self, a, seed, t0, count, y, z)
+Oracle.grid_graph = _grid_graph
+
+
 class Reference:
     """The reference's own functions (oracle/_ref/libperman_ref.so)."""
 
@@ -144,6 +182,7 @@ class Reference:
         L.ref_cpu_perman64_range_f64.argtypes = [_P, i, ll, ll, i]
         L.ref_read_matrix_f64.argtypes = [ctypes.c_char_p, i, _P, i, ctypes.POINTER(i)]
         L.ref_compress_f64.argtypes = [i, _P, i, i, _P, _P, _P, _P, _P, _P]
+        L.ref_grid_graph.argtypes = [i, i, _P, i]
 
     def parallel_perman64(self, a, threads: int) -> float:
         a = np.ascontiguousarray(a, dtype=np.float64)
@@ -180,6 +219,14 @@ class Reference:
         if n < 0:
             raise RuntimeError(f"reference reader failed ({n})")
         return buf[: n * n].reshape(n, n).copy()
+
+    def grid_graph(self, m: int, n: int) -> np.ndarray:
+        cap = max(1, m * n // 2)
+        out = np.zeros(cap * cap)
+        k = self.lib.ref_grid_graph(m, n, _ptr(out), cap)
+        if k < 0:
+            raise ValueError("both sides odd")
+        return out[: k * k].reshape(k, k).copy()
 
     def compress(self, mode: int, a) -> dict:
         a = np.array(a, dtype=np.float64, order="C", copy=True)

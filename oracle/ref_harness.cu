@@ -96,6 +96,25 @@ int ref_compress_f64(int mode, double* mat, int nov, int nnz, int* cptrs, int* r
   return compress_into<double>(mode, mat, nov, nnz, cptrs, rows, cvals, rptrs, cols, rvals);
 }
 
+// Grid-graph matrix (util.h:403-520) into a caller buffer of cap x cap
+// doubles; returns nov or <0.
+int ref_grid_graph(int m, int n, double* out, int cap) {
+  int *mat, *cptrs, *rows, *rptrs, *cols;
+  int nnz = gridGraph2compressed(m, n, mat, cptrs, rows, rptrs, cols);
+  if (nnz == -1) return -1;
+  const int nov = m * n / 2;
+  int rc = nov;
+  if (nov > cap) rc = -2;
+  else
+    for (int i = 0; i < nov * nov; i++) out[i] = mat[i];
+  delete[] mat;
+  delete[] cptrs;
+  delete[] rows;
+  delete[] rptrs;
+  delete[] cols;
+  return rc;
+}
+
 // ---- CPU exact (algo.h) ----------------------------------------------------
 double ref_parallel_perman64_f64(const double* mat, int nov, int threads) {   // algo.h:663
   double* m = copy_mat(mat, nov);

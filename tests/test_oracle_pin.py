@@ -141,3 +141,36 @@ def test_mc_oracle_is_unbiased(orc):
         v = fn()
         mean, se = v.mean(), v.std(ddof=1) / math.sqrt(len(v))
         assert abs(mean - exact) < 5 * se + 1e-12
+
+
+# domino tilings of small boards (OEIS A004003 for n x n; 2 x n are Fibonacci numbers)
+TILINGS = {(2, 2): 2, (2, 3): 3, (2, 4): 5, (3, 4): 11, (4, 4): 36, (4, 5): 95, (6, 6): 6728, (4, 6): 281,
+           (6, 5): 1183}
+
+
+def test_grid_graph_counts_domino_tilings(orc, pb):
+    for (m, n), t in TILINGS.items():
+        G = orc.grid_graph(m, n)
+        np.testing.assert_array_equal(G, pb.grid_graph(m, n))
+        assert orc.perm_exact_int(G)[0] == t, (m, n)
+
+
+def test_grid_graph_matches_reference(ref, pb):
+    for m, n in [(2, 2), (3, 4), (6, 5), (8, 8), (5, 6), (10, 12)]:
+        np.testing.assert_array_equal(pb.grid_graph(m, n), ref.grid_graph(m, n))
+    with pytest.raises(pb.PermError):
+        pb.grid_graph(3, 5)
+
+
+def test_sparse_estimator_restatement_equals_dense_on_patterns(orc):
+    rng = np.random.default_rng(12)
+    A = bernoulli(rng, 30, 0.4)
+    np.testing.assert_array_equal(orc.rasmussen_sparse_trials(A, 5, 0, 500), orc.rasmussen_trials(A, 5, 0, 500))
+    np.testing.assert_array_equal(orc.scaling_sparse_trials(A, 4, 5, 5, 0, 300), orc.scaling_trials(A, 4, 5, 5, 0, 300))
+
+
+def test_sparse_estimators_large_order_unbiased(orc):
+    G = orc.grid_graph(8, 8)  # order 32: 12988816 tilings
+    for v in (orc.rasmussen_sparse_trials(G, 3, 0, 20000), orc.scaling_sparse_trials(G, 4, 5, 3, 0, 5000)):
+        mean, se = v.mean(), v.std(ddof=1) / math.sqrt(len(v))
+        assert abs(mean - 12988816) < 5 * se

@@ -51,7 +51,8 @@ extern "C" {
 
 /* Limits of this build. */
 #define PERM_MAX_EXACT_N 64  /* Gray indices are 64-bit                 */
-#define PERM_MAX_MC_N 64     /* trial masks are 64-bit                  */
+#define PERM_MAX_MC_N 64     /* dense estimators: trial masks are 64-bit */
+#define PERM_MAX_MC_SPARSE_N 2047 /* sparse estimators: bitsets            */
 
 typedef struct perm_ctx perm_ctx;       /* one device, one stream, scratch */
 typedef struct perm_matrix perm_matrix; /* device-resident dense matrix    */
@@ -120,6 +121,12 @@ int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, const int* cols
  * PERM_KERNEL_DENSE_INT forces int32 X (PERM_EUNSUPPORTED if not exact). */
 int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard, int nshards,
                         perm_result* out);
+
+/* Measures, for orders n_lo..n_hi (within 8..40), whether the int32-X or the
+ * FP64-X kernel is faster on this device for integer inputs and makes variant
+ * 0 follow the measurement in this context.  choice_out receives
+ * n_hi - n_lo + 1 kernel ids. */
+int perm_dense_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* choice_out);
 
 /* Device-resident dense matrices: upload once, run many times (no host copy
  * inside perm_exact_dense_resident). */
@@ -214,6 +221,10 @@ int perm_approx_rasmussen(perm_ctx* ctx, const void* mat, int n, int dtype, int6
 int perm_approx_scaling(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trials,
                         int scale_intervals, int scale_times, uint64_t seed, double* trial_values,
                         perm_estimate* out);
+/* Sparse forms take the CRS of the pattern (columns ascending within a row),
+ * orders 1..2047 (the reference's sparse kernels stop at 672); above 64 they
+ * run a bitset kernel with the same streams and arithmetic, and the CCS
+ * arguments of the scaling form are rebuilt from the CRS. */
 int perm_approx_rasmussen_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
                                  int64_t trials, uint64_t seed, double* trial_values,
                                  perm_estimate* out);
@@ -223,6 +234,11 @@ int perm_approx_scaling_sparse(perm_ctx* ctx, int n, const int* rptrs, const int
                                double* trial_values, perm_estimate* out);
 
 /* ---- matrix input (host only; no device needed) ------------------------------ */
+/* The reference's grid-graph input mode (util.h:403-520): the dense 0/1
+ * adjacency between the two colour classes of an m x n board (order
+ * m*n/2, written row-major to out with room for cap_n^2 doubles); its
+ * permanent counts the board's domino tilings. */
+int perm_grid_graph(int m, int n, int cap_n, double* out, int* nov_out);
 /* Reads the reference text format ("n nnz type" then "i j value" lines,
  * util.h:344).  binary != 0 stores 1 for every entry (the -b flag).  `out`
  * must hold cap_n * cap_n doubles; the matrix is written row-major with

@@ -32,17 +32,18 @@ PERM_F64, PERM_F32, PERM_I32 = 0, 1, 2
 PERM_KERNEL_DENSE, PERM_KERNEL_SKIPPER, PERM_KERNEL_DENSE_INT = 1, 2, 3
 MAX_EXACT_N = 64
 MAX_MC_N = 64
+MAX_MC_SPARSE_N = 2047
 
 # Every extern "C" symbol declared in include/perman_b200.h.
 EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
-    "perm_exact_dense_resident", "perm_exact_dense_noalloc",
+    "perm_exact_dense_resident", "perm_exact_dense_noalloc", "perm_dense_autotune",
     "perm_batch_create", "perm_batch_run", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
-    "perm_approx_scaling_sparse", "perm_read_matrix", "perm_compress", "perm_fp64_peak",
+    "perm_approx_scaling_sparse", "perm_read_matrix", "perm_compress", "perm_grid_graph", "perm_fp64_peak",
     "gpu_perman64_xshared_coalescing_mshared_int", "gpu_perman64_xshared_coalescing_mshared_float",
     "gpu_perman64_xshared_coalescing_mshared_double",
     "gpu_perman64_xshared_coalescing_mshared_skipper_int",
@@ -126,12 +127,14 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_read_matrix": (i, [ctypes.c_char_p, i, i, _P, ctypes.POINTER(i), ctypes.POINTER(i),
                                  ctypes.c_char_p]),
         "perm_compress": (i, [i, _P, i, _P, _P, _P, _P, _P, _P]),
+        "perm_grid_graph": (i, [i, i, i, _P, ctypes.POINTER(i)]),
         "perm_fp64_peak": (i, [_P, ctypes.POINTER(d), ctypes.POINTER(d)]),
         "perm_batch_create": (i, [_P, i, _P, _P, ctypes.POINTER(_P)]),
         "perm_batch_run": (i, [_P, _P, _P, ctypes.POINTER(d)]),
         "perm_batch_destroy": (None, [_P, _P]),
         "perm_batch_exact": (i, [_P, i, _P, _P, _P, ctypes.POINTER(d)]),
         "perm_batch_autotune": (i, [_P, i, i, _P]),
+        "perm_dense_autotune": (i, [_P, i, i, _P]),
         "perm_server_create": (i, [i, i, ctypes.c_size_t, u64, ctypes.POINTER(_P)]),
         "perm_server_submit": (i, [_P, ctypes.POINTER(PermRequest), ctypes.POINTER(u64)]),
         "perm_server_wait": (i, [_P, u64, i, ctypes.POINTER(PermResponse)]),
@@ -327,6 +330,12 @@ class Engine:
         self._check(self.lib.perm_batch_autotune(self.ctx, n_lo, n_hi, _ptr(out)))
         return {n_lo + i: int(m) for i, m in enumerate(out)}
 
+    def dense_autotune(self, n_lo: int, n_hi: int) -> dict:
+        """Per order: which register kernel the automatic choice uses for integer inputs."""
+        out = np.zeros(n_hi - n_lo + 1, dtype=np.int32)
+        self._check(self.lib.perm_dense_autotune(self.ctx, n_lo, n_hi, _ptr(out)))
+        return {n_lo + i: int(k) for i, k in enumerate(out)}
+
     def fp64_peak(self) -> tuple[float, float]:
         ops, ms = ctypes.c_double(), ctypes.c_double()
         self._check(self.lib.perm_fp64_peak(self.ctx, ctypes.byref(ops), ctypes.byref(ms)))
@@ -435,6 +444,18 @@ def read_matrix(path, binary: bool = False, cap_n: int = 4096) -> tuple[np.ndarr
         raise PermError(rc, f"cannot read matrix file {path}")
     k = n.value
     return buf[: k * k].reshape(k, k).copy(), typ.value.decode(), nnz.value
+
+
+def grid_graph(m: int, n: int) -> np.ndarray:
+    """The reference's grid-graph matrix of an m x n board (util.h:403-520)."""
+    lib = load_library()
+    nov = m * n // 2
+    buf = np.zeros(max(nov, 1) ** 2, dtype=np.float64)
+    k = ctypes.c_int()
+    rc = lib.perm_grid_graph(m, n, max(nov, 1), _ptr(buf), ctypes.byref(k))
+    if rc != PERM_OK:
+        raise PermError(rc, f"no grid graph for a {m}x{n} board")
+    return buf[: k.value * k.value].reshape(k.value, k.value).copy()
 
 
 def compress(mode: int, mat) -> dict:

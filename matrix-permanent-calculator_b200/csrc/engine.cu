@@ -30,6 +30,7 @@
 #include "batch.h"
 #include "matrix_io.h"
 #include "mc.h"
+#include "mc_sparse.h"
 #include "perman_common.cuh"
 #include "ryser_dense.cuh"
 #include "ryser_dense_int.cuh"
@@ -113,6 +114,7 @@ struct perm_ctx {
   size_t d_trials_cap = 0;
   int dense_occ[8][PERM_MAX_EXACT_N + 1] = {};  // [0]: FP64-X, [G]: int32-X groups of G
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
+  int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: int32-X)
   int batch_occ = 0;
   std::string err;
   std::mutex mu;
@@ -174,6 +176,31 @@ static void pack_columns(const void* mat, int n, int dtype, double* dst) {
     for (int j = 0; j < n; j++) dst[(size_t)k * np + j] = elem(mat, dtype, (size_t)j * n + k);
     for (int j = n; j < np; j++) dst[(size_t)k * np + j] = 0.0;
   }
+}
+
+// Raise a kernel's dynamic shared-memory limit to the device's opt-in
+// maximum, once per (device, kernel).  The limit is a per-function setting
+// shared by every thread of the process: setting it to each call's own size
+// would let a concurrent call shrink it between another call's set and
+// launch, so it is only ever raised, to one fixed value.
+static int allow_smem(perm_ctx* ctx, const void* fn, size_t need) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<int, const void*>, size_t>> done;
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& d : done)
+    if (d.first.first == ctx->device && d.first.second == fn) {
+      if (need > d.second) return fail(ctx, PERM_EUNSUPPORTED, "kernel needs %zu B of shared memory (max %zu)", need, d.second);
+      return PERM_OK;
+    }
+  int optin = 0;
+  CU(ctx, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+  cudaFuncAttributes fa;
+  CU(ctx, cudaFuncGetAttributes(&fa, fn));
+  const size_t maxdyn = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+  CU(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxdyn));
+  done.push_back({{ctx->device, fn}, maxdyn});
+  if (need > maxdyn) return fail(ctx, PERM_EUNSUPPORTED, "kernel needs %zu B of shared memory (max %zu)", need, maxdyn);
+  return PERM_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -326,7 +353,8 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
   std::vector<double> a((size_t)n * n);
   for (size_t i = 0; i < a.size(); i++) a[i] = elem(mat, dtype, i);
   op->n = n;
-  int G = (variant == PERM_KERNEL_DENSE) ? 0 : int_group_size(a, n);
+  const bool prefer_fp64 = variant == 0 && n <= PERM_MAX_EXACT_N && ctx->dense_pref[n] == PERM_KERNEL_DENSE;
+  int G = (variant == PERM_KERNEL_DENSE || prefer_fp64) ? 0 : int_group_size(a, n);
   if (variant == PERM_KERNEL_DENSE_INT && G == 0)
     return fail(ctx, PERM_EUNSUPPORTED,
                 "int32-X kernel needs an integer matrix of order >= 8 whose row products fit in int32");
@@ -582,6 +610,37 @@ extern "C" int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, pe
   return dense_collect(ctx, m->op, p, out);
 }
 
+// Autotuner for the automatic dense-kernel choice on integer inputs: for each
+// order in [n_lo, n_hi] (8..40) time the int32-X and FP64-X kernels on a
+// seeded binary matrix and keep the faster one in the context.  choice_out
+// (n_hi - n_lo + 1 ints) receives PERM_KERNEL_DENSE_INT or PERM_KERNEL_DENSE.
+extern "C" int perm_dense_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* choice_out) {
+  if (!ctx) return PERM_EINVAL;
+  if (n_lo < 8 || n_hi > 40 || n_lo > n_hi) return fail(ctx, PERM_EINVAL, "orders [%d, %d] outside [8, 40]", n_lo, n_hi);
+  uint64_t state = 0xD1B54A32D192ED03ull;
+  for (int n = n_lo; n <= n_hi; n++) {
+    std::vector<double> a((size_t)n * n);
+    for (double& v : a) {
+      state = state * 6364136223846793005ull + 1442695040888963407ull;
+      v = (state >> 63) ? 1.0 : 0.0;
+    }
+    for (int j = 0; j < n; j++) a[(size_t)j * n + j] = 1.0;  // no empty row or column
+    double best_ms[2] = {1e30, 1e30};
+    const int variants[2] = {PERM_KERNEL_DENSE_INT, PERM_KERNEL_DENSE};
+    for (int v = 0; v < 2; v++) {
+      for (int rep = 0; rep < 3; rep++) {
+        perm_result r;
+        int rc = perm_exact_dense_ex(ctx, a.data(), n, PERM_F64, variants[v], 0, 1, &r);
+        if (rc) return rc;
+        if (rep) best_ms[v] = std::min(best_ms[v], r.kernel_ms);
+      }
+    }
+    ctx->dense_pref[n] = best_ms[1] < best_ms[0] ? PERM_KERNEL_DENSE : PERM_KERNEL_DENSE_INT;
+    if (choice_out) choice_out[n - n_lo] = ctx->dense_pref[n];
+  }
+  return PERM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // SkipPer
 // ---------------------------------------------------------------------------
@@ -628,7 +687,7 @@ static int run_skipper(perm_ctx* ctx, int n, const int* rptrs, const int* cols, 
   const int block = 128;
   const size_t smem = skipper_smem_bytes(a.pack_bytes, n, block);
   if (smem > 227 * 1024) return fail(ctx, PERM_EUNSUPPORTED, "SkipPer operand needs %zu B of shared memory", smem);
-  CU(ctx, cudaFuncSetAttribute(skipper_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if ((rc = allow_smem(ctx, (const void*)skipper_kernel, smem))) return rc;
   int occ = 0;
   CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, skipper_kernel, block, smem));
   occ = std::max(occ, 1);
@@ -776,7 +835,7 @@ static int mc_run(perm_ctx* ctx, const std::vector<uint64_t>& rowmask, const std
   }
   const size_t smem = mc_smem_bytes(a.pack_bytes, scaling);
   const void* fn = scaling ? (const void*)scaling_kernel : (const void*)rasmussen_kernel;
-  CU(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if ((rc = allow_smem(ctx, fn, smem))) return rc;
   int occ = 0;
   CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kMcBlock, smem));
   occ = std::max(occ, 1);
@@ -841,22 +900,124 @@ static int mc_dense(perm_ctx* ctx, const void* mat, int n, int dtype, bool scali
   return mc_run(ctx, mask, &dense, n, scaling, trials, y, z, seed, tv, out);
 }
 
+// Orders above 64: bitset kernel on the packed CRS + CCS of the pattern.
+static int mc_sparse_large(perm_ctx* ctx, int n, const int* rptrs, const int* cols, bool scaling, int64_t trials,
+                           int y, int z, uint64_t seed, double* tv, perm_estimate* out) {
+  if (trials < 1) return fail(ctx, PERM_EINVAL, "trials must be >= 1 (got %lld)", (long long)trials);
+  if (scaling && (y < 1 || z < 0)) return fail(ctx, PERM_EINVAL, "scale interval must be >= 1 and scale times >= 0");
+  const int nnz = rptrs[n];
+  // CCS rebuilt from the CRS so that both lists are in ascending order
+  std::vector<int> cptrs(n + 1, 0), rows(std::max(nnz, 1));
+  for (int p = 0; p < nnz; p++) cptrs[cols[p] + 1]++;
+  for (int j = 0; j < n; j++) cptrs[j + 1] += cptrs[j];
+  std::vector<int> fill(cptrs.begin(), cptrs.end() - 1);
+  for (int i = 0; i < n; i++)
+    for (int p = rptrs[i]; p < rptrs[i + 1]; p++) rows[fill[cols[p]]++] = i;
+  McSparseArgs a;
+  a.n = n;
+  a.scaling = scaling ? 1 : 0;
+  a.y = y;
+  a.z = z;
+  a.ptr_ints = (n + 1 + 3) & ~3;
+  a.idx_ints = (nnz + 3) & ~3;
+  a.pack_bytes = (uint32_t)(sizeof(int) * (2 * (size_t)a.ptr_ints + 2 * (size_t)a.idx_ints));
+  const size_t smem = mc_sparse_smem_bytes(a.pack_bytes, n, a.scaling);
+  if (smem > 227 * 1024)
+    return fail(ctx, PERM_EUNSUPPORTED, "order %d with %d nonzeros needs %zu B of shared memory", n, nnz, smem);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  int rc = ensure_stage(ctx, a.pack_bytes);
+  if (rc) return rc;
+  int* h = reinterpret_cast<int*>(ctx->h_stage);
+  memset(h, 0, a.pack_bytes);
+  memcpy(h, rptrs, sizeof(int) * (n + 1));
+  memcpy(h + a.ptr_ints, cptrs.data(), sizeof(int) * (n + 1));
+  memcpy(h + 2 * a.ptr_ints, cols, sizeof(int) * nnz);
+  memcpy(h + 2 * a.ptr_ints + a.idx_ints, rows.data(), sizeof(int) * nnz);
+  if ((rc = allow_smem(ctx, (const void*)mc_sparse_kernel, smem))) return rc;
+  int occ = 0;
+  CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mc_sparse_kernel, kMcSparseBlock, smem));
+  occ = std::max(occ, 1);
+  const int wpb = kMcSparseBlock / 32;
+  int grid = (int)std::min<uint64_t>(std::min(kMaxBlocks, ctx->num_sms * occ), ((uint64_t)trials + wpb - 1) / wpb);
+  grid = std::max(grid, 1);
+  if (tv && (size_t)trials > ctx->d_trials_cap) {
+    cudaFree(ctx->d_trials);
+    ctx->d_trials = nullptr;
+    ctx->d_trials_cap = 0;
+    CU(ctx, cudaMalloc(&ctx->d_trials, sizeof(double) * trials));
+    ctx->d_trials_cap = trials;
+  }
+  a.pack = ctx->d_stage;
+  a.trials = trials;
+  a.trial0 = 0;
+  a.seed = seed;
+  a.trial_out = tv ? ctx->d_trials : nullptr;
+  a.partials = reinterpret_cast<double*>(ctx->partials);
+  a.ticket = ctx->ticket;
+  a.out = ctx->d_out;
+  a.err = ctx->d_err;
+  CU(ctx, cudaMemcpyAsync(ctx->d_stage, h, a.pack_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  void* kargs[] = {&a};
+  CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  CU(ctx, cudaLaunchKernel((const void*)mc_sparse_kernel, dim3(grid), dim3(kMcSparseBlock), kargs, smem, ctx->stream));
+  CU(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  if (tv) CU(ctx, cudaMemcpyAsync(tv, ctx->d_trials, sizeof(double) * trials, cudaMemcpyDeviceToHost, ctx->stream));
+  rc = finish_and_read(ctx, 3);
+  if (rc) return rc;
+  float ms = 0;
+  CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  const double T = (double)trials, sum = ctx->h_out[0], sq = ctx->h_out[1];
+  out->trials = T;
+  out->sum = sum;
+  out->sum_sq = sq;
+  out->zero_trials = ctx->h_out[2];
+  out->mean = sum / T;
+  double var = T > 1 ? (sq - sum * out->mean) / (T - 1) : 0.0;
+  if (!(var > 0)) var = 0;
+  out->std_error = std::sqrt(var / T);
+  out->kernel_ms = ms;
+  return PERM_OK;
+}
+
 static int mc_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols, bool scaling, int64_t trials,
                      int y, int z, uint64_t seed, double* tv, perm_estimate* out) {
   if (!ctx) return PERM_EINVAL;
   if (!rptrs || !cols || !out) return fail(ctx, PERM_EINVAL, "null CRS or result pointer");
-  if (n < 1 || n > PERM_MAX_MC_N) return fail(ctx, PERM_EUNSUPPORTED, "order %d outside [1, %d]", n, PERM_MAX_MC_N);
-  std::vector<uint64_t> mask(n, 0);
-  std::vector<double> pattern((size_t)n * n, 0.0);
+  if (n < 1 || n > kMcSparseMaxOrder)
+    return fail(ctx, PERM_EUNSUPPORTED, "order %d outside [1, %d]", n, kMcSparseMaxOrder);
+  if (rptrs[0] != 0) return fail(ctx, PERM_EINVAL, "rptrs[0] must be 0");
   for (int i = 0; i < n; i++) {
     if (rptrs[i + 1] < rptrs[i]) return fail(ctx, PERM_EINVAL, "rptrs must be non-decreasing");
     for (int p = rptrs[i]; p < rptrs[i + 1]; p++) {
       if (cols[p] < 0 || cols[p] >= n) return fail(ctx, PERM_EINVAL, "column index out of range");
+      if (p > rptrs[i] && cols[p] <= cols[p - 1]) return fail(ctx, PERM_EINVAL, "CRS columns must ascend within a row");
+    }
+  }
+  if (n > PERM_MAX_MC_N) return mc_sparse_large(ctx, n, rptrs, cols, scaling, trials, y, z, seed, tv, out);
+  std::vector<uint64_t> mask(n, 0);
+  std::vector<double> pattern((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++)
+    for (int p = rptrs[i]; p < rptrs[i + 1]; p++) {
       mask[i] |= 1ull << cols[p];
       pattern[(size_t)i * n + cols[p]] = 1.0;  // the sparse estimators use the pattern only
     }
-  }
   return mc_run(ctx, mask, &pattern, n, scaling, trials, y, z, seed, tv, out);
+}
+
+// Grid-graph input (util.h:403-520): dense 0/1 matrix of an m x n board.
+extern "C" int perm_grid_graph(int m, int n, int cap_n, double* out, int* nov_out) {
+  if (!out || !nov_out) return PERM_EINVAL;
+  HostMatrix g;
+  std::string err = grid_graph(m, n, &g);
+  if (!err.empty()) {
+    fprintf(stderr, "perm_grid_graph: %s\n", err.c_str());
+    return PERM_EINVAL;
+  }
+  if (g.n > cap_n) return PERM_EUNSUPPORTED;
+  std::copy(g.a.begin(), g.a.end(), out);
+  *nov_out = g.n;
+  return PERM_OK;
 }
 
 extern "C" int perm_approx_rasmussen(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trials,
@@ -975,7 +1136,10 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
   BT(cudaMemcpy(b->d_mats, q.data(), sizeof(BatchMatrix) * count, cudaMemcpyHostToDevice));
   BT(cudaMemset(b->d_mat_done, 0, sizeof(unsigned) * count));
   if (!ctx->batch_occ) {
-    BT(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem_bytes()));
+    if (int rc2 = allow_smem(ctx, (const void*)batch_kernel, batch_smem_bytes())) {
+      batch_free(b);
+      return rc2;
+    }
     int occ = 0;
     BT(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, kBatchBlock, batch_smem_bytes()));
     ctx->batch_occ = std::max(occ, 1);

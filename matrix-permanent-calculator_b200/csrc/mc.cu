@@ -171,45 +171,47 @@ __global__ void __launch_bounds__(kMcBlock) scaling_kernel(McArgs a) {
         const unsigned key = min_row_key(rowmask, n, colext, rowext, lane);
         const int row = (int)(key & 0xffu);
         if (it % a.y == 0) {
+          // only the rows/columns still in the submatrix take part; both
+          // passes walk them in ascending order (the CPU restatement's order)
+          const uint64_t full = n == 64 ? ~0ull : ((1ull << n) - 1);
+          const uint64_t rows_left = ~rowext & full, cols_left = ~colext & full;
+          const int j0 = lane, j1 = lane + 32;
+          const bool c0 = (cols_left >> j0) & 1, c1 = j1 < 64 && ((cols_left >> j1) & 1);
+          const bool r0 = (rows_left >> j0) & 1, r1 = j1 < 64 && ((rows_left >> j1) & 1);
           for (int k = 0; k < a.z; k++) {
             // column pass: lane owns columns lane, lane + 32
-            bool fail = false;
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-              const int j = lane + 32 * h;
-              if (j < n && !((colext >> j) & 1)) {
-                double cs = 0.0;
-                for (int i = 0; i < n; i++)
-                  if (!((rowext >> i) & 1)) cs = __dadd_rn(cs, __dmul_rn(dr[i], A[i * np + j]));
-                if (cs == 0.0)
-                  fail = true;
-                else
-                  dc[j] = __drcp_rn(cs);
-              }
+            double cs0 = 0.0, cs1 = 0.0;
+            for (uint64_t m = rows_left; m; m &= m - 1) {
+              const int i = __ffsll((long long)m) - 1;
+              const double d = dr[i];
+              const double* Ai = A + i * np;
+              if (c0) cs0 = __dadd_rn(cs0, __dmul_rn(d, Ai[j0]));
+              if (c1) cs1 = __dadd_rn(cs1, __dmul_rn(d, Ai[j1]));
             }
+            bool fail = (c0 && cs0 == 0.0) || (c1 && cs1 == 0.0);
             if (__any_sync(0xffffffffu, fail)) {
               ok = false;
               break;
             }
+            if (c0) dc[j0] = __drcp_rn(cs0);
+            if (c1) dc[j1] = __drcp_rn(cs1);
             __syncwarp();
             // row pass: lane owns rows lane, lane + 32 (reads the transposed copy)
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-              const int i = lane + 32 * h;
-              if (i < n && !((rowext >> i) & 1)) {
-                double rs = 0.0;
-                for (int j = 0; j < n; j++)
-                  if (!((colext >> j) & 1)) rs = __dadd_rn(rs, __dmul_rn(AT[j * np + i], dc[j]));
-                if (rs == 0.0)
-                  fail = true;
-                else
-                  dr[i] = __drcp_rn(rs);
-              }
+            double rs0 = 0.0, rs1 = 0.0;
+            for (uint64_t m = cols_left; m; m &= m - 1) {
+              const int j = __ffsll((long long)m) - 1;
+              const double d = dc[j];
+              const double* ATj = AT + j * np;
+              if (r0) rs0 = __dadd_rn(rs0, __dmul_rn(ATj[j0], d));
+              if (r1) rs1 = __dadd_rn(rs1, __dmul_rn(ATj[j1], d));
             }
+            fail = (r0 && rs0 == 0.0) || (r1 && rs1 == 0.0);
             if (__any_sync(0xffffffffu, fail)) {
               ok = false;
               break;
             }
+            if (r0) dr[j0] = __drcp_rn(rs0);
+            if (r1) dr[j1] = __drcp_rn(rs1);
             __syncwarp();
           }
           if (!ok) break;

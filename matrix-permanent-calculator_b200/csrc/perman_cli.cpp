@@ -13,8 +13,9 @@
 //   -t N                accepted, unused (host threads of the CPU algorithms)
 //   -c                  CPU algorithms: not part of this engine -> error
 //   --seed N            Monte-Carlo seed (default: time, like the reference)
-// The reference's grid-graph generator (-i, with -m/-n as grid sizes) is not
-// built; -n is accepted and ignored.
+//   -i -m M -n N        grid-graph mode (main.cu:250-313): approximate
+//                       permanent of the M x N board's grid graph (domino
+//                       tilings); with -i, -m and -n are the board sides.
 #include <getopt.h>
 
 #include <algorithm>
@@ -33,7 +34,8 @@
 namespace {
 
 struct Options {
-  std::string file;
+  std::string file, m_arg;
+  int gridn = 36;
   bool binary = false, sparse = false, approx = false, cpu = false, gpu = false, grid = false;
   int algo = 1, threads = 16, gpu_num = 2, pre = 0;
   int times = 100000, y = 4, z = 5;
@@ -104,6 +106,64 @@ int multi_gpu_dense(const std::vector<double>& a, int n, int gpus, perm_result* 
   return 0;
 }
 
+// Grid-graph mode: approximate algorithms only, on the board's sparse pattern
+// (main.cu:250-313 calls the sparse GPU estimators with grid_graph = true).
+int run_grid(const Options& o) {
+  const int gm = o.m_arg.empty() ? 36 : atoi(o.m_arg.c_str());
+  const int gn = o.gridn;
+  if (o.cpu && !o.gpu) return usage("perman: the CPU algorithms (-c) are not part of the B200 engine; run with -g");
+  const int nov = gm * gn / 2;
+  if (gm < 1 || gn < 1 || nov > PERM_MAX_MC_SPARSE_N) return usage("perman: grid sides out of range");
+  std::vector<double> a((size_t)nov * nov);
+  int k = 0;
+  if (perm_grid_graph(gm, gn, nov, a.data(), &k) != PERM_OK) {
+    printf("one of the grid dimensions should be positive.");
+    return 0;
+  }
+  std::vector<int> rptrs(nov + 1, 0), cols, cptrs(nov + 1, 0), rows;
+  for (int i = 0; i < nov; i++) {
+    for (int j = 0; j < nov; j++)
+      if (a[(size_t)i * nov + j] != 0) cols.push_back(j);
+    rptrs[i + 1] = (int)cols.size();
+  }
+  for (int j = 0; j < nov; j++) {
+    for (int i = 0; i < nov; i++)
+      if (a[(size_t)i * nov + j] != 0) rows.push_back(i);
+    cptrs[j + 1] = (int)rows.size();
+  }
+  static const char* names[] = {nullptr, "gpu_perman64_rasmussen_sparse", "gpu_perman64_approximation_sparse",
+                                "gpu_perman64_rasmussen_multigpucpu_chunks",
+                                "gpu_perman64_approximation_multigpucpu_chunks_sparse"};
+  if (o.algo < 1 || o.algo > 4) {
+    printf("Unknown Algorithm ID\n");
+    return 0;
+  }
+  perm_ctx* ctx = nullptr;
+  const double t0 = now();
+  int rc = perm_ctx_create(0, &ctx);
+  if (rc != PERM_OK) {
+    fprintf(stderr, "perman: cannot use a B200: %s\n", perm_status_string(rc));
+    return 3;
+  }
+  perm_estimate e;
+  const bool scaling = o.algo == 2 || o.algo == 4;
+  rc = scaling ? perm_approx_scaling_sparse(ctx, nov, rptrs.data(), cols.data(), cptrs.data(), rows.data(), o.times,
+                                            o.y, o.z, (uint64_t)o.seed, nullptr, &e)
+               : perm_approx_rasmussen_sparse(ctx, nov, rptrs.data(), cols.data(), o.times, (uint64_t)o.seed,
+                                              nullptr, &e);
+  int status = 0;
+  if (rc != PERM_OK) {
+    status = die(ctx, rc);
+  } else {
+    printf("kernel in %.6f\n", e.kernel_ms * 1e-3);
+    printf("number of zeros: %.0f\n", e.zero_trials);
+    printf("std error: %.17g (%.0f trials, seed %lld)\n", e.std_error, e.trials, o.seed);
+    print_result(names[o.algo], e.mean, now() - t0);
+  }
+  perm_ctx_destroy(ctx);
+  return status;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -131,7 +191,7 @@ int main(int argc, char** argv) {
       case 'r': o.pre = atoi(optarg); break;
       case 't': o.threads = atoi(optarg); break;
       case 'f': o.file = optarg; break;
-      case 'm': o.file = optarg; break;
+      case 'm': o.m_arg = optarg; break;
       case 'g': o.gpu = true; break;
       case 'd': o.gpu_num = atoi(optarg); break;
       case 'c': o.cpu = true; break;
@@ -141,13 +201,15 @@ int main(int argc, char** argv) {
       case 'y': o.y = atoi(optarg); break;
       case 'z': o.z = atoi(optarg); break;
       case 'i': o.grid = true; break;
-      case 'n': break;
+      case 'n': o.gridn = atoi(optarg); break;
       case 'S': o.seed = atoll(optarg); break;
       default: return 1;
     }
   }
   for (int i = optind; i < argc; i++) printf("Non-option argument %s\n", argv[i]);
-  if (o.grid) return usage("perman: grid-graph mode (-i) is not part of the B200 engine");
+  if (o.seed < 0) o.seed = (long long)time(nullptr);
+  if (!o.grid && o.file.empty()) o.file = o.m_arg;
+  if (o.grid) return run_grid(o);
   if (o.file.empty()) return usage("Option -f (or -m) is a required argument.");
   if (o.cpu && !o.gpu)
     return usage("perman: the CPU algorithms (-c) are not part of the B200 engine; run with -g");

@@ -28,7 +28,9 @@ def test_batch_matches_single_matrix_kernel(engine, pb):
     assert ms > 0
     for m, v in zip(mats, vals):
         want = engine.exact_dense(m, variant=pb.PERM_KERNEL_DENSE).value
-        assert rel_err(v, want) < 1e-10, (m.shape, v, want)
+        # a binary matrix without a perfect matching has permanent 0; both
+        # kernels then return rounding noise of order 1e-17
+        assert rel_err(v, want) < 1e-10 or abs(v - want) < 1e-12, (m.shape, v, want)
 
 
 def test_batch_vs_oracle_and_golden(engine, orc, golden):

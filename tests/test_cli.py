@@ -38,9 +38,9 @@ def test_cpu_algorithms_rejected(pb, tmp_path):
     assert r.returncode != 0 and "CPU" in r.stderr
 
 
-def test_grid_mode_rejected(pb):
-    r = run(pb, "-i", "-m", "4", "-n", "4")
-    assert r.returncode != 0 and "grid" in r.stderr
+def test_grid_mode_odd_board(pb):
+    r = run(pb, "-i", "-m", "3", "-n", "5")
+    assert r.returncode == 0 and "should be positive" in r.stdout
 
 
 def test_unreadable_file(pb, tmp_path):
@@ -100,3 +100,15 @@ def test_multi_gpu_id_on_available_devices(pb, orc, tmp_path):
     assert r.returncode == 0, r.stderr
     _, v = result_value(r.stdout)
     assert rel_err(v, orc.perm_exact_int(A)[0]) < 1e-13
+
+
+@pytest.mark.gpu
+def test_grid_mode_estimates_tilings(pb):
+    # 8 x 8 board: 12988816 domino tilings
+    r = run(pb, "-i", "-m", "8", "-n", "8", "-p1", "-x", "200000", "--seed", "5")
+    assert r.returncode == 0, r.stderr
+    name, v = result_value(r.stdout)
+    se = float(re.search(r"std error: (\S+)", r.stdout).group(1))
+    assert name == "gpu_perman64_rasmussen_sparse" and abs(v - 12988816) < 5 * se
+    r = run(pb, "-i", "-m", "20", "-n", "10", "-p2", "-x", "20000")
+    assert r.returncode == 0, r.stderr

@@ -189,3 +189,13 @@ def test_int_kernel_shards(engine, pb):
     whole = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT).value
     parts = [engine.exact_dense_shard(A, s, 5, variant=pb.PERM_KERNEL_DENSE_INT) for s in range(5)]
     assert rel_err(sum(p.hi + p.lo for p in parts), whole) < 1e-12
+
+
+def test_dense_autotune_sets_the_automatic_choice(pb):
+    with pb.Engine(0) as eng:
+        table = eng.dense_autotune(8, 22)
+        assert set(table.values()) <= {pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_INT}
+        rng = np.random.default_rng(1)
+        for n, k in table.items():
+            A = bernoulli(rng, n, 0.5)
+            assert eng.exact_dense(A).kernel == k

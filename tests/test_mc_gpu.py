@@ -100,3 +100,45 @@ def test_reference_signature_mc(pb):
     assert pb.gpu_perman64_rasmussen(A, 8, 1000) == math.factorial(8)
     v = pb.gpu_perman64_approximation(A, 8, 1000, 4, 5)
     assert abs(v - math.factorial(8)) < 1e-6 * math.factorial(8)
+
+
+# ---- sparse estimators above order 64 (bitset kernel) -------------------------------
+
+def _crs(pb, A):
+    c = pb.compress(0, A)
+    return c["n"], c["rptrs"], c["cols"], c["cptrs"], c["rows"]
+
+
+@pytest.mark.parametrize("board", [(10, 14), (18, 20), (36, 36)])
+def test_grid_graph_trials_bit_identical_above_64(engine, orc, pb, board):
+    G = pb.grid_graph(*board)
+    n, rp, cl, cp, rw = _crs(pb, G)
+    assert n > 64
+    e = engine.rasmussen_sparse(n, rp, cl, 600, seed=4, keep_trials=True)
+    np.testing.assert_array_equal(e.trial_values, orc.rasmussen_sparse_trials(G, 4, 0, 600))
+    s = engine.scaling_sparse(n, rp, cl, cp, rw, 100, 4, 5, seed=6, keep_trials=True)
+    np.testing.assert_array_equal(s.trial_values, orc.scaling_sparse_trials(G, 4, 5, 6, 0, 100))
+
+
+def test_random_sparse_above_64(engine, orc, pb):
+    rng = np.random.default_rng(88)
+    A = bernoulli(rng, 150, 0.05)
+    n, rp, cl, cp, rw = _crs(pb, A)
+    e = engine.rasmussen_sparse(n, rp, cl, 500, seed=9, keep_trials=True)
+    np.testing.assert_array_equal(e.trial_values, orc.rasmussen_sparse_trials(A, 9, 0, 500))
+    s = engine.scaling_sparse(n, rp, cl, cp, rw, 80, 2, 3, seed=9, keep_trials=True)
+    np.testing.assert_array_equal(s.trial_values, orc.scaling_sparse_trials(A, 2, 3, 9, 0, 80))
+
+
+def test_estimators_agree_above_64(engine, pb):
+    G = pb.grid_graph(10, 14)
+    n, rp, cl, cp, rw = _crs(pb, G)
+    r = engine.rasmussen_sparse(n, rp, cl, 400000, seed=1)
+    s = engine.scaling_sparse(n, rp, cl, cp, rw, 100000, 4, 5, seed=2)
+    assert abs(r.mean - s.mean) < 5 * math.hypot(r.std_error, s.std_error)
+
+
+def test_large_order_limits(engine, pb):
+    rp = np.zeros(2049, np.int32)
+    with pytest.raises(pb.PermError):
+        engine.rasmussen_sparse(2048, rp, np.zeros(0, np.int32), 10)

@@ -48,6 +48,7 @@ extern "C" {
 #define PERM_KERNEL_DENSE 1   /* register-X Gray-code Ryser                 */
 #define PERM_KERNEL_SKIPPER 2 /* SkipPer on CRS/CCS                          */
 #define PERM_KERNEL_DENSE_INT 3 /* int32-X Gray-code Ryser (integer matrices) */
+#define PERM_KERNEL_DENSE_DD 4  /* double-double Gray-code Ryser (orders <= 40) */
 
 /* Limits of this build. */
 #define PERM_MAX_EXACT_N 64  /* Gray indices are 64-bit                 */
@@ -65,6 +66,8 @@ typedef struct {
   double kernel_ms;   /* device time of the compute kernel (CUDA events)    */
   int kernel;         /* PERM_KERNEL_*                                      */
   int n;
+  double abs_term_sum;       /* estimate of sum_i |term(i)| (cancellation scale) */
+  double rel_error_estimate; /* estimated relative error of value (0: not estimated) */
 } perm_result;
 
 typedef struct {
@@ -121,6 +124,12 @@ int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, const int* cols
  * PERM_KERNEL_DENSE_INT forces int32 X (PERM_EUNSUPPORTED if not exact). */
 int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard, int nshards,
                         perm_result* out);
+/* Whole-walk dense results carry rel_error_estimate (cancellation estimated
+ * from 65536 sampled Gray terms).  With variant 0, a result whose estimate
+ * exceeds the context's target (default 1e-10; <= 0 disables the rerun) is
+ * recomputed by the double-double kernel (orders <= 40).  PERM_KERNEL_DENSE_DD
+ * forces that kernel. */
+int perm_ctx_set_rel_target(perm_ctx* ctx, double rel_target);
 
 /* Measures, for orders n_lo..n_hi (within 8..40), whether the int32-X or the
  * FP64-X kernel is faster on this device for integer inputs and makes variant

@@ -29,7 +29,7 @@ CLI_PATH = PKG_DIR / "bin" / "perman"
 
 PERM_OK, PERM_EINVAL, PERM_ECUDA, PERM_ENOMEM, PERM_EUNSUPPORTED, PERM_ETIMEOUT, PERM_EIO = 0, -1, -2, -3, -4, -5, -6
 PERM_F64, PERM_F32, PERM_I32 = 0, 1, 2
-PERM_KERNEL_DENSE, PERM_KERNEL_SKIPPER, PERM_KERNEL_DENSE_INT = 1, 2, 3
+PERM_KERNEL_DENSE, PERM_KERNEL_SKIPPER, PERM_KERNEL_DENSE_INT, PERM_KERNEL_DENSE_DD = 1, 2, 3, 4
 MAX_EXACT_N = 64
 MAX_MC_N = 64
 MAX_MC_SPARSE_N = 2047
@@ -39,7 +39,7 @@ EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
-    "perm_exact_dense_resident", "perm_exact_dense_noalloc", "perm_dense_autotune",
+    "perm_exact_dense_resident", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target",
     "perm_batch_create", "perm_batch_run", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
@@ -67,7 +67,8 @@ class PermError(RuntimeError):
 class PermResult(ctypes.Structure):
     _fields_ = [("value", ctypes.c_double), ("hi", ctypes.c_double), ("lo", ctypes.c_double),
                 ("steps", ctypes.c_double), ("total_steps", ctypes.c_double),
-                ("kernel_ms", ctypes.c_double), ("kernel", ctypes.c_int), ("n", ctypes.c_int)]
+                ("kernel_ms", ctypes.c_double), ("kernel", ctypes.c_int), ("n", ctypes.c_int),
+                ("abs_term_sum", ctypes.c_double), ("rel_error_estimate", ctypes.c_double)]
 
 
 class PermRequest(ctypes.Structure):
@@ -135,6 +136,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_batch_exact": (i, [_P, i, _P, _P, _P, ctypes.POINTER(d)]),
         "perm_batch_autotune": (i, [_P, i, i, _P]),
         "perm_dense_autotune": (i, [_P, i, i, _P]),
+        "perm_ctx_set_rel_target": (i, [_P, d]),
         "perm_server_create": (i, [i, i, ctypes.c_size_t, u64, ctypes.POINTER(_P)]),
         "perm_server_submit": (i, [_P, ctypes.POINTER(PermRequest), ctypes.POINTER(u64)]),
         "perm_server_wait": (i, [_P, u64, i, ctypes.POINTER(PermResponse)]),
@@ -178,6 +180,8 @@ class ExactResult:
     kernel_ms: float
     kernel: int
     n: int
+    abs_term_sum: float = 0.0
+    rel_error_estimate: float = 0.0
 
 
 @dataclass
@@ -191,7 +195,8 @@ class Estimate:
 
 
 def _exact(r: PermResult) -> ExactResult:
-    return ExactResult(r.value, r.hi, r.lo, r.steps, r.total_steps, r.kernel_ms, r.kernel, r.n)
+    return ExactResult(r.value, r.hi, r.lo, r.steps, r.total_steps, r.kernel_ms, r.kernel, r.n, r.abs_term_sum,
+                       r.rel_error_estimate)
 
 
 class Engine:
@@ -329,6 +334,10 @@ class Engine:
         out = np.zeros(n_hi - n_lo + 1, dtype=np.int32)
         self._check(self.lib.perm_batch_autotune(self.ctx, n_lo, n_hi, _ptr(out)))
         return {n_lo + i: int(m) for i, m in enumerate(out)}
+
+    def set_rel_target(self, target: float):
+        """Relative-error target above which automatic dense calls rerun in double-double."""
+        self._check(self.lib.perm_ctx_set_rel_target(self.ctx, target))
 
     def dense_autotune(self, n_lo: int, n_hi: int) -> dict:
         """Per order: which register kernel the automatic choice uses for integer inputs."""

@@ -33,6 +33,7 @@
 #include "mc_sparse.h"
 #include "perman_common.cuh"
 #include "ryser_dense.cuh"
+#include "ryser_dense_dd.cuh"
 #include "ryser_dense_int.cuh"
 #include "skipper.h"
 
@@ -47,6 +48,8 @@ const void* dense_int_kernel_g3(int n);
 const void* dense_int_kernel_g4(int n);
 const void* dense_int_kernel_g5(int n);
 const void* dense_int_kernel_g6(int n);
+
+const void* dense_dd_kernel(int n);
 
 static const void* dense_int_kernel(int n, int g) {
   switch (g) {
@@ -65,6 +68,48 @@ static const void* dense_kernel(int n) {
   if (n <= 52) return dense_kernel_3(n);
   if (n <= 64) return dense_kernel_4(n);
   return nullptr;
+}
+
+// Estimate of sum_i |term(i)| from `samples` Gray indices spread over the
+// walk (index s * stride mod 2^(n-1), stride odd): each thread builds x(i)
+// from scratch in FP64 and adds |prod x_j|; out[0] receives the sample sum.
+__global__ void __launch_bounds__(256) ryser_abs_sample_kernel(const double* colA, int n, int np, uint64_t samples,
+                                                                uint64_t stride, double* out) {
+  __shared__ double sA[64 * 64];
+  __shared__ double x0[64];
+  __shared__ double red[8];
+  for (int idx = threadIdx.x; idx < n * np; idx += blockDim.x) sA[idx] = colA[idx];
+  __syncthreads();
+  if (threadIdx.x < n) {
+    const int j = threadIdx.x;
+    double rs = 0.0;
+    for (int k = 0; k < n; k++) rs += sA[k * np + j];
+    x0[j] = sA[(n - 1) * np + j] - rs * 0.5;
+  }
+  __syncthreads();
+  const uint64_t mask = (n >= 2) ? ((1ull << (n - 1)) - 1) : 0;
+  double local = 0.0;
+  for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < samples;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = (s * stride) & mask;
+    const uint64_t g = i ^ (i >> 1);
+    double p = 1.0;
+    for (int j = 0; j < n; j++) {
+      double xj = x0[j];
+      for (int k = 0; k < n - 1; k++)
+        if ((g >> k) & 1) xj += sA[k * np + j];
+      p *= xj;
+    }
+    local += fabs(p);
+  }
+  for (int d = 16; d >= 1; d >>= 1) local += __shfl_down_sync(0xffffffffu, local, d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = local;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    atomicAdd(out, t);
+  }
 }
 
 __global__ void fp64_peak_kernel(double* out, int iters, double a, double b) {
@@ -115,6 +160,8 @@ struct perm_ctx {
   int dense_occ[8][PERM_MAX_EXACT_N + 1] = {};  // [0]: FP64-X, [G]: int32-X groups of G
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: int32-X)
+  double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
+  double* d_est = nullptr;                       // sample-kernel accumulator
   int batch_occ = 0;
   std::string err;
   std::mutex mu;
@@ -241,6 +288,7 @@ extern "C" void perm_ctx_destroy(perm_ctx* ctx) {
   cudaFree(ctx->d_out);
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_counters);
+  cudaFree(ctx->d_est);
   cudaFree(ctx->d_stage);
   cudaFree(ctx->d_trials);
   if (ctx->h_out) cudaFreeHost(ctx->h_out);
@@ -272,6 +320,7 @@ static int ctx_init(perm_ctx* ctx, int device) {
   CU(ctx, cudaMalloc(&ctx->d_out, sizeof(double) * 8));
   CU(ctx, cudaMalloc(&ctx->d_err, sizeof(int) * 4));
   CU(ctx, cudaMalloc(&ctx->d_counters, sizeof(unsigned long long) * 4));
+  CU(ctx, cudaMalloc(&ctx->d_est, sizeof(double) * 2));
   CU(ctx, cudaMemset(ctx->ticket, 0, sizeof(unsigned) * 4));
   CU(ctx, cudaMemset(ctx->d_err, 0, sizeof(int) * 4));
   CU(ctx, cudaMallocHost(&ctx->h_out, sizeof(double) * 16));
@@ -354,7 +403,7 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
   for (size_t i = 0; i < a.size(); i++) a[i] = elem(mat, dtype, i);
   op->n = n;
   const bool prefer_fp64 = variant == 0 && n <= PERM_MAX_EXACT_N && ctx->dense_pref[n] == PERM_KERNEL_DENSE;
-  int G = (variant == PERM_KERNEL_DENSE || prefer_fp64) ? 0 : int_group_size(a, n);
+  int G = (variant == PERM_KERNEL_DENSE || variant == PERM_KERNEL_DENSE_DD || prefer_fp64) ? 0 : int_group_size(a, n);
   if (variant == PERM_KERNEL_DENSE_INT && G == 0)
     return fail(ctx, PERM_EUNSUPPORTED,
                 "int32-X kernel needs an integer matrix of order >= 8 whose row products fit in int32");
@@ -374,7 +423,7 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
     }
   } else {
     const int np = (n + 1) & ~1;
-    op->variant = PERM_KERNEL_DENSE;
+    op->variant = variant == PERM_KERNEL_DENSE_DD ? PERM_KERNEL_DENSE_DD : PERM_KERNEL_DENSE;
     op->group = 0;
     op->image.assign(sizeof(double) * (size_t)n * np, 0);
     double* img = reinterpret_cast<double*>(op->image.data());
@@ -391,10 +440,13 @@ struct perm_matrix {
 
 static const void* operand_kernel(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_kernel(op.n, op.group);
+  if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
   return dense_kernel(op.n);
 }
 static size_t operand_smem(const DenseOperand& op) {
-  return op.variant == PERM_KERNEL_DENSE_INT ? dense_int_smem_bytes(op.n) : dense_smem_bytes(op.n);
+  if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_smem_bytes(op.n);
+  if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_smem_bytes(op.n);
+  return dense_smem_bytes(op.n);
 }
 
 struct DensePlan {
@@ -432,7 +484,8 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
   const int n = op.n;
   const void* fn = operand_kernel(op);
   if (!fn) return fail(ctx, PERM_EUNSUPPORTED, "dense exact order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
-  int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? op.group : 0][n];
+  int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? op.group
+                                 : op.variant == PERM_KERNEL_DENSE_DD ? 7 : 0][n];
   if (!occ_slot) {
     int occ = 0;
     CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, operand_smem(op)));
@@ -527,8 +580,50 @@ static int check_dense_args(perm_ctx* ctx, const void* mat, int n, int dtype, co
 }
 
 static int check_variant(perm_ctx* ctx, int variant) {
-  if (variant != 0 && variant != PERM_KERNEL_DENSE && variant != PERM_KERNEL_DENSE_INT)
+  if (variant != 0 && variant != PERM_KERNEL_DENSE && variant != PERM_KERNEL_DENSE_INT &&
+      variant != PERM_KERNEL_DENSE_DD)
     return fail(ctx, PERM_EINVAL, "unknown dense kernel variant %d", variant);
+  return PERM_OK;
+}
+
+// Error estimate of a whole-walk result: sum_i |term(i)| is estimated from
+// 65536 Gray indices spread over the walk (sample kernel), and the relative
+// error is taken as C * u * |factor| * sum|term| / |perm| with unit roundoff
+// u = 2^-53 and C = 2n + 16 (FP64 X: n roundings in the x updates and n - 1
+// in the product, plus the compensated sums), ceil(n/G) + 16 (int32 X: exact
+// x and group products, only the group products' FP64 multiplications
+// round), or (4n + 32) u for double-double.  A statistical estimate of the
+// cancellation, used to decide whether the double-double kernel must run.
+static int estimate_error(perm_ctx* ctx, const void* d_col_fp64, int n, const DenseOperand& op, perm_result* out) {
+  out->abs_term_sum = 0;
+  out->rel_error_estimate = 0;
+  if (n < 2) return PERM_OK;
+  const int np = (n + 1) & ~1;
+  const uint64_t total = 1ull << (n - 1);
+  const uint64_t samples = std::min<uint64_t>(total, 65536);
+  CU(ctx, cudaMemsetAsync(ctx->d_est, 0, sizeof(double), ctx->stream));
+  ryser_abs_sample_kernel<<<(unsigned)((samples + 255) / 256), 256, 0, ctx->stream>>>(
+      static_cast<const double*>(d_col_fp64), n, np, samples, 0x9E3779B97F4A7C15ull | 1ull, ctx->d_est);
+  CU(ctx, cudaGetLastError());
+  CU(ctx, cudaMemcpyAsync(ctx->h_out + 12, ctx->d_est, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(ctx, cudaStreamSynchronize(ctx->stream));
+  const double sum_abs = ctx->h_out[12] * ((double)total / (double)samples) * 2.0;
+  const double u = std::ldexp(1.0, -53);
+  double c;
+  if (op.variant == PERM_KERNEL_DENSE_DD)
+    c = (4.0 * n + 32.0) * u * u;
+  else if (op.variant == PERM_KERNEL_DENSE_INT)
+    c = (std::ceil((double)n / op.group) + 16.0) * u;
+  else
+    c = (2.0 * n + 16.0) * u;
+  out->abs_term_sum = sum_abs;
+  out->rel_error_estimate = out->value != 0.0 ? c * sum_abs / std::fabs(out->value) : (sum_abs > 0 ? INFINITY : 0.0);
+  return PERM_OK;
+}
+
+extern "C" int perm_ctx_set_rel_target(perm_ctx* ctx, double rel_target) {
+  if (!ctx) return PERM_EINVAL;
+  ctx->rel_target = rel_target;
   return PERM_OK;
 }
 
@@ -549,7 +644,37 @@ extern "C" int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dt
   if ((rc = dense_plan(ctx, op, shard, nshards, &p))) return rc;
   CU(ctx, cudaMemcpyAsync(ctx->d_stage, ctx->h_stage, op.image.size(), cudaMemcpyHostToDevice, ctx->stream));
   if ((rc = dense_launch(ctx, op, ctx->d_stage, p))) return rc;
-  return dense_collect(ctx, op, p, out);
+  if ((rc = dense_collect(ctx, op, p, out))) return rc;
+  out->abs_term_sum = out->rel_error_estimate = 0;
+  if (nshards != 1 || ctx->rel_target < 0) return PERM_OK;
+  // the estimate samples an FP64 column image; the int32 operand is rebuilt as one
+  const void* d_fp64 = ctx->d_stage;
+  DenseOperand f;
+  if (op.variant == PERM_KERNEL_DENSE_INT) {
+    if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE, &f))) return rc;
+    if ((rc = ensure_stage(ctx, f.image.size()))) return rc;
+    memcpy(ctx->h_stage, f.image.data(), f.image.size());
+    CU(ctx, cudaMemcpyAsync(ctx->d_stage, ctx->h_stage, f.image.size(), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if ((rc = estimate_error(ctx, d_fp64, n, op, out))) return rc;
+  if (variant == 0 && ctx->rel_target > 0 && out->rel_error_estimate > ctx->rel_target && n <= 40 &&
+      op.variant != PERM_KERNEL_DENSE_DD) {
+    DenseOperand dd_op;
+    if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE_DD, &dd_op))) return rc;
+    if (op.variant == PERM_KERNEL_DENSE_INT) {
+      // d_stage already holds the FP64 image (same bytes as dd_op's)
+    } else {
+      // d_stage holds the FP64 image already
+    }
+    DensePlan pd;
+    if ((rc = dense_plan(ctx, dd_op, 0, 1, &pd))) return rc;
+    const double fast_ms = out->kernel_ms;
+    if ((rc = dense_launch(ctx, dd_op, ctx->d_stage, pd))) return rc;
+    if ((rc = dense_collect(ctx, dd_op, pd, out))) return rc;
+    out->kernel_ms += fast_ms;
+    if ((rc = estimate_error(ctx, ctx->d_stage, n, dd_op, out))) return rc;
+  }
+  return PERM_OK;
 }
 
 extern "C" int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int shard,
@@ -607,7 +732,9 @@ extern "C" int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, pe
   int rc = dense_plan(ctx, m->op, 0, 1, &p);
   if (rc) return rc;
   if ((rc = dense_launch(ctx, m->op, m->d_image, p))) return rc;
-  return dense_collect(ctx, m->op, p, out);
+  rc = dense_collect(ctx, m->op, p, out);
+  out->abs_term_sum = out->rel_error_estimate = 0;
+  return rc;
 }
 
 // Autotuner for the automatic dense-kernel choice on integer inputs: for each

@@ -199,3 +199,50 @@ def test_dense_autotune_sets_the_automatic_choice(pb):
         for n, k in table.items():
             A = bernoulli(rng, n, 0.5)
             assert eng.exact_dense(A).kernel == k
+
+
+# ---- double-double kernel and per-result error estimates ------------------------------
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 12, 19, 24])
+def test_dd_kernel_vs_oracle(engine, orc, pb, n):
+    rng = np.random.default_rng(700 + n)
+    for A in (rng.standard_normal((n, n)), 1.0 - rng.random((n, n))):
+        r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_DD)
+        assert r.kernel == pb.PERM_KERNEL_DENSE_DD
+        hi, lo = orc.perm_dd(A)
+        # both are double-double evaluations: agree far below FP64 roundoff
+        assert abs((r.hi - hi) + (r.lo - lo)) <= 1e-24 * abs(hi) + 1e-300, (r.hi, r.lo, hi, lo)
+
+
+def test_dd_kernel_exact_on_integers(engine, orc, pb):
+    rng = np.random.default_rng(31)
+    A = bernoulli(rng, 22, 0.5) * rng.integers(1, 5, (22, 22))
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_DD)
+    exact = orc.perm_exact_int(A)[0]
+    assert int(r.hi) + int(r.lo) == exact
+
+
+def test_error_estimate_bounds_the_fp64_error(engine, orc, pb):
+    rng = np.random.default_rng(32)
+    for n in (14, 18, 22):
+        for _ in range(3):
+            A = rng.standard_normal((n, n))
+            r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE)
+            hi, lo = orc.perm_dd(A)
+            actual = abs(r.value - hi - lo) / abs(hi)
+            assert r.rel_error_estimate > 0 and r.abs_term_sum > 0
+            assert actual <= r.rel_error_estimate, (n, actual, r.rel_error_estimate)
+
+
+def test_automatic_double_double_rerun(pb, orc):
+    rng = np.random.default_rng(33)
+    A = rng.standard_normal((20, 20))
+    with pb.Engine(0) as eng:
+        eng.set_rel_target(1e-16)  # unreachable in FP64: forces the double-double rerun
+        r = eng.exact_dense(A)
+        assert r.kernel == pb.PERM_KERNEL_DENSE_DD
+        hi, lo = orc.perm_dd(A)
+        assert abs((r.hi - hi) + (r.lo - lo)) <= 1e-24 * abs(hi)
+        assert r.rel_error_estimate < 1e-20
+        eng.set_rel_target(0.0)  # no reruns
+        assert eng.exact_dense(A).kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_INT)

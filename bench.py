@@ -397,7 +397,7 @@ def batched_secondary(pb, eng, count=8192):
     b.run()
     times = []
     for _ in range(3):
-        vals, ms = b.run()
+        vals, est, reruns, ms = b.run_ex()
         times.append(ms)
     b.free()
     batch_ms = min(times)
@@ -415,7 +415,8 @@ def batched_secondary(pb, eng, count=8192):
     return {"matrices": count, "batch_ms": batch_ms, "batch_perms_per_s": count / (batch_ms * 1e-3),
             "batch_steps_per_s": steps / (batch_ms * 1e-3),
             "one_launch_per_matrix_ms": per_ms, "one_launch_per_matrix_perms_per_s": count / (per_ms * 1e-3),
-            "speedup_vs_one_launch_per_matrix": per_ms / batch_ms, "max_rel_diff_vs_single": err, "max_abs_diff_where_perm_below_1e-3": noise,
+            "speedup_vs_one_launch_per_matrix": per_ms / batch_ms, "max_rel_diff_vs_single": err,
+            "double_double_reruns": reruns, "max_rel_error_estimate": float(np.max(est)), "max_abs_diff_where_perm_below_1e-3": noise,
             "autotune_s": tune_s, "autotuned_lane_log2": table,
             "timing": "CUDA events around the graph launch (queue reset + kernel + 128 KB readback)"}
 

@@ -176,6 +176,12 @@ int perm_exact_dense_noalloc(const double* d_mat, int n, double* d_out, void* st
 typedef struct perm_batch perm_batch;
 int perm_batch_create(perm_ctx* ctx, int count, const int* orders, const double* values, perm_batch** out);
 int perm_batch_run(perm_ctx* ctx, perm_batch* b, double* results, double* kernel_ms);
+/* As perm_batch_run, and: the batch kernel also sums |term| per matrix, from
+ * which each result's relative-error estimate is formed (rel_err[count], may
+ * be NULL); matrices above the context's target (perm_ctx_set_rel_target)
+ * are recomputed by the double-double kernel, their count in *reruns. */
+int perm_batch_run_ex(perm_ctx* ctx, perm_batch* b, double* results, double* rel_err, int* reruns,
+                      double* kernel_ms);
 void perm_batch_destroy(perm_ctx* ctx, perm_batch* b);
 int perm_batch_exact(perm_ctx* ctx, int count, const int* orders, const double* values, double* results,
                      double* kernel_ms);

@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
     "perm_exact_dense_resident", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target",
-    "perm_batch_create", "perm_batch_run", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune",
+    "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
     "perm_approx_scaling_sparse", "perm_read_matrix", "perm_compress", "perm_grid_graph", "perm_fp64_peak",
@@ -132,6 +132,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_fp64_peak": (i, [_P, ctypes.POINTER(d), ctypes.POINTER(d)]),
         "perm_batch_create": (i, [_P, i, _P, _P, ctypes.POINTER(_P)]),
         "perm_batch_run": (i, [_P, _P, _P, ctypes.POINTER(d)]),
+        "perm_batch_run_ex": (i, [_P, _P, _P, _P, ctypes.POINTER(i), ctypes.POINTER(d)]),
         "perm_batch_destroy": (None, [_P, _P]),
         "perm_batch_exact": (i, [_P, i, _P, _P, _P, ctypes.POINTER(d)]),
         "perm_batch_autotune": (i, [_P, i, i, _P]),
@@ -359,10 +360,18 @@ class Batch:
 
     def run(self) -> tuple[np.ndarray, float]:
         """Returns (values, device ms); values[i] = hi + lo of matrix i."""
+        vals, _, _, ms = self.run_ex()
+        return vals, ms
+
+    def run_ex(self) -> tuple[np.ndarray, np.ndarray, int, float]:
+        """(values, relative-error estimates, double-double reruns, device ms of the batch graph)."""
         res = np.zeros(2 * self.count, dtype=np.float64)
+        est = np.zeros(self.count, dtype=np.float64)
         ms = ctypes.c_double()
-        self.engine._check(self.engine.lib.perm_batch_run(self.engine.ctx, self.handle, _ptr(res), ctypes.byref(ms)))
-        return res[0::2] + res[1::2], ms.value
+        reruns = ctypes.c_int()
+        self.engine._check(self.engine.lib.perm_batch_run_ex(self.engine.ctx, self.handle, _ptr(res), _ptr(est),
+                                                             ctypes.byref(reruns), ctypes.byref(ms)))
+        return res[0::2] + res[1::2], est, reruns.value, ms.value
 
     def free(self):
         if self.handle:

@@ -25,7 +25,7 @@ namespace {
 // whose columns are at col (stride np) and x0 at x0s.
 template <int N>
 __device__ __noinline__ void walk_range(const double* col, int np, const double* x0s, uint64_t s, uint64_t e,
-                                           Acc& acc) {
+                                           Acc& acc, double& abs_sum) {
   double x[N];
 #pragma unroll
   for (int j = 0; j < N; j++) x[j] = x0s[j];
@@ -37,7 +37,11 @@ __device__ __noinline__ void walk_range(const double* col, int np, const double*
       for (int j = 0; j < N; j++) x[j] += col[k * np + j];
     }
   }
-  acc.add(prod_only<N>(x));
+  {
+    const double p0 = prod_only<N>(x);
+    acc.add(p0);
+    abs_sum += fabs(p0);
+  }
   const double* c0 = col;
   const double* c1 = col + np;
   const double* c2 = col + 2 * np;
@@ -58,6 +62,7 @@ __device__ __noinline__ void walk_range(const double* col, int np, const double*
     double t7 = step<N, -1>(x, c0, 0.0);
     double t8 = step<N, 0>(x, col + k8 * np, s8);
     acc.add(((t2 - t1) + (t4 - t3)) + ((t6 - t5) + (t8 - t7)));
+    abs_sum += ((fabs(t1) + fabs(t2)) + (fabs(t3) + fabs(t4))) + ((fabs(t5) + fabs(t6)) + (fabs(t7) + fabs(t8)));
   }
   const double s4 = ((base >> 3) & 1) ? -1.0 : 1.0;
   double t1 = step<N, +1>(x, c0, 0.0);
@@ -68,10 +73,11 @@ __device__ __noinline__ void walk_range(const double* col, int np, const double*
   double t6 = step<N, -1>(x, c1, 0.0);
   double t7 = step<N, -1>(x, c0, 0.0);
   acc.add(((t2 - t1) + (t4 - t3)) + ((t6 - t5) - t7));
+  abs_sum += ((fabs(t1) + fabs(t2)) + (fabs(t3) + fabs(t4))) + ((fabs(t5) + fabs(t6)) + fabs(t7));
 }
 
 // Orders below 9 have fewer than 256 Gray indices: lane 0 walks them all.
-__device__ void walk_small(const double* col, int np, const double* x0s, int n, Acc& acc) {
+__device__ void walk_small(const double* col, int np, const double* x0s, int n, Acc& acc, double& abs_sum) {
   double x[8];
   for (int j = 0; j < n; j++) x[j] = x0s[j];
   const uint64_t total = 1ull << (n - 1);
@@ -84,14 +90,15 @@ __device__ void walk_small(const double* col, int np, const double* x0s, int n, 
     double p = x[0];
     for (int j = 1; j < n; j++) p *= x[j];
     acc.add((i & 1) ? -p : p);
+    abs_sum += fabs(p);
   }
 }
 
 __device__ __forceinline__ void walk_dispatch(int n, const double* col, int np, const double* x0s, uint64_t s,
-                                              uint64_t e, Acc& acc) {
+                                              uint64_t e, Acc& acc, double& abs_sum) {
   switch (n) {
 #define PERM_BATCH_CASE(N) \
-  case N: walk_range<N>(col, np, x0s, s, e, acc); break;
+  case N: walk_range<N>(col, np, x0s, s, e, acc, abs_sum); break;
     PERM_BATCH_CASE(9) PERM_BATCH_CASE(10) PERM_BATCH_CASE(11) PERM_BATCH_CASE(12) PERM_BATCH_CASE(13)
     PERM_BATCH_CASE(14) PERM_BATCH_CASE(15) PERM_BATCH_CASE(16) PERM_BATCH_CASE(17) PERM_BATCH_CASE(18)
     PERM_BATCH_CASE(19) PERM_BATCH_CASE(20) PERM_BATCH_CASE(21) PERM_BATCH_CASE(22) PERM_BATCH_CASE(23)
@@ -147,20 +154,25 @@ __global__ void __launch_bounds__(kBatchBlock) batch_kernel(BatchArgs a) {
     }
     const double* x0 = slot + n * np;
     Acc acc;
+    double abs_sum = 0.0;
     if (n < 9) {
-      if (lane == 0) walk_small(slot, np, x0, n, acc);
+      if (lane == 0) walk_small(slot, np, x0, n, acc, abs_sum);
     } else {
       const uint64_t q = t - M.first_tile;
       const uint64_t L = 1ull << M.m;
       const uint64_t s = (q * 32 + lane) * L;
-      walk_dispatch(n, slot, np, x0, s, s + L, acc);
+      walk_dispatch(n, slot, np, x0, s, s + L, acc, abs_sum);
     }
     dd v = acc.value();
 #pragma unroll
-    for (int d = 16; d >= 1; d >>= 1) v = dd_add(v, dd_shfl_down(v, d));
+    for (int d = 16; d >= 1; d >>= 1) {
+      v = dd_add(v, dd_shfl_down(v, d));
+      abs_sum += __shfl_down_sync(0xffffffffu, abs_sum, d);
+    }
     bool last = false;
     if (lane == 0) {
       a.tile_partials[t] = v;
+      a.tile_abs[t] = abs_sum;
       __threadfence();
       const unsigned prev = atomicAdd(&a.mat_done[mi], 1u);
       last = (prev == M.ntiles - 1);
@@ -169,18 +181,24 @@ __global__ void __launch_bounds__(kBatchBlock) batch_kernel(BatchArgs a) {
     if (last) {
       __threadfence();
       dd s = {0.0, 0.0};
+      double sa = 0.0;
       for (uint64_t k = lane; k < M.ntiles; k += 32) {
         dd p;
         p.hi = __ldcg(&a.tile_partials[M.first_tile + k].hi);
         p.lo = __ldcg(&a.tile_partials[M.first_tile + k].lo);
         s = dd_add(s, p);
+        sa += __ldcg(&a.tile_abs[M.first_tile + k]);
       }
 #pragma unroll
-      for (int d = 16; d >= 1; d >>= 1) s = dd_add(s, dd_shfl_down(s, d));
+      for (int d = 16; d >= 1; d >>= 1) {
+        s = dd_add(s, dd_shfl_down(s, d));
+        sa += __shfl_down_sync(0xffffffffu, sa, d);
+      }
       if (lane == 0) {
         const double f = (n & 1) ? 2.0 : -2.0;
-        a.results[2 * M.index] = s.hi * f;
-        a.results[2 * M.index + 1] = s.lo * f;
+        a.results[3 * M.index] = s.hi * f;
+        a.results[3 * M.index + 1] = s.lo * f;
+        a.results[3 * M.index + 2] = sa * 2.0;
         a.mat_done[mi] = 0u;
       }
     }

@@ -28,8 +28,9 @@ struct BatchArgs {
   uint64_t total_tiles;
   unsigned long long* next_tile;  // queue head, zero before launch
   dd* tile_partials;              // one per tile
+  double* tile_abs;               // sum of |term| per tile
   unsigned* mat_done;             // per-matrix tickets, zero before launch (re-armed by the kernel)
-  double* results;                // (hi, lo) per matrix, caller order
+  double* results;                // (hi, lo, sum |term|) per matrix, caller order
 };
 
 __global__ void batch_kernel(BatchArgs a);

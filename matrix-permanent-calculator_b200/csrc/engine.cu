@@ -1177,10 +1177,14 @@ struct perm_batch {
   double* d_operands = nullptr;
   BatchMatrix* d_mats = nullptr;
   dd* d_tile_partials = nullptr;
+  double* d_tile_abs = nullptr;
   unsigned* d_mat_done = nullptr;
   unsigned long long* d_next = nullptr;
   double* d_results = nullptr;
-  double* h_results = nullptr;  // pinned
+  double* h_results = nullptr;  // pinned: (hi, lo, sum |term|) per matrix
+  std::vector<int> orders;       // host copies for double-double reruns
+  std::vector<uint64_t> offsets;
+  std::vector<double> values;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -1192,6 +1196,7 @@ static void batch_free(perm_batch* b) {
   cudaFree(b->d_operands);
   cudaFree(b->d_mats);
   cudaFree(b->d_tile_partials);
+  cudaFree(b->d_tile_abs);
   cudaFree(b->d_mat_done);
   cudaFree(b->d_next);
   cudaFree(b->d_results);
@@ -1243,6 +1248,9 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
   perm_batch* b = new perm_batch();
   b->count = count;
   b->total_tiles = tiles;
+  b->orders.assign(orders, orders + count);
+  b->offsets = src_off;
+  b->values.assign(values, values + off);
   cudaError_t e;
 #define BT(expr)                                    \
   do {                                              \
@@ -1255,10 +1263,11 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
   BT(cudaMalloc(&b->d_operands, sizeof(double) * std::max<uint64_t>(img, 1)));
   BT(cudaMalloc(&b->d_mats, sizeof(BatchMatrix) * count));
   BT(cudaMalloc(&b->d_tile_partials, sizeof(dd) * tiles));
+  BT(cudaMalloc(&b->d_tile_abs, sizeof(double) * tiles));
   BT(cudaMalloc(&b->d_mat_done, sizeof(unsigned) * count));
   BT(cudaMalloc(&b->d_next, sizeof(unsigned long long)));
-  BT(cudaMalloc(&b->d_results, sizeof(double) * 2 * count));
-  BT(cudaMallocHost(&b->h_results, sizeof(double) * 2 * count));
+  BT(cudaMalloc(&b->d_results, sizeof(double) * 3 * count));
+  BT(cudaMallocHost(&b->h_results, sizeof(double) * 3 * count));
   BT(cudaMemcpy(b->d_operands, image.data(), sizeof(double) * img, cudaMemcpyHostToDevice));
   BT(cudaMemcpy(b->d_mats, q.data(), sizeof(BatchMatrix) * count, cudaMemcpyHostToDevice));
   BT(cudaMemset(b->d_mat_done, 0, sizeof(unsigned) * count));
@@ -1282,13 +1291,14 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
   args.total_tiles = tiles;
   args.next_tile = b->d_next;
   args.tile_partials = b->d_tile_partials;
+  args.tile_abs = b->d_tile_abs;
   args.mat_done = b->d_mat_done;
   args.results = b->d_results;
   void* kargs[] = {&args};
   BT(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), ctx->stream);
   cudaLaunchKernel((const void*)batch_kernel, dim3(b->grid), dim3(kBatchBlock), kargs, batch_smem_bytes(), ctx->stream);
-  cudaMemcpyAsync(b->h_results, b->d_results, sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(b->h_results, b->d_results, sizeof(double) * 3 * count, cudaMemcpyDeviceToHost, ctx->stream);
   BT(cudaStreamEndCapture(ctx->stream, &b->graph));
   BT(cudaGraphInstantiate(&b->exec, b->graph, 0));
 #undef BT
@@ -1313,15 +1323,52 @@ static int batch_run_locked(perm_ctx* ctx, perm_batch* b, double* results, doubl
   float ms = 0;
   CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   if (kernel_ms) *kernel_ms = ms;
-  if (results) memcpy(results, b->h_results, sizeof(double) * 2 * b->count);
+  if (results)
+    for (int i = 0; i < b->count; i++) {
+      results[2 * i] = b->h_results[3 * i];
+      results[2 * i + 1] = b->h_results[3 * i + 1];
+    }
+  return PERM_OK;
+}
+
+extern "C" int perm_batch_run_ex(perm_ctx* ctx, perm_batch* b, double* results, double* rel_err, int* reruns,
+                                 double* kernel_ms) {
+  if (!ctx || !b) return ctx ? fail(ctx, PERM_EINVAL, "null batch") : PERM_EINVAL;
+  {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CU(ctx, cudaSetDevice(ctx->device));
+    int rc = batch_run_locked(ctx, b, results, kernel_ms);
+    if (rc) return rc;
+  }
+  // per-matrix error estimate from the exact sum of |term| (FP64-X walk), and
+  // a double-double rerun of every matrix above the context's target
+  const double u = std::ldexp(1.0, -53);
+  int rerun = 0;
+  for (int i = 0; i < b->count; i++) {
+    const int n = b->orders[i];
+    const double v = b->h_results[3 * i] + b->h_results[3 * i + 1];
+    const double sa = b->h_results[3 * i + 2];
+    double est = v != 0.0 ? (2.0 * n + 16.0) * u * sa / std::fabs(v) : (sa > 0 ? INFINITY : 0.0);
+    if (ctx->rel_target > 0 && est > ctx->rel_target && n <= 40 && n >= 2) {
+      perm_result r;
+      int rc = perm_exact_dense_ex(ctx, b->values.data() + b->offsets[i], n, PERM_F64, PERM_KERNEL_DENSE_DD, 0, 1, &r);
+      if (rc) return rc;
+      if (results) {
+        results[2 * i] = r.hi;
+        results[2 * i + 1] = r.lo;
+      }
+      est = r.rel_error_estimate;
+      if (kernel_ms) *kernel_ms += r.kernel_ms;  // reruns count toward the batch's device time
+      rerun++;
+    }
+    if (rel_err) rel_err[i] = est;
+  }
+  if (reruns) *reruns = rerun;
   return PERM_OK;
 }
 
 extern "C" int perm_batch_run(perm_ctx* ctx, perm_batch* b, double* results, double* kernel_ms) {
-  if (!ctx || !b) return ctx ? fail(ctx, PERM_EINVAL, "null batch") : PERM_EINVAL;
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  CU(ctx, cudaSetDevice(ctx->device));
-  return batch_run_locked(ctx, b, results, kernel_ms);
+  return perm_batch_run_ex(ctx, b, results, nullptr, nullptr, kernel_ms);
 }
 
 extern "C" void perm_batch_destroy(perm_ctx* ctx, perm_batch* b) {

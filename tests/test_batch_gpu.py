@@ -72,3 +72,23 @@ def test_autotune_keeps_results(engine, pb):
 def test_batch_rejects_large_order(engine, pb):
     with pytest.raises(pb.PermError):
         engine.batch_exact([np.ones((41, 41))])
+
+
+def test_batch_error_estimates_and_reruns(engine, orc, pb):
+    rng = np.random.default_rng(12)
+    mats = [rng.standard_normal((n, n)) for n in (12, 15, 18, 20)]
+    b = engine.batch(mats)
+    try:
+        vals, est, reruns, _ = b.run_ex()
+        for m, v, e in zip(mats, vals, est):
+            hi, lo = orc.perm_dd(m)
+            assert abs(v - hi - lo) / abs(hi) <= max(e, 1e-15)
+        engine.set_rel_target(1e-16)  # unreachable in FP64: every matrix reruns in double-double
+        vals, est, reruns, _ = b.run_ex()
+        assert reruns == len(mats)
+        for m, v, e in zip(mats, vals, est):
+            hi, lo = orc.perm_dd(m)
+            assert abs(v - hi - lo) <= 1e-15 * abs(hi) and e < 1e-20
+    finally:
+        engine.set_rel_target(1e-10)
+        b.free()

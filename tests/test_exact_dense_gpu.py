@@ -82,12 +82,13 @@ def test_shards_sum_to_whole(engine, nshards):
     assert rel_err(hi + lo, whole.value) < 1e-12
 
 
-def test_resident_matrix_matches_one_shot(engine):
+def test_resident_matrix_matches_one_shot(engine, pb):
     rng = np.random.default_rng(6)
     A = 1.0 - rng.random((25, 25))
     m = engine.upload_dense(A)
     try:
-        assert m.run().value == engine.exact_dense(A).value
+        # same kernel both ways (the automatic path may rerun this real matrix in double-double)
+        assert m.run().value == engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE).value
     finally:
         m.free()
 
@@ -246,3 +247,17 @@ def test_automatic_double_double_rerun(pb, orc):
         assert r.rel_error_estimate < 1e-20
         eng.set_rel_target(0.0)  # no reruns
         assert eng.exact_dense(A).kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_INT)
+
+
+def test_fp64_error_grows_and_double_double_fixes_it(engine, pb):
+    """Dense positive real matrices cancel more with n: the FP64-X result's
+    estimate flags it and the automatic path returns the double-double value."""
+    rng = np.random.default_rng(4)
+    A = 1.0 - rng.random((30, 30))
+    f = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE)
+    d = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_DD)
+    auto = engine.exact_dense(A)
+    actual = abs(f.value - d.value) / abs(d.value)
+    assert actual <= f.rel_error_estimate
+    if f.rel_error_estimate > 1e-10:
+        assert auto.kernel == pb.PERM_KERNEL_DENSE_DD and auto.value == d.value

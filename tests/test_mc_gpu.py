@@ -142,3 +142,13 @@ def test_large_order_limits(engine, pb):
     rp = np.zeros(2049, np.int32)
     with pytest.raises(pb.PermError):
         engine.rasmussen_sparse(2048, rp, np.zeros(0, np.int32), 10)
+
+
+def test_n64_estimators_agree_at_bench_size(engine):
+    """Order 64, 2e5 trials each (the serving workload's approximate size):
+    the two estimators agree within their combined standard error."""
+    rng = np.random.default_rng(55)
+    A = (rng.random((64, 64)) < 0.5).astype(np.float64)
+    r = engine.rasmussen(A, 200000, seed=1)
+    s = engine.scaling(A, 200000, 4, 5, seed=2)
+    assert abs(r.mean - s.mean) < 5 * math.hypot(r.std_error, s.std_error)

@@ -124,11 +124,18 @@ int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, const int* cols
  * PERM_KERNEL_DENSE_INT forces int32 X (PERM_EUNSUPPORTED if not exact). */
 int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard, int nshards,
                         perm_result* out);
-/* Whole-walk dense results carry rel_error_estimate (cancellation estimated
- * from 65536 sampled Gray terms).  With variant 0, a result whose estimate
- * exceeds the context's target (default 1e-10; <= 0 disables the rerun) is
- * recomputed by the double-double kernel (orders <= 40).  PERM_KERNEL_DENSE_DD
- * forces that kernel. */
+/* Whole-walk dense results carry rel_error_estimate, a worst-case bound
+ * formed from sum |term| over 65536 sampled Gray terms.  With variant 0 and a
+ * context target (default 1e-10; <= 0 disables the policy; < 0 also skips
+ * the estimate):
+ *  - a zero pattern without a perfect matching returns exactly 0;
+ *  - a result whose bound exceeds the target is cross-checked against
+ *    B = A^T with its first row times 3 (perm(B) = 3 perm(A), independent
+ *    roundings) and kept when max(4-sigma independent-rounding estimate from
+ *    sum term^2, 16 |perm(A) - perm(B)/3| / |perm(A)|) meets the target, which
+ *    then is the reported estimate;
+ *  - otherwise it is recomputed by the double-double kernel (orders <= 40).
+ * kernel_ms covers every launch.  PERM_KERNEL_DENSE_DD forces that kernel. */
 int perm_ctx_set_rel_target(perm_ctx* ctx, double rel_target);
 
 /* Measures, for orders n_lo..n_hi (within 8..40), whether the int32-X or the
@@ -170,16 +177,19 @@ int perm_exact_dense_noalloc(const double* d_mat, int n, double* d_out, void* st
  * has order orders[i], 1 <= order <= 40, and occupies orders[i]^2 doubles).
  * perm_batch_create uploads them and captures the run (queue reset, one
  * persistent kernel, result readback) as a CUDA graph; perm_batch_run replays
- * it and writes (hi, lo) per matrix into results[2 * count] in caller order.
+ * it and writes (hi, lo) per matrix into results[2 * count] in caller order
+ * (the plain FP64-X values: no error estimate, no accuracy policy).
  * No counterpart in the reference, which computes one matrix per call
  * (gpu_exact_dense.cu:641); each result equals perm_exact_dense's to rounding. */
 typedef struct perm_batch perm_batch;
 int perm_batch_create(perm_ctx* ctx, int count, const int* orders, const double* values, perm_batch** out);
 int perm_batch_run(perm_ctx* ctx, perm_batch* b, double* results, double* kernel_ms);
 /* As perm_batch_run, and: the batch kernel also sums |term| per matrix, from
- * which each result's relative-error estimate is formed (rel_err[count], may
- * be NULL); matrices above the context's target (perm_ctx_set_rel_target)
- * are recomputed by the double-double kernel, their count in *reruns. */
+ * which each result's worst-case relative-error bound is formed (rel_err[count],
+ * may be NULL); matrices above the context's target (perm_ctx_set_rel_target)
+ * go through perm_exact_dense_ex's policy with the batch value as the first
+ * evaluation (exact zero, cross-check or double-double), their count in
+ * *reruns; kernel_ms includes those launches. */
 int perm_batch_run_ex(perm_ctx* ctx, perm_batch* b, double* results, double* rel_err, int* reruns,
                       double* kernel_ms);
 void perm_batch_destroy(perm_ctx* ctx, perm_batch* b);

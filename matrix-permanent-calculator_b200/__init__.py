@@ -337,7 +337,9 @@ class Engine:
         return {n_lo + i: int(m) for i, m in enumerate(out)}
 
     def set_rel_target(self, target: float):
-        """Relative-error target above which automatic dense calls rerun in double-double."""
+        """Relative-error target of the automatic dense path's accuracy policy
+        (exact zeros, transpose cross-check, double-double); 0 keeps the
+        estimate without the policy, < 0 skips the estimate too."""
         self._check(self.lib.perm_ctx_set_rel_target(self.ctx, target))
 
     def dense_autotune(self, n_lo: int, n_hi: int) -> dict:
@@ -359,12 +361,17 @@ class Batch:
         self.engine, self.handle, self.count = engine, handle, count
 
     def run(self) -> tuple[np.ndarray, float]:
-        """Returns (values, device ms); values[i] = hi + lo of matrix i."""
-        vals, _, _, ms = self.run_ex()
-        return vals, ms
+        """Returns (values, device ms) of one graph replay; values[i] = hi + lo
+        of matrix i (plain FP64-X walk, no accuracy policy)."""
+        res = np.zeros(2 * self.count, dtype=np.float64)
+        ms = ctypes.c_double()
+        self.engine._check(self.engine.lib.perm_batch_run(self.engine.ctx, self.handle, _ptr(res),
+                                                          ctypes.byref(ms)))
+        return res[0::2] + res[1::2], ms.value
 
     def run_ex(self) -> tuple[np.ndarray, np.ndarray, int, float]:
-        """(values, relative-error estimates, double-double reruns, device ms of the batch graph)."""
+        """(values, relative-error estimates, matrices re-evaluated by the
+        accuracy policy, device ms of the graph plus those re-evaluations)."""
         res = np.zeros(2 * self.count, dtype=np.float64)
         est = np.zeros(self.count, dtype=np.float64)
         ms = ctypes.c_double()
@@ -550,9 +557,13 @@ _default_engine: Engine | None = None
 
 
 def default_engine() -> Engine:
+    """Engine of the reference-named functions below.  Like the reference they
+    evaluate once (no error estimate, no accuracy policy) unless
+    PERM_REL_TARGET sets a target; PERM_DEVICE picks the device."""
     global _default_engine
     if _default_engine is None:
         _default_engine = Engine(int(os.environ.get("PERM_DEVICE", "0")))
+        _default_engine.set_rel_target(float(os.environ.get("PERM_REL_TARGET", "-1")))
     return _default_engine
 
 

@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -70,14 +71,15 @@ static const void* dense_kernel(int n) {
   return nullptr;
 }
 
-// Estimate of sum_i |term(i)| from `samples` Gray indices spread over the
-// walk (index s * stride mod 2^(n-1), stride odd): each thread builds x(i)
-// from scratch in FP64 and adds |prod x_j|; out[0] receives the sample sum.
+// Estimates of sum_i |term(i)| and sum_i term(i)^2 from `samples` Gray
+// indices spread over the walk (index s * stride mod 2^(n-1), stride odd):
+// each thread builds x(i) from scratch in FP64; out[0] and out[1] receive the
+// sample sums of |prod x_j| and of its square.
 __global__ void __launch_bounds__(256) ryser_abs_sample_kernel(const double* colA, int n, int np, uint64_t samples,
                                                                 uint64_t stride, double* out) {
   __shared__ double sA[64 * 64];
   __shared__ double x0[64];
-  __shared__ double red[8];
+  __shared__ double red[8], red2[8];
   for (int idx = threadIdx.x; idx < n * np; idx += blockDim.x) sA[idx] = colA[idx];
   __syncthreads();
   if (threadIdx.x < n) {
@@ -88,7 +90,7 @@ __global__ void __launch_bounds__(256) ryser_abs_sample_kernel(const double* col
   }
   __syncthreads();
   const uint64_t mask = (n >= 2) ? ((1ull << (n - 1)) - 1) : 0;
-  double local = 0.0;
+  double local = 0.0, local2 = 0.0;
   for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < samples;
        s += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t i = (s * stride) & mask;
@@ -101,14 +103,25 @@ __global__ void __launch_bounds__(256) ryser_abs_sample_kernel(const double* col
       p *= xj;
     }
     local += fabs(p);
+    local2 += p * p;
   }
-  for (int d = 16; d >= 1; d >>= 1) local += __shfl_down_sync(0xffffffffu, local, d);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = local;
+  for (int d = 16; d >= 1; d >>= 1) {
+    local += __shfl_down_sync(0xffffffffu, local, d);
+    local2 += __shfl_down_sync(0xffffffffu, local2, d);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = local;
+    red2[threadIdx.x >> 5] = local2;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    double t = 0.0, t2 = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      t += red[w];
+      t2 += red2[w];
+    }
     atomicAdd(out, t);
+    atomicAdd(out + 1, t2);
   }
 }
 
@@ -586,44 +599,165 @@ static int check_variant(perm_ctx* ctx, int variant) {
   return PERM_OK;
 }
 
-// Error estimate of a whole-walk result: sum_i |term(i)| is estimated from
-// 65536 Gray indices spread over the walk (sample kernel), and the relative
-// error is taken as C * u * |factor| * sum|term| / |perm| with unit roundoff
-// u = 2^-53 and C = 2n + 16 (FP64 X: n roundings in the x updates and n - 1
-// in the product, plus the compensated sums), ceil(n/G) + 16 (int32 X: exact
-// x and group products, only the group products' FP64 multiplications
-// round), or (4n + 32) u for double-double.  A statistical estimate of the
-// cancellation, used to decide whether the double-double kernel must run.
-static int estimate_error(perm_ctx* ctx, const void* d_col_fp64, int n, const DenseOperand& op, perm_result* out) {
-  out->abs_term_sum = 0;
-  out->rel_error_estimate = 0;
+// Error estimate of a whole-walk result.  The sample kernel estimates
+// S1 = sum_i |term(i)| and S2 = sum_i term(i)^2 from 65536 Gray indices
+// spread over the walk; with unit roundoff u = 2^-53 and r roundings per term
+// (FP64 X: n x updates and n - 1 products, r ~ 2n; int32 X: x and the group
+// products are exact, r = ceil(n/G) - 1 FP64 products):
+//  * worst: every rounding of every term in the same direction,
+//    (r + 16) u S1 / |perm|;
+//  * random: four standard deviations of the sum when roundings are
+//    independent and uniform (variance u^2 / 3 each), 4 u sqrt(r / 3)
+//    sqrt(S2) / |perm|.  Not a bound -- terms with equal values round alike --
+//    so it is only used together with an independent second evaluation;
+//  * double-double: (4n + 32) u^2 S1 / |perm|.
+struct ErrEstimate {
+  double s1 = 0, worst = 0, random = 0;
+};
+
+static int estimate_error(perm_ctx* ctx, const void* d_col_fp64, int n, const DenseOperand& op, double value,
+                          ErrEstimate* e) {
+  *e = ErrEstimate();
   if (n < 2) return PERM_OK;
   const int np = (n + 1) & ~1;
   const uint64_t total = 1ull << (n - 1);
   const uint64_t samples = std::min<uint64_t>(total, 65536);
-  CU(ctx, cudaMemsetAsync(ctx->d_est, 0, sizeof(double), ctx->stream));
+  CU(ctx, cudaMemsetAsync(ctx->d_est, 0, 2 * sizeof(double), ctx->stream));
   ryser_abs_sample_kernel<<<(unsigned)((samples + 255) / 256), 256, 0, ctx->stream>>>(
       static_cast<const double*>(d_col_fp64), n, np, samples, 0x9E3779B97F4A7C15ull | 1ull, ctx->d_est);
   CU(ctx, cudaGetLastError());
-  CU(ctx, cudaMemcpyAsync(ctx->h_out + 12, ctx->d_est, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(ctx, cudaMemcpyAsync(ctx->h_out + 12, ctx->d_est, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CU(ctx, cudaStreamSynchronize(ctx->stream));
-  const double sum_abs = ctx->h_out[12] * ((double)total / (double)samples) * 2.0;
+  const double scale = (double)total / (double)samples;
+  const double s1 = ctx->h_out[12] * scale * 2.0;       // |factor| = 2
+  const double s2 = ctx->h_out[13] * scale * 4.0;
   const double u = std::ldexp(1.0, -53);
-  double c;
-  if (op.variant == PERM_KERNEL_DENSE_DD)
-    c = (4.0 * n + 32.0) * u * u;
-  else if (op.variant == PERM_KERNEL_DENSE_INT)
-    c = (std::ceil((double)n / op.group) + 16.0) * u;
-  else
-    c = (2.0 * n + 16.0) * u;
-  out->abs_term_sum = sum_abs;
-  out->rel_error_estimate = out->value != 0.0 ? c * sum_abs / std::fabs(out->value) : (sum_abs > 0 ? INFINITY : 0.0);
+  const double av = std::fabs(value);
+  e->s1 = s1;
+  if (av == 0.0) {
+    e->worst = e->random = s1 > 0 ? INFINITY : 0.0;
+    return PERM_OK;
+  }
+  if (op.variant == PERM_KERNEL_DENSE_DD) {
+    e->worst = e->random = (4.0 * n + 32.0) * u * u * s1 / av;
+  } else if (op.variant == PERM_KERNEL_DENSE_INT) {
+    const double groups = std::ceil((double)n / op.group);
+    e->worst = (groups + 16.0) * u * s1 / av;
+    e->random = 4.0 * u * std::sqrt(std::max(1.0, groups - 1.0) / 3.0) * std::sqrt(s2) / av;
+  } else {
+    e->worst = (2.0 * n + 16.0) * u * s1 / av;
+    e->random = 4.0 * u * std::sqrt(2.0 * n / 3.0) * std::sqrt(s2) / av;
+  }
   return PERM_OK;
 }
 
 extern "C" int perm_ctx_set_rel_target(perm_ctx* ctx, double rel_target) {
   if (!ctx) return PERM_EINVAL;
   ctx->rel_target = rel_target;
+  return PERM_OK;
+}
+
+static int stage_operand(perm_ctx* ctx, const DenseOperand& op) {
+  int rc = ensure_stage(ctx, op.image.size());
+  if (rc) return rc;
+  memcpy(ctx->h_stage, op.image.data(), op.image.size());
+  CU(ctx, cudaMemcpyAsync(ctx->d_stage, ctx->h_stage, op.image.size(), cudaMemcpyHostToDevice, ctx->stream));
+  return PERM_OK;
+}
+
+// the whole walk of `op` from the staging buffer (context lock held)
+static int run_whole(perm_ctx* ctx, const DenseOperand& op, perm_result* out) {
+  int rc = stage_operand(ctx, op);
+  if (rc) return rc;
+  DensePlan p;
+  if ((rc = dense_plan(ctx, op, 0, 1, &p))) return rc;
+  if ((rc = dense_launch(ctx, op, ctx->d_stage, p))) return rc;
+  return dense_collect(ctx, op, p, out);
+}
+
+// Bipartite perfect matching of the nonzero pattern (augmenting paths,
+// O(n^3) on the host).  Without one every Gray term sum cancels to exactly 0.
+static bool has_perfect_matching(const void* mat, int n, int dtype) {
+  std::vector<int> match_col(n, -1);
+  std::vector<char> seen(n);
+  std::function<bool(int)> augment = [&](int r) -> bool {
+    for (int c = 0; c < n; c++) {
+      if (elem(mat, dtype, (size_t)r * n + c) == 0.0 || seen[c]) continue;
+      seen[c] = 1;
+      if (match_col[c] < 0 || augment(match_col[c])) {
+        match_col[c] = r;
+        return true;
+      }
+    }
+    return false;
+  };
+  for (int r = 0; r < n; r++) {
+    std::fill(seen.begin(), seen.end(), 0);
+    if (!augment(r)) return false;
+  }
+  return true;
+}
+
+// Error estimate of the whole-walk result in `out` (computed by `op`'s
+// kernel) and, with `policy`, the accuracy policy for the context's target:
+//  1. a zero pattern without a perfect matching has permanent exactly 0;
+//  2. the worst-case bound meets the target: keep;
+//  3. cross-check against B = A^T with its first row times 3
+//     (perm(B) = 3 perm(A)): B's x vectors are column sums and the factor 3
+//     changes every product's significand, even for symmetric or constant
+//     matrices, so B's roundings are independent of A's.  Keep when
+//     max(independent-rounding estimate, 16 |perm(A) - perm(B)/3| / |perm(A)|)
+//     meets the target;
+//  4. otherwise recompute in double-double (orders <= 40).
+// Context lock held.
+static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const DenseOperand& op, bool policy,
+                         perm_result* out) {
+  int rc;
+  if (policy && !has_perfect_matching(mat, n, dtype)) {
+    out->value = out->hi = out->lo = 0.0;
+    out->abs_term_sum = out->rel_error_estimate = 0.0;
+    return PERM_OK;
+  }
+  // the estimate samples an FP64 column image; an int32 operand is replaced by one
+  DenseOperand f;
+  const DenseOperand* fp = &op;
+  if (op.variant == PERM_KERNEL_DENSE_INT) {
+    if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE, &f))) return rc;
+    fp = &f;
+  }
+  if ((rc = stage_operand(ctx, *fp))) return rc;
+  ErrEstimate e;
+  if ((rc = estimate_error(ctx, ctx->d_stage, n, op, out->value, &e))) return rc;
+  out->abs_term_sum = e.s1;
+  out->rel_error_estimate = e.worst;
+  const double target = ctx->rel_target;
+  if (!policy || e.worst <= target || op.variant == PERM_KERNEL_DENSE_DD) return PERM_OK;
+  if (out->value != 0.0) {
+    std::vector<double> b((size_t)n * n);
+    for (int i2 = 0; i2 < n; i2++)
+      for (int j2 = 0; j2 < n; j2++)
+        b[(size_t)i2 * n + j2] = elem(mat, dtype, (size_t)j2 * n + i2) * (i2 == 0 ? 3.0 : 1.0);
+    DenseOperand t;
+    perm_result rt;
+    if ((rc = build_operand(ctx, b.data(), n, PERM_F64, 0, &t))) return rc;
+    if ((rc = run_whole(ctx, t, &rt))) return rc;
+    out->kernel_ms += rt.kernel_ms;
+    const double diff = std::fabs(out->value - rt.value / 3.0) / std::fabs(out->value);
+    const double est = std::max(e.random, 16.0 * diff);
+    if (est <= target) {
+      out->rel_error_estimate = est;
+      return PERM_OK;
+    }
+  }
+  if (n > 40) return PERM_OK;  // no double-double kernel above order 40: keep the bound
+  DenseOperand dd_op;
+  if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE_DD, &dd_op))) return rc;
+  const double first_ms = out->kernel_ms;
+  if ((rc = run_whole(ctx, dd_op, out))) return rc;
+  out->kernel_ms += first_ms;
+  if ((rc = estimate_error(ctx, ctx->d_stage, n, dd_op, out->value, &e))) return rc;
+  out->abs_term_sum = e.s1;
+  out->rel_error_estimate = e.worst;
   return PERM_OK;
 }
 
@@ -647,34 +781,7 @@ extern "C" int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dt
   if ((rc = dense_collect(ctx, op, p, out))) return rc;
   out->abs_term_sum = out->rel_error_estimate = 0;
   if (nshards != 1 || ctx->rel_target < 0) return PERM_OK;
-  // the estimate samples an FP64 column image; the int32 operand is rebuilt as one
-  const void* d_fp64 = ctx->d_stage;
-  DenseOperand f;
-  if (op.variant == PERM_KERNEL_DENSE_INT) {
-    if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE, &f))) return rc;
-    if ((rc = ensure_stage(ctx, f.image.size()))) return rc;
-    memcpy(ctx->h_stage, f.image.data(), f.image.size());
-    CU(ctx, cudaMemcpyAsync(ctx->d_stage, ctx->h_stage, f.image.size(), cudaMemcpyHostToDevice, ctx->stream));
-  }
-  if ((rc = estimate_error(ctx, d_fp64, n, op, out))) return rc;
-  if (variant == 0 && ctx->rel_target > 0 && out->rel_error_estimate > ctx->rel_target && n <= 40 &&
-      op.variant != PERM_KERNEL_DENSE_DD) {
-    DenseOperand dd_op;
-    if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE_DD, &dd_op))) return rc;
-    if (op.variant == PERM_KERNEL_DENSE_INT) {
-      // d_stage already holds the FP64 image (same bytes as dd_op's)
-    } else {
-      // d_stage holds the FP64 image already
-    }
-    DensePlan pd;
-    if ((rc = dense_plan(ctx, dd_op, 0, 1, &pd))) return rc;
-    const double fast_ms = out->kernel_ms;
-    if ((rc = dense_launch(ctx, dd_op, ctx->d_stage, pd))) return rc;
-    if ((rc = dense_collect(ctx, dd_op, pd, out))) return rc;
-    out->kernel_ms += fast_ms;
-    if ((rc = estimate_error(ctx, ctx->d_stage, n, dd_op, out))) return rc;
-  }
-  return PERM_OK;
+  return refine_result(ctx, mat, n, dtype, op, variant == 0 && ctx->rel_target > 0, out);
 }
 
 extern "C" int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int shard,
@@ -1334,14 +1441,13 @@ static int batch_run_locked(perm_ctx* ctx, perm_batch* b, double* results, doubl
 extern "C" int perm_batch_run_ex(perm_ctx* ctx, perm_batch* b, double* results, double* rel_err, int* reruns,
                                  double* kernel_ms) {
   if (!ctx || !b) return ctx ? fail(ctx, PERM_EINVAL, "null batch") : PERM_EINVAL;
-  {
-    std::lock_guard<std::mutex> lock(ctx->mu);
-    CU(ctx, cudaSetDevice(ctx->device));
-    int rc = batch_run_locked(ctx, b, results, kernel_ms);
-    if (rc) return rc;
-  }
-  // per-matrix error estimate from the exact sum of |term| (FP64-X walk), and
-  // a double-double rerun of every matrix above the context's target
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  int rc = batch_run_locked(ctx, b, results, kernel_ms);
+  if (rc) return rc;
+  // per-matrix worst-case bound from the exact sum of |term| (FP64-X walk);
+  // a matrix above the context's target goes through the single-matrix
+  // accuracy policy with the batch's value as the first evaluation
   const double u = std::ldexp(1.0, -53);
   int rerun = 0;
   for (int i = 0; i < b->count; i++) {
@@ -1349,16 +1455,23 @@ extern "C" int perm_batch_run_ex(perm_ctx* ctx, perm_batch* b, double* results, 
     const double v = b->h_results[3 * i] + b->h_results[3 * i + 1];
     const double sa = b->h_results[3 * i + 2];
     double est = v != 0.0 ? (2.0 * n + 16.0) * u * sa / std::fabs(v) : (sa > 0 ? INFINITY : 0.0);
-    if (ctx->rel_target > 0 && est > ctx->rel_target && n <= 40 && n >= 2) {
-      perm_result r;
-      int rc = perm_exact_dense_ex(ctx, b->values.data() + b->offsets[i], n, PERM_F64, PERM_KERNEL_DENSE_DD, 0, 1, &r);
-      if (rc) return rc;
+    if (ctx->rel_target > 0 && est > ctx->rel_target && n >= 2) {
+      const double* mat = b->values.data() + b->offsets[i];
+      DenseOperand op;
+      if ((rc = build_operand(ctx, mat, n, PERM_F64, PERM_KERNEL_DENSE, &op))) return rc;
+      perm_result r{};
+      r.hi = b->h_results[3 * i];
+      r.lo = b->h_results[3 * i + 1];
+      r.value = v;
+      r.n = n;
+      r.kernel = PERM_KERNEL_DENSE;
+      if ((rc = refine_result(ctx, mat, n, PERM_F64, op, true, &r))) return rc;
       if (results) {
         results[2 * i] = r.hi;
         results[2 * i + 1] = r.lo;
       }
       est = r.rel_error_estimate;
-      if (kernel_ms) *kernel_ms += r.kernel_ms;  // reruns count toward the batch's device time
+      if (kernel_ms) *kernel_ms += r.kernel_ms;  // checks and reruns count toward the batch's device time
       rerun++;
     }
     if (rel_err) rel_err[i] = est;
@@ -1368,7 +1481,10 @@ extern "C" int perm_batch_run_ex(perm_ctx* ctx, perm_batch* b, double* results, 
 }
 
 extern "C" int perm_batch_run(perm_ctx* ctx, perm_batch* b, double* results, double* kernel_ms) {
-  return perm_batch_run_ex(ctx, b, results, nullptr, nullptr, kernel_ms);
+  if (!ctx || !b) return ctx ? fail(ctx, PERM_EINVAL, "null batch") : PERM_EINVAL;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  return batch_run_locked(ctx, b, results, kernel_ms);
 }
 
 extern "C" void perm_batch_destroy(perm_ctx* ctx, perm_batch* b) {
@@ -1499,13 +1615,21 @@ extern "C" int perm_fp64_peak(perm_ctx* ctx, double* ops, double* kernel_ms) {
 // ---------------------------------------------------------------------------
 // reference-signature entry points on a process default context
 // ---------------------------------------------------------------------------
+// Context of the reference-signature entry points.  Like the reference they
+// evaluate once and return that value: no error estimate and no accuracy
+// policy unless PERM_REL_TARGET sets a target.  PERM_DEVICE picks the device.
 static perm_ctx* default_ctx() {
   static std::once_flag once;
   static perm_ctx* ctx = nullptr;
   std::call_once(once, [] {
     const char* d = getenv("PERM_DEVICE");
     int dev = d ? atoi(d) : 0;
-    if (perm_ctx_create(dev, &ctx) != PERM_OK) ctx = nullptr;
+    if (perm_ctx_create(dev, &ctx) != PERM_OK) {
+      ctx = nullptr;
+      return;
+    }
+    const char* t = getenv("PERM_REL_TARGET");
+    perm_ctx_set_rel_target(ctx, t ? atof(t) : -1.0);
   });
   return ctx;
 }

@@ -83,6 +83,15 @@ def test_batch_error_estimates_and_reruns(engine, orc, pb):
         for m, v, e in zip(mats, vals, est):
             hi, lo = orc.perm_dd(m)
             assert abs(v - hi - lo) / abs(hi) <= max(e, 1e-15)
+        # a zero pattern without a perfect matching: exactly 0, estimate 0
+        Z = rng.random((16, 16))
+        Z[:, 3] = 0.0
+        bz = engine.batch([Z])
+        try:
+            vz, ez, _, _ = bz.run_ex()
+            assert vz[0] == 0.0 and ez[0] == 0.0
+        finally:
+            bz.free()
         engine.set_rel_target(1e-16)  # unreachable in FP64: every matrix reruns in double-double
         vals, est, reruns, _ = b.run_ex()
         assert reruns == len(mats)

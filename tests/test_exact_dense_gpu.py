@@ -1,6 +1,7 @@
 """Dense exact Ryser kernel on the B200 against the oracle (tolerance 1e-10
 relative, the exact-algorithm bar; integer inputs that fit are compared exactly)."""
 import math
+from fractions import Fraction
 
 import numpy as np
 import pytest
@@ -260,4 +261,65 @@ def test_fp64_error_grows_and_double_double_fixes_it(engine, pb):
     actual = abs(f.value - d.value) / abs(d.value)
     assert actual <= f.rel_error_estimate
     if f.rel_error_estimate > 1e-10:
-        assert auto.kernel == pb.PERM_KERNEL_DENSE_DD and auto.value == d.value
+        # kept after the transpose cross-check, or recomputed in double-double
+        if auto.kernel == pb.PERM_KERNEL_DENSE_DD:
+            assert auto.value == d.value
+        else:
+            assert auto.kernel == pb.PERM_KERNEL_DENSE
+            assert abs(auto.value - d.value) / abs(d.value) <= auto.rel_error_estimate <= 1e-10
+
+
+@pytest.mark.parametrize("n", [28, 32])
+def test_transpose_cross_check_meets_the_target(engine, pb, n):
+    """Positive real matrices: the worst-case bound exceeds 1e-10 at these
+    orders; whatever the automatic path returns is within 1e-10 of the
+    double-double value."""
+    rng = np.random.default_rng(40 + n)
+    A = 1.0 - rng.random((n, n))
+    d = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_DD)
+    auto = engine.exact_dense(A)
+    assert abs(auto.value - d.value) <= 1e-10 * abs(d.value)
+    assert auto.rel_error_estimate <= 1e-10
+
+
+def test_int_kernel_estimate_covers_signed_cancellation(engine, orc, pb):
+    """Signed integer entries cancel heavily; the int32-X estimate (independent
+    roundings of exact group products) still covers the actual error."""
+    rng = np.random.default_rng(41)
+    for n in (16, 20, 24):
+        A = rng.integers(-2, 3, (n, n)).astype(np.float64)
+        r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
+        exact = orc.perm_exact_int(A)[0]
+        if exact == 0:
+            continue
+        actual = float(abs(Fraction(r.hi) + Fraction(r.lo) - exact) / abs(exact))
+        assert actual <= max(r.rel_error_estimate, 2.0 ** -52), (n, actual, r.rel_error_estimate)
+
+
+@pytest.mark.parametrize("n", [32, 36, 40])
+def test_int_kernel_estimate_at_headline_distribution(engine, pb, n):
+    """U{1..4} entries at density 0.5 (the headline workload's distribution):
+    the int32-X result's estimate covers its distance to the double-double
+    value, and the automatic path returns a result within the 1e-10 target."""
+    rng = np.random.default_rng(900 + n)
+    A = bernoulli(rng, n, 0.5) * rng.integers(1, 5, (n, n))
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
+    d = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_DD)
+    actual = abs(r.value - d.value) / abs(d.value)
+    assert actual <= max(r.rel_error_estimate, 2.0 ** -52), (actual, r.rel_error_estimate)
+    auto = engine.exact_dense(A)
+    assert abs(auto.value - d.value) <= 1e-10 * abs(d.value)
+
+
+def test_structural_zero_is_exact(engine, pb):
+    """A zero pattern without a perfect matching (rows 0 and 1 share one
+    nonzero column) has permanent exactly 0 on the automatic path."""
+    rng = np.random.default_rng(42)
+    A = rng.random((24, 24))
+    A[0, :] = 0.0
+    A[1, :] = 0.0
+    A[0, 5] = A[1, 5] = 1.0
+    r = engine.exact_dense(A)
+    assert r.value == 0.0 and r.hi == 0.0 and r.lo == 0.0 and r.rel_error_estimate == 0.0
+    f = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE)
+    assert abs(f.value) <= 1e-12 * f.abs_term_sum

@@ -177,6 +177,16 @@ def run_reference_arm(args):
     return 0
 
 
+def load_profile(kernel: str, n: int) -> dict | None:
+    """ncu figures of one launch of `kernel` at order n (profiles/), if recorded."""
+    prof = ROOT / "profiles" / "ryser_dense_n40_issue.json"
+    try:
+        rec = json.loads(prof.read_text()).get(kernel)
+    except Exception:
+        return None
+    return rec if rec and rec.get("n") == n else None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -186,8 +196,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--order", type=int, default=N_ORDER, help="matrix order (profiling runs use a smaller one)")
-    ap.add_argument("--variant", choices=["auto", "fp64", "int"], default="auto",
-                    help="dense kernel: automatic, FP64-X or int32-X")
+    ap.add_argument("--variant", choices=["auto", "fp64", "int", "tc"], default="auto",
+                    help="dense kernel: automatic, FP64-X, int32-X or tensor-core row sums")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -209,7 +219,8 @@ def main():
     eng = pb.Engine(device)
     A = make_matrix(rank, args.order)
     n = A.shape[0]
-    variant = {"auto": 0, "fp64": pb.PERM_KERNEL_DENSE, "int": pb.PERM_KERNEL_DENSE_INT}[args.variant]
+    variant = {"auto": 0, "fp64": pb.PERM_KERNEL_DENSE, "int": pb.PERM_KERNEL_DENSE_INT,
+               "tc": pb.PERM_KERNEL_DENSE_TC}[args.variant]
     total_steps = 2.0 ** (n - 1)
     ops_per_step = 2.0 * n  # n X-updates + n multiplies per Gray step (algorithmic)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")  # 256 MB > L2
@@ -278,22 +289,20 @@ def main():
 
     # the same call through perm_exact_dense with the accuracy policy
     # (target 1e-10): estimate, cross-check and, if needed, double-double
-    t = time.perf_counter()
-    rp = eng.exact_dense(A, variant=variant)
-    policy = {"ms": (time.perf_counter() - t) * 1e3, "kernel_ms": rp.kernel_ms, "kernel": rp.kernel,
-              "rel_error_estimate": rp.rel_error_estimate,
-              "rel_diff_vs_single_evaluation": abs(rp.value - perm_value) / abs(perm_value)}
+    policy = None
+    if not args.no_secondary:
+        t = time.perf_counter()
+        rp = eng.exact_dense(A, variant=variant)
+        policy = {"ms": (time.perf_counter() - t) * 1e3, "kernel_ms": rp.kernel_ms, "kernel": rp.kernel,
+                  "rel_error_estimate": rp.rel_error_estimate,
+                  "rel_diff_vs_single_evaluation": abs(rp.value - perm_value) / abs(perm_value)}
     barrier()
 
     mean_ms = statistics.mean(kernel_ms)
     achieved = total_steps * ops_per_step / (mean_ms * 1e-3)
-    traffic = None
-    prof = ROOT / "profiles" / "ryser_dense_n40_traffic.json"
-    if prof.exists():
-        try:
-            traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+    kname = {1: "fp64x", 3: "int32x", 5: "tc"}.get(r.kernel, "")
+    prof_rec = load_profile(kname, n)
+    traffic = prof_rec.get("dram_bytes_per_launch") if prof_rec else None
 
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
@@ -318,10 +327,42 @@ def main():
         "wall_s_timed": wall,
     }
     line["clocks"] = clk.summary()
+    if kname in ("int32x", "tc"):
+        # The integer and tensor-core kernels do not run the FP64-X algorithm:
+        # their binding resource is instruction issue (one warp instruction per
+        # cycle per SM sub-partition).  achieved = the kernel's warp
+        # instructions per launch (ncu, profiles/) / the CUDA-event launch time;
+        # peak = 4 x SMs x the median SM clock sampled during the timed region.
+        fp64_equiv = line["roofline"]
+        fp64_equiv["note"] = ("FP64-X-equivalent rate: this kernel moves the x updates off the FP64 pipe, "
+                              "so it can exceed the FP64 roofline")
+        sm_mhz = line["clocks"].get("sm_mhz") or 1965.0
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+        peak_issue = 4.0 * sms * sm_mhz * 1e6
+        inst = prof_rec.get("warp_inst_per_launch") if prof_rec else None
+        ach = inst / (mean_ms * 1e-3) if inst else None
+        line["roofline"] = {"bound": "issue", "achieved": ach / 1e12 if ach else None,
+                            "peak": peak_issue / 1e12, "unit": "Twarp-inst/s",
+                            "frac": ach / peak_issue if ach else None, "traffic": traffic,
+                            "peak_source": f"4 warp instructions / cycle / SM x {sms} SMs x "
+                                           f"{sm_mhz:.0f} MHz (median sampled SM clock)",
+                            "algorithmic": "smsp__inst_executed.sum of one launch of this kernel and order (ncu, "
+                                           "profiles/ryser_dense_n40_issue.json)",
+                            "fp64_equivalent": fp64_equiv}
 
-    line["config"]["kernel"] = {1: "FP64-X register kernel", 3: "int32-X register kernel"}.get(r.kernel, r.kernel)
+    line["config"]["kernel"] = {1: "FP64-X register kernel", 3: "int32-X register kernel",
+                                5: "tensor-core row sums (tcgen05 kind::i8) + int32 products"}.get(r.kernel, r.kernel)
     if rank == 0 and not args.no_secondary:
         line["secondary"] = secondary(pb, eng)
+        # the same n=40 matrix through the int32-X and tensor-core kernels
+        for key, v in (("dense_n40_int32x_same_matrix", pb.PERM_KERNEL_DENSE_INT),
+                       ("dense_n40_tensor_core_same_matrix", pb.PERM_KERNEL_DENSE_TC)):
+            rm = eng.upload_dense(A, variant=v)
+            rm.run()
+            ir = rm.run()
+            rm.free()
+            line["secondary"][key] = {"kernel_ms": ir.kernel_ms, "steps_per_s": total_steps / (ir.kernel_ms * 1e-3),
+                                      "rel_diff_vs_headline": abs(ir.value - perm_value) / abs(perm_value)}
         # the same n=40 matrix through the FP64-X kernel (the kernel used for real-valued inputs)
         f64 = eng.upload_dense(A, variant=pb.PERM_KERNEL_DENSE)
         f64.run()

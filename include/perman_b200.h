@@ -49,6 +49,8 @@ extern "C" {
 #define PERM_KERNEL_SKIPPER 2 /* SkipPer on CRS/CCS                          */
 #define PERM_KERNEL_DENSE_INT 3 /* int32-X Gray-code Ryser (integer matrices) */
 #define PERM_KERNEL_DENSE_DD 4  /* double-double Gray-code Ryser (orders <= 40) */
+#define PERM_KERNEL_DENSE_TC 5  /* tensor-core row sums (kind::i8) + int32 products:
+                                   integer matrices, |a| <= 63, orders 16..64 */
 
 /* Limits of this build. */
 #define PERM_MAX_EXACT_N 64  /* Gray indices are 64-bit                 */
@@ -120,8 +122,12 @@ int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, const int* cols
 
 /* Dense Ryser with an explicit kernel: variant 0 picks automatically (the
  * int32-X kernel for integer matrices whose grouped row products provably fit
- * in int32, the FP64-X kernel otherwise), PERM_KERNEL_DENSE forces FP64 X,
- * PERM_KERNEL_DENSE_INT forces int32 X (PERM_EUNSUPPORTED if not exact). */
+ * in int32, the FP64-X kernel otherwise; perm_dense_autotune can switch
+ * integer inputs to the FP64-X or the tensor-core kernel), PERM_KERNEL_DENSE
+ * forces FP64 X, PERM_KERNEL_DENSE_INT forces int32 X and PERM_KERNEL_DENSE_TC
+ * the tensor-core kernel (PERM_EUNSUPPORTED where not exact).  The
+ * tensor-core kernel runs whole walks only: with nshards > 1 its matrices use
+ * the int32-X kernel. */
 int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard, int nshards,
                         perm_result* out);
 /* Whole-walk dense results carry rel_error_estimate, a worst-case bound
@@ -138,10 +144,10 @@ int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int va
  * kernel_ms covers every launch.  PERM_KERNEL_DENSE_DD forces that kernel. */
 int perm_ctx_set_rel_target(perm_ctx* ctx, double rel_target);
 
-/* Measures, for orders n_lo..n_hi (within 8..40), whether the int32-X or the
- * FP64-X kernel is faster on this device for integer inputs and makes variant
- * 0 follow the measurement in this context.  choice_out receives
- * n_hi - n_lo + 1 kernel ids. */
+/* Measures, for orders n_lo..n_hi (within 8..40), which of the int32-X, the
+ * FP64-X and (n >= 16) the tensor-core kernel is fastest on this device for
+ * integer inputs and makes variant 0 follow the measurement in this context.
+ * choice_out receives n_hi - n_lo + 1 kernel ids. */
 int perm_dense_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* choice_out);
 
 /* Device-resident dense matrices: upload once, run many times (no host copy
@@ -150,6 +156,15 @@ int perm_matrix_create_dense(perm_ctx* ctx, const void* mat, int n, int dtype, p
 int perm_matrix_create_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, perm_matrix** out);
 void perm_matrix_destroy(perm_ctx* ctx, perm_matrix* m);
 int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, perm_result* out);
+
+/* The tensor-core kernel over rounds [round0, round0 + nrounds) only: the
+ * subsets whose columns 9 .. n-2 follow the Gray code of the round index,
+ * every choice of columns 0 .. 8 (512 subsets per round), scaled like the
+ * whole sum; round indices go up to 2^(n - 10).  No counterpart in the
+ * reference: for verification of the kernel at orders whose full walk is
+ * long, and for callers that partition the subsets themselves. */
+int perm_exact_dense_tc_rounds(perm_ctx* ctx, const void* mat, int n, int dtype, uint64_t round0,
+                               uint64_t nrounds, perm_result* out);
 
 /* ---- allocation-free dense exact permanent ------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate device

@@ -30,6 +30,7 @@ CLI_PATH = PKG_DIR / "bin" / "perman"
 PERM_OK, PERM_EINVAL, PERM_ECUDA, PERM_ENOMEM, PERM_EUNSUPPORTED, PERM_ETIMEOUT, PERM_EIO = 0, -1, -2, -3, -4, -5, -6
 PERM_F64, PERM_F32, PERM_I32 = 0, 1, 2
 PERM_KERNEL_DENSE, PERM_KERNEL_SKIPPER, PERM_KERNEL_DENSE_INT, PERM_KERNEL_DENSE_DD = 1, 2, 3, 4
+PERM_KERNEL_DENSE_TC = 5
 MAX_EXACT_N = 64
 MAX_MC_N = 64
 MAX_MC_SPARSE_N = 2047
@@ -39,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
-    "perm_exact_dense_resident", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target",
+    "perm_exact_dense_resident", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target",
     "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
@@ -120,6 +121,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_matrix_create_dense": (i, [_P, _P, i, i, ctypes.POINTER(_P)]),
         "perm_matrix_destroy": (None, [_P, _P]),
         "perm_exact_dense_resident": (i, [_P, _P, ctypes.POINTER(PermResult)]),
+        "perm_exact_dense_tc_rounds": (i, [_P, _P, i, i, u64, u64, ctypes.POINTER(PermResult)]),
         "perm_approx_rasmussen": (i, [_P, _P, i, i, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
         "perm_approx_scaling": (i, [_P, _P, i, i, i64, i, i, u64, _P, ctypes.POINTER(PermEstimate)]),
         "perm_approx_rasmussen_sparse": (i, [_P, i, _P, _P, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
@@ -236,7 +238,8 @@ class Engine:
 
     # ---- exact ----
     def exact_dense(self, mat, variant: int = 0) -> ExactResult:
-        """Dense Ryser; variant 0 = automatic, PERM_KERNEL_DENSE = FP64 X, PERM_KERNEL_DENSE_INT = int32 X."""
+        """Dense Ryser; variant 0 = automatic, PERM_KERNEL_DENSE = FP64 X, PERM_KERNEL_DENSE_INT = int32 X,
+        PERM_KERNEL_DENSE_TC = tensor-core row sums, PERM_KERNEL_DENSE_DD = double-double."""
         a, dt = _as_matrix(mat)
         r = PermResult()
         if variant:
@@ -268,6 +271,14 @@ class Engine:
         c = compress(order, mat)
         return self.exact_sparse(c["n"], c["rptrs"], c["cols"], c["rvals"], c["cptrs"], c["rows"], c["cvals"],
                                  variant)
+
+    def exact_dense_tc_rounds(self, mat, round0: int, nrounds: int) -> ExactResult:
+        """Tensor-core kernel over a range of its rounds (partial, scaled sum)."""
+        a, dt = _as_matrix(mat)
+        r = PermResult()
+        self._check(self.lib.perm_exact_dense_tc_rounds(self.ctx, _ptr(a), a.shape[0], dt, round0, nrounds,
+                                                        ctypes.byref(r)))
+        return _exact(r)
 
     def upload_dense(self, mat, variant: int = 0) -> "ResidentMatrix":
         a, dt = _as_matrix(mat)

@@ -33,6 +33,7 @@ LIB_SOURCES = [
     "ryser_dense_inst_0.cu", "ryser_dense_inst_1.cu", "ryser_dense_inst_2.cu",
     "ryser_dense_inst_3.cu", "ryser_dense_inst_4.cu", "ryser_dense_int_g3.cu", "ryser_dense_int_g4.cu",
     "ryser_dense_int_g5.cu", "ryser_dense_int_g6.cu", "ryser_dense_dd_inst.cu", "matrix_io.cpp",
+    "ryser_dense_tc_g3.cu", "ryser_dense_tc_g4.cu", "ryser_dense_tc_g5.cu", "ryser_dense_tc_g6.cu",
 ]
 CLI_SOURCES = ["perman_cli.cpp"]
 

@@ -35,6 +35,7 @@
 #include "perman_common.cuh"
 #include "ryser_dense.cuh"
 #include "ryser_dense_dd.cuh"
+#include "ryser_dense_tc.cuh"
 #include "ryser_dense_int.cuh"
 #include "skipper.h"
 
@@ -51,6 +52,21 @@ const void* dense_int_kernel_g5(int n);
 const void* dense_int_kernel_g6(int n);
 
 const void* dense_dd_kernel(int n);
+
+const void* dense_tc_kernel_g3(int n);
+const void* dense_tc_kernel_g4(int n);
+const void* dense_tc_kernel_g5(int n);
+const void* dense_tc_kernel_g6(int n);
+
+static const void* dense_tc_kernel(int n, int g) {
+  switch (g) {
+    case 3: return dense_tc_kernel_g3(n);
+    case 4: return dense_tc_kernel_g4(n);
+    case 5: return dense_tc_kernel_g5(n);
+    case 6: return dense_tc_kernel_g6(n);
+    default: return nullptr;
+  }
+}
 
 static const void* dense_int_kernel(int n, int g) {
   switch (g) {
@@ -170,9 +186,9 @@ struct perm_ctx {
   size_t h_stage_cap = 0;
   double* d_trials = nullptr;
   size_t d_trials_cap = 0;
-  int dense_occ[8][PERM_MAX_EXACT_N + 1] = {};  // [0]: FP64-X, [G]: int32-X groups of G
+  int dense_occ[12][PERM_MAX_EXACT_N + 1] = {};  // [0]: FP64-X, [G]: int32-X, [7]: dd, [8 + G - 3]: tensor core
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
-  int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: int32-X)
+  int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
   double* d_est = nullptr;                       // sample-kernel accumulator
   int batch_occ = 0;
@@ -411,18 +427,35 @@ static int int_group_size(const std::vector<double>& a, int n) {
   return 0;
 }
 
+// The tensor-core kernel takes int8 operands: |2a| <= 127, which also keeps
+// every row-sum value within its three base digits (|y| <= 63 x 64 = 4032).
+static bool tc_eligible(const std::vector<double>& a, int n) {
+  if (n < 16 || n > 64) return false;
+  for (double v : a)
+    if (std::fabs(v) > 63.0) return false;
+  return true;
+}
+
 static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, DenseOperand* op) {
   std::vector<double> a((size_t)n * n);
   for (size_t i = 0; i < a.size(); i++) a[i] = elem(mat, dtype, i);
   op->n = n;
-  const bool prefer_fp64 = variant == 0 && n <= PERM_MAX_EXACT_N && ctx->dense_pref[n] == PERM_KERNEL_DENSE;
+  const int pref = variant == 0 && n <= PERM_MAX_EXACT_N ? ctx->dense_pref[n] : 0;
+  const bool prefer_fp64 = pref == PERM_KERNEL_DENSE;
   int G = (variant == PERM_KERNEL_DENSE || variant == PERM_KERNEL_DENSE_DD || prefer_fp64) ? 0 : int_group_size(a, n);
   if (variant == PERM_KERNEL_DENSE_INT && G == 0)
     return fail(ctx, PERM_EUNSUPPORTED,
                 "int32-X kernel needs an integer matrix of order >= 8 whose row products fit in int32");
+  const bool tc_ok = G && tc_eligible(a, n);
+  if (variant == PERM_KERNEL_DENSE_TC && !tc_ok)
+    return fail(ctx, PERM_EUNSUPPORTED,
+                "tensor-core kernel needs an integer matrix of order 16..64 with |a| <= 63 whose row products "
+                "fit in int32");
   if (G) {
     const int np4 = (n + 3) & ~3;
-    op->variant = PERM_KERNEL_DENSE_INT;
+    op->variant = (variant == PERM_KERNEL_DENSE_TC || (variant == 0 && pref == PERM_KERNEL_DENSE_TC && tc_ok))
+                      ? PERM_KERNEL_DENSE_TC
+                      : PERM_KERNEL_DENSE_INT;
     op->group = G;
     op->image.assign(sizeof(int) * (size_t)(n + 1) * np4, 0);
     int* img = reinterpret_cast<int*>(op->image.data());
@@ -453,11 +486,14 @@ struct perm_matrix {
 
 static const void* operand_kernel(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_kernel(op.n, op.group);
+  if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
   return dense_kernel(op.n);
 }
+static int operand_threads(const DenseOperand& op) { return op.variant == PERM_KERNEL_DENSE_TC ? kTcThreads : 128; }
 static size_t operand_smem(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_smem_bytes(op.n);
+  if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_smem_bytes(op.n);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_smem_bytes(op.n);
   return dense_smem_bytes(op.n);
 }
@@ -498,11 +534,26 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
   const void* fn = operand_kernel(op);
   if (!fn) return fail(ctx, PERM_EUNSUPPORTED, "dense exact order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
   int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? op.group
-                                 : op.variant == PERM_KERNEL_DENSE_DD ? 7 : 0][n];
+                                 : op.variant == PERM_KERNEL_DENSE_DD ? 7
+                                 : op.variant == PERM_KERNEL_DENSE_TC ? 8 + op.group - 3 : 0][n];
   if (!occ_slot) {
+    int rc = allow_smem(ctx, fn, operand_smem(op));
+    if (rc) return rc;
     int occ = 0;
-    CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, operand_smem(op)));
+    CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, operand_threads(op), operand_smem(op)));
     occ_slot = std::max(occ, 1);
+  }
+  if (op.variant == PERM_KERNEL_DENSE_TC) {
+    // whole walk only: rounds of 512 subsets, one CTA per SM (it holds all
+    // 512 TMEM columns)
+    if (shard != 0 || nshards != 1) return fail(ctx, PERM_EINVAL, "tensor-core kernel runs whole walks only");
+    const int rb = tc_round_bits(n);
+    const uint64_t rounds = 1ull << rb;
+    p->grid = (int)std::min<uint64_t>((uint64_t)ctx->num_sms, rounds);
+    p->m = n - 1 - rb;
+    p->block0 = 0;
+    p->nblocks = rounds;
+    return PERM_OK;
   }
   uint64_t first = 0, last = 0;
   int ms = 0;
@@ -532,7 +583,20 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
 static int dense_launch(perm_ctx* ctx, const DenseOperand& op, const void* d_image, const DensePlan& p) {
   const int n = op.n;
   CU(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-  if (op.variant == PERM_KERNEL_DENSE_INT) {
+  if (op.variant == PERM_KERNEL_DENSE_TC) {
+    DenseTcArgs args;
+    args.colI = static_cast<const int*>(d_image);
+    args.np4 = (n + 3) & ~3;
+    args.round0 = p.block0;
+    args.nrounds = p.nblocks;
+    args.partials = ctx->partials;
+    args.ticket = ctx->ticket;
+    args.out = ctx->d_out;
+    args.err = ctx->d_err;
+    void* kargs[] = {&args};
+    CU(ctx, cudaLaunchKernel(operand_kernel(op), dim3(p.grid), dim3(kTcThreads), kargs, operand_smem(op),
+                             ctx->stream));
+  } else if (op.variant == PERM_KERNEL_DENSE_INT) {
     DenseIntArgs args;
     const int np4 = (n + 3) & ~3;
     args.colI = static_cast<const int*>(d_image);
@@ -594,7 +658,7 @@ static int check_dense_args(perm_ctx* ctx, const void* mat, int n, int dtype, co
 
 static int check_variant(perm_ctx* ctx, int variant) {
   if (variant != 0 && variant != PERM_KERNEL_DENSE && variant != PERM_KERNEL_DENSE_INT &&
-      variant != PERM_KERNEL_DENSE_DD)
+      variant != PERM_KERNEL_DENSE_DD && variant != PERM_KERNEL_DENSE_TC)
     return fail(ctx, PERM_EINVAL, "unknown dense kernel variant %d", variant);
   return PERM_OK;
 }
@@ -640,7 +704,7 @@ static int estimate_error(perm_ctx* ctx, const void* d_col_fp64, int n, const De
   }
   if (op.variant == PERM_KERNEL_DENSE_DD) {
     e->worst = e->random = (4.0 * n + 32.0) * u * u * s1 / av;
-  } else if (op.variant == PERM_KERNEL_DENSE_INT) {
+  } else if (op.variant == PERM_KERNEL_DENSE_INT || op.variant == PERM_KERNEL_DENSE_TC) {
     const double groups = std::ceil((double)n / op.group);
     e->worst = (groups + 16.0) * u * s1 / av;
     e->random = 4.0 * u * std::sqrt(std::max(1.0, groups - 1.0) / 3.0) * std::sqrt(s2) / av;
@@ -721,7 +785,7 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
   // the estimate samples an FP64 column image; an int32 operand is replaced by one
   DenseOperand f;
   const DenseOperand* fp = &op;
-  if (op.variant == PERM_KERNEL_DENSE_INT) {
+  if (op.variant == PERM_KERNEL_DENSE_INT || op.variant == PERM_KERNEL_DENSE_TC) {
     if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE, &f))) return rc;
     fp = &f;
   }
@@ -770,6 +834,9 @@ extern "C" int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dt
     return fail(ctx, PERM_EINVAL, "shard %d of %d", shard, nshards);
   DenseOperand op;
   if ((rc = build_operand(ctx, mat, n, dtype, variant, &op))) return rc;
+  // shards are Gray-index ranges of the walking kernels; the tensor-core
+  // kernel's operand image is the int32-X one
+  if (nshards > 1 && op.variant == PERM_KERNEL_DENSE_TC) op.variant = PERM_KERNEL_DENSE_INT;
   std::lock_guard<std::mutex> lock(ctx->mu);
   CU(ctx, cudaSetDevice(ctx->device));
   if ((rc = ensure_stage(ctx, op.image.size()))) return rc;
@@ -831,6 +898,32 @@ extern "C" void perm_matrix_destroy(perm_ctx* ctx, perm_matrix* m) {
   delete m;
 }
 
+extern "C" int perm_exact_dense_tc_rounds(perm_ctx* ctx, const void* mat, int n, int dtype, uint64_t round0,
+                                          uint64_t nrounds, perm_result* out) {
+  int rc = check_dense_args(ctx, mat, n, dtype, out);
+  if (rc) return rc;
+  DenseOperand op;
+  if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE_TC, &op))) return rc;
+  const uint64_t rounds = 1ull << tc_round_bits(n);
+  if (nrounds < 1 || round0 >= rounds || nrounds > rounds - round0)
+    return fail(ctx, PERM_EINVAL, "rounds [%llu, +%llu) outside [0, %llu)", (unsigned long long)round0,
+                (unsigned long long)nrounds, (unsigned long long)rounds);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  DensePlan p;
+  if ((rc = dense_plan(ctx, op, 0, 1, &p))) return rc;
+  p.block0 = round0;
+  p.nblocks = nrounds;
+  // at least 16 rounds per CTA, so that short ranges run through the
+  // in-place round updates and not only the from-scratch first rounds
+  p.grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)p.grid, nrounds / 16));
+  if ((rc = stage_operand(ctx, op))) return rc;
+  if ((rc = dense_launch(ctx, op, ctx->d_stage, p))) return rc;
+  rc = dense_collect(ctx, op, p, out);
+  out->abs_term_sum = out->rel_error_estimate = 0;
+  return rc;
+}
+
 extern "C" int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, perm_result* out) {
   if (!ctx || !m || !out) return ctx ? fail(ctx, PERM_EINVAL, "null argument") : PERM_EINVAL;
   std::lock_guard<std::mutex> lock(ctx->mu);
@@ -845,9 +938,9 @@ extern "C" int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, pe
 }
 
 // Autotuner for the automatic dense-kernel choice on integer inputs: for each
-// order in [n_lo, n_hi] (8..40) time the int32-X and FP64-X kernels on a
-// seeded binary matrix and keep the faster one in the context.  choice_out
-// (n_hi - n_lo + 1 ints) receives PERM_KERNEL_DENSE_INT or PERM_KERNEL_DENSE.
+// order in [n_lo, n_hi] (8..40) time the int32-X, FP64-X and (orders >= 16)
+// tensor-core kernels on a seeded binary matrix and keep the fastest in the
+// context.  choice_out (n_hi - n_lo + 1 ints) receives the kernel ids.
 extern "C" int perm_dense_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* choice_out) {
   if (!ctx) return PERM_EINVAL;
   if (n_lo < 8 || n_hi > 40 || n_lo > n_hi) return fail(ctx, PERM_EINVAL, "orders [%d, %d] outside [8, 40]", n_lo, n_hi);
@@ -859,9 +952,10 @@ extern "C" int perm_dense_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* choic
       v = (state >> 63) ? 1.0 : 0.0;
     }
     for (int j = 0; j < n; j++) a[(size_t)j * n + j] = 1.0;  // no empty row or column
-    double best_ms[2] = {1e30, 1e30};
-    const int variants[2] = {PERM_KERNEL_DENSE_INT, PERM_KERNEL_DENSE};
-    for (int v = 0; v < 2; v++) {
+    const int variants[3] = {PERM_KERNEL_DENSE_INT, PERM_KERNEL_DENSE, PERM_KERNEL_DENSE_TC};
+    const int nv = n >= 16 ? 3 : 2;
+    double best_ms[3] = {1e30, 1e30, 1e30};
+    for (int v = 0; v < nv; v++) {
       for (int rep = 0; rep < 3; rep++) {
         perm_result r;
         int rc = perm_exact_dense_ex(ctx, a.data(), n, PERM_F64, variants[v], 0, 1, &r);
@@ -869,7 +963,10 @@ extern "C" int perm_dense_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* choic
         if (rep) best_ms[v] = std::min(best_ms[v], r.kernel_ms);
       }
     }
-    ctx->dense_pref[n] = best_ms[1] < best_ms[0] ? PERM_KERNEL_DENSE : PERM_KERNEL_DENSE_INT;
+    int best = 0;
+    for (int v = 1; v < nv; v++)
+      if (best_ms[v] < best_ms[best]) best = v;
+    ctx->dense_pref[n] = variants[best];
     if (choice_out) choice_out[n - n_lo] = ctx->dense_pref[n];
   }
   return PERM_OK;
@@ -1018,7 +1115,7 @@ extern "C" int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, cons
     if (cols[p] < 0 || cols[p] >= n || rows[p] < 0 || rows[p] >= n)
       return fail(ctx, PERM_EINVAL, "index out of range at entry %d", p);
   if (variant != 0 && variant != PERM_KERNEL_SKIPPER && variant != PERM_KERNEL_DENSE &&
-      variant != PERM_KERNEL_DENSE_INT)
+      variant != PERM_KERNEL_DENSE_INT && variant != PERM_KERNEL_DENSE_TC)
     return fail(ctx, PERM_EINVAL, "unknown sparse kernel variant %d", variant);
   bool skipper = variant == PERM_KERNEL_SKIPPER;
   if (variant == 0) skipper = n < 8 || zero_term_fraction(n, rptrs, rvals, cptrs, rows, cvals, 2048) >= kSkipperZeroFraction;

@@ -184,8 +184,9 @@ namespace perm {
 // Shared-memory staging with the Blackwell bulk-copy (TMA) engine:
 // cp.async.bulk global -> shared, completion tracked by an mbarrier
 // transaction count.  Source and destination must be 16-byte aligned and the
-// size a multiple of 16 (callers pad their packed buffers).  No cluster
-// multicast.  The wait is bounded: after kMbarSpinLimit polls the kernel
+// size a multiple of 16 (callers pad their packed buffers).  Each CTA copies
+// from this GPU's global memory into its own shared memory only.  The wait is
+// bounded: after kMbarSpinLimit polls the kernel
 // records an error in *err and carries on without the data (callers then
 // skip their compute), so a lost completion can never hang the GPU.
 // ---------------------------------------------------------------------------

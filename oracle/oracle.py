@@ -127,6 +127,42 @@ class Oracle:
         return out
 
 
+def tc_rounds_sum(a, round0: int, nrounds: int):
+    """Exact (fractions.Fraction) partial Ryser sum over the subsets that the
+    tensor-core kernel assigns to rounds [round0, round0 + nrounds): every
+    choice of columns 0 .. 8 and the remaining columns 9 .. n - 2 by the Gray
+    code of the round index, each term (-1)^|S| prod_j y_j(S) with y = 2x (the
+    Nijenhuis-Wilf form of the reference's Ryser sum, gpu_exact_dense.cu:
+    330-399), scaled by (4(n&1) - 2) / 2^n like the whole sum.  Returns
+    (sum, sum of |terms|), both scaled.  Pure-Python integers: small round
+    counts only."""
+    from fractions import Fraction
+    a = np.asarray(a, dtype=np.int64)
+    n = a.shape[0]
+    low = 9
+    rb = n - 1 - low
+    cols = [[2 * int(a[j, k]) for j in range(n)] for k in range(n)]
+    y0 = [2 * int(a[j, n - 1]) - int(a[j].sum()) for j in range(n)]
+    total = abs_total = 0
+    for r in range(round0, round0 + nrounds):
+        g = r ^ (r >> 1)
+        base = list(y0)
+        for k in range(rb):
+            if (g >> k) & 1:
+                base = [b + c for b, c in zip(base, cols[low + k])]
+        for s in range(1 << low):
+            y = list(base)
+            for k in range(low):
+                if (s >> k) & 1:
+                    y = [v + c for v, c in zip(y, cols[k])]
+            t = 1
+            for v in y:
+                t *= v
+            total += -t if (bin(s).count("1") + bin(g).count("1")) & 1 else t
+            abs_total += abs(t)
+    return Fraction(total * (2 if n & 1 else -2), 2 ** n), Fraction(abs_total * 2, 2 ** n)
+
+
 def _crs_ccs(a):
     a = np.asarray(a) != 0
     n = a.shape[0]

@@ -323,3 +323,96 @@ def test_structural_zero_is_exact(engine, pb):
     assert r.value == 0.0 and r.hi == 0.0 and r.lo == 0.0 and r.rel_error_estimate == 0.0
     f = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE)
     assert abs(f.value) <= 1e-12 * f.abs_term_sum
+
+
+# ---- tensor-core kernel (kind::i8 row sums, int32 products) ----------------------------
+
+@pytest.mark.parametrize("n", [16, 17, 20, 23, 24, 27])
+def test_tc_kernel_vs_oracle(engine, orc, pb, n):
+    rng = np.random.default_rng(1100 + n)
+    A = bernoulli(rng, n, 0.5) * rng.integers(1, 5, (n, n))
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_TC)
+    assert r.kernel == pb.PERM_KERNEL_DENSE_TC and r.steps == r.total_steps == 2.0 ** (n - 1)
+    exact = orc.perm_exact_int(A)[0]
+    assert rel_err(r.value, exact) < 1e-12, (r.value, exact)
+
+
+@pytest.mark.parametrize("n", [32, 33, 36])
+def test_tc_kernel_vs_int_kernel(engine, pb, n):
+    """Orders where the CPU oracle is slow: against the int32-X kernel (pinned
+    to the oracle up to n = 30)."""
+    rng = np.random.default_rng(1150 + n)
+    A = bernoulli(rng, n, 0.5) * rng.integers(1, 5, (n, n))
+    t = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_TC)
+    i = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
+    assert t.kernel == pb.PERM_KERNEL_DENSE_TC
+    assert rel_err(t.value, i.value) < 1e-11, (t.value, i.value)
+
+
+@pytest.mark.parametrize("n,round0,nrounds", [(16, 0, 64), (31, 5, 6), (33, 0, 5), (40, 12345, 6),
+                                              (48, 2 ** 35 - 2, 4), (49, 3, 5), (57, 2 ** 40 - 3, 5),
+                                              (64, 2 ** 50 - 2, 4), (64, 2 ** 53 + 2 ** 52 + 11, 3)])
+def test_tc_kernel_round_ranges_vs_oracle(engine, pb, n, round0, nrounds):
+    """Every operand layout (16, 32, 48, 64 columns per block) up to order
+    64, on round ranges that one CTA walks (from-scratch first rounds, then
+    in-place updates, including round columns >= 32 at 2^35 and 2^50) and
+    the oracle sums exactly."""
+    from oracle import tc_rounds_sum
+    rng = np.random.default_rng(1170 + n)
+    lim = 63 if n <= 33 else 20  # keeps the int32 product grouping available
+    A = rng.integers(-lim, lim + 1, (n, n)).astype(np.float64) * (rng.random((n, n)) < 0.5)
+    A[0, 0], A[1, 1] = 63, -63  # int8 operand limits (2a = +-126)
+    r = engine.exact_dense_tc_rounds(A, round0, nrounds)
+    want, abs_sum = tc_rounds_sum(A, round0, nrounds)
+    assert r.steps == nrounds * 512.0
+    got = Fraction(r.hi) + Fraction(r.lo)
+    # group products are exact int32; only the <= 21 FP64 products across
+    # groups round: |error| <= (21 + 16) u sum |terms|
+    assert abs(got - want) <= Fraction(37, 2 ** 53) * abs_sum, (float(got), float(want), float(abs_sum))
+
+
+def test_tc_kernel_signed_and_extreme_entries(engine, orc, pb):
+    """Entries at the int8 limits of the operands (|2a| = 126) and mixed signs."""
+    rng = np.random.default_rng(1200)
+    for n, vals in ((18, (-63, 63)), (21, (-1, 1)), (24, (-5, 5))):
+        A = rng.integers(vals[0], vals[1] + 1, (n, n)).astype(np.float64)
+        A[0, 0] = vals[1]
+        r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_TC)
+        exact = orc.perm_exact_int(A)[0]
+        assert abs(r.value - exact) <= 1e-12 * max(abs(exact), r.abs_term_sum), (n, r.value, exact)
+
+
+def test_tc_kernel_matches_int_kernel_at_40(engine, pb):
+    rng = np.random.default_rng(1300)
+    A = bernoulli(rng, 40, 0.5) * rng.integers(1, 5, (40, 40))
+    t = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_TC)
+    i = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
+    assert rel_err(t.value, i.value) < 1e-10
+
+
+def test_tc_kernel_eligibility(engine, pb):
+    rng = np.random.default_rng(1400)
+    A = bernoulli(rng, 24, 0.5) * rng.integers(1, 5, (24, 24))
+    assert engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_TC).kernel == pb.PERM_KERNEL_DENSE_TC
+    B = A.copy()
+    B[0, 0] = 64  # beyond int8 operands
+    with pytest.raises(pb.PermError):
+        engine.exact_dense(B, variant=pb.PERM_KERNEL_DENSE_TC)
+    with pytest.raises(pb.PermError):
+        engine.exact_dense(A[:15, :15], variant=pb.PERM_KERNEL_DENSE_TC)
+    with pytest.raises(pb.PermError):
+        engine.exact_dense(A + 0.5, variant=pb.PERM_KERNEL_DENSE_TC)
+
+
+def test_tc_kernel_resident_and_shards(engine, pb):
+    rng = np.random.default_rng(1500)
+    A = bernoulli(rng, 26, 0.5) * rng.integers(1, 5, (26, 26))
+    whole = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_TC).value
+    res = engine.upload_dense(A, variant=pb.PERM_KERNEL_DENSE_TC)
+    try:
+        assert res.run().value == whole
+    finally:
+        res.free()
+    parts = [engine.exact_dense_shard(A, s, 3, variant=pb.PERM_KERNEL_DENSE_TC) for s in range(3)]
+    assert all(p.kernel == pb.PERM_KERNEL_DENSE_INT for p in parts)
+    assert rel_err(pb.dd_sum([(p.hi, p.lo) for p in parts])[0], whole) < 1e-12

@@ -174,3 +174,15 @@ def test_sparse_estimators_large_order_unbiased(orc):
     for v in (orc.rasmussen_sparse_trials(G, 3, 0, 20000), orc.scaling_sparse_trials(G, 4, 5, 3, 0, 5000)):
         mean, se = v.mean(), v.std(ddof=1) / math.sqrt(len(v))
         assert abs(mean - 12988816) < 5 * se
+
+
+def test_tc_round_restatement_sums_to_the_permanent(orc):
+    """The tensor-core kernel's subset split (rounds x 4 blocks x 128 lanes),
+    restated exactly in the oracle, covers every subset once with the right
+    signs: all rounds together give the permanent (orders 16, 17, 18)."""
+    from oracle import tc_rounds_sum
+    rng = np.random.default_rng(77)
+    for n in (16, 17, 18):
+        A = rng.integers(-3, 4, (n, n)).astype(np.float64)
+        total, _ = tc_rounds_sum(A, 0, 2 ** (n - 10))
+        assert total == orc.perm_exact_int(A)[0]

@@ -219,6 +219,7 @@ class Reference:
         L.ref_read_matrix_f64.argtypes = [ctypes.c_char_p, i, _P, i, ctypes.POINTER(i)]
         L.ref_compress_f64.argtypes = [i, _P, i, i, _P, _P, _P, _P, _P, _P]
         L.ref_grid_graph.argtypes = [i, i, _P, i]
+        L.ref_last_cuda_error.restype = ctypes.c_char_p
 
     def parallel_perman64(self, a, threads: int) -> float:
         a = np.ascontiguousarray(a, dtype=np.float64)

@@ -234,4 +234,8 @@ double ref_gpu_approximation_f64(const double* mat, int nov, int times, int y, i
   return r;
 }
 
+// The reference's GPU wrappers check no CUDA status; this reports (and
+// clears) the last error after one of them, as a string.
+const char* ref_last_cuda_error() { return cudaGetErrorString(cudaGetLastError()); }
+
 }  // extern "C"

@@ -7,11 +7,12 @@
 //   y_j(0) = 2 a[j][n-1] - rowsum_j,   y += 2 s A[:, k]   (integer adds)
 // and the n-way product is split into groups of G consecutive rows whose
 // product is formed exactly with 32-bit integer multiplies (the host proves
-// prod_{j in group} sum_k |a_jk| < 2^31 before choosing this kernel), biased by
-// 2^31 in the same IMAD, and converted to FP64 with one subtraction
-// (2^52 + u as a double has u in its low mantissa bits).  The group values are
-// multiplied in FP64 (four chains); terms are accumulated exactly as in the
-// FP64-X kernel and the final sum is scaled by (4(n&1)-2) / 2^n (exact).
+// prod_{j in group} sum_k |a_jk| < 2^31 before choosing this kernel) and
+// converted to FP64 with one (exact) int32 -> double conversion, one
+// instruction per group (measured 8% faster at n = 40 than forming 2^52 + u
+// from the bits and subtracting).  The group values are multiplied in FP64
+// (four chains); terms are accumulated exactly as in the FP64-X kernel and
+// the final sum is scaled by (4(n&1)-2) / 2^n (exact).
 //
 // Per Gray step this moves the X update and (G-1)/G of the product off the
 // FP64 pipe onto the integer pipes: ~n integer adds + n integer multiplies +
@@ -40,11 +41,6 @@ __device__ __forceinline__ int4 lds4i(const int* p) {
   return v;
 }
 
-// 2^52 + u for u < 2^32 (exact), minus 2^52 + 2^31 -> the signed group product.
-__device__ __forceinline__ double biased_to_double(uint32_t u) {
-  return __dsub_rn(__hiloint2double(0x43300000, (int)u), 4503601774854144.0);
-}
-
 template <int N, int G>
 __device__ __forceinline__ double group_product(const int (&y)[N]) {
   constexpr int NG = (N + G - 1) / G;
@@ -56,7 +52,7 @@ __device__ __forceinline__ double group_product(const int (&y)[N]) {
 #pragma unroll
     for (int t = 1; t < G; t++)
       if (j0 + t < N) pr = pr * (uint32_t)y[j0 + t];
-    const double d = biased_to_double(pr + 0x80000000u);
+    const double d = __int2double_rn((int)pr);
     if ((g & 3) == 0) p0 = g < 4 ? d : p0 * d;
     if ((g & 3) == 1) p1 = g < 4 ? d : p1 * d;
     if ((g & 3) == 2) p2 = g < 4 ? d : p2 * d;

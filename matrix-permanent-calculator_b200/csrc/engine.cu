@@ -1149,13 +1149,26 @@ static int mc_run(perm_ctx* ctx, const std::vector<uint64_t>& rowmask, const std
   a.y = y;
   a.z = z;
   a.mask_bytes = sizeof(uint64_t) * np;
-  a.pack_bytes = a.mask_bytes + (scaling ? 2 * sizeof(double) * (size_t)n * np : 0);
+  // 0/1 matrices take the mask-only scaling kernel (same FP64 results)
+  bool binary = scaling;
+  if (scaling)
+    for (double v : *dense)
+      if (v != 0.0 && v != 1.0) {
+        binary = false;
+        break;
+      }
+  a.pack_bytes = a.mask_bytes + (binary ? a.mask_bytes : scaling ? 2 * sizeof(double) * (size_t)n * np : 0);
   int rc = ensure_stage(ctx, a.pack_bytes);
   if (rc) return rc;
   unsigned char* h = ctx->h_stage;
   memset(h, 0, a.pack_bytes);
   memcpy(h, rowmask.data(), sizeof(uint64_t) * n);
-  if (scaling) {
+  if (binary) {
+    uint64_t* colmask = reinterpret_cast<uint64_t*>(h + a.mask_bytes);
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++)
+        if ((*dense)[(size_t)i * n + j] != 0.0) colmask[j] |= 1ull << i;
+  } else if (scaling) {
     double* A = reinterpret_cast<double*>(h + a.mask_bytes);
     double* AT = A + (size_t)n * np;
     for (int i = 0; i < n; i++)
@@ -1165,7 +1178,9 @@ static int mc_run(perm_ctx* ctx, const std::vector<uint64_t>& rowmask, const std
       }
   }
   const size_t smem = mc_smem_bytes(a.pack_bytes, scaling);
-  const void* fn = scaling ? (const void*)scaling_kernel : (const void*)rasmussen_kernel;
+  const void* fn = binary ? (const void*)scaling_kernel_binary
+                 : scaling ? (const void*)scaling_kernel
+                           : (const void*)rasmussen_kernel;
   if ((rc = allow_smem(ctx, fn, smem))) return rc;
   int occ = 0;
   CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kMcBlock, smem));

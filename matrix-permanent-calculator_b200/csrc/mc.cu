@@ -139,20 +139,29 @@ __global__ void __launch_bounds__(kMcBlock) rasmussen_kernel(McArgs a) {
   finish3(s, s2, zeros, slots, a);
 }
 
-__global__ void __launch_bounds__(kMcBlock) scaling_kernel(McArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// kBinary: every nonzero of the matrix is 1 and the pack holds the row masks
+// then the column masks.  A Sinkhorn sum over a 0/1 matrix adds exactly the
+// scaling factors of its 1 entries (a * d = d for a = 1; a zero entry adds
+// +0.0 to a non-negative sum), so walking the set bits of the masks in
+// ascending order gives the same FP64 value as the general sum over the
+// rows/columns still in the submatrix.
+template <bool kBinary>
+__device__ __forceinline__ void scaling_trials(const McArgs& a, unsigned char* smem) {
   const int n = a.n, np = a.np;
   const uint64_t* rowmask = reinterpret_cast<const uint64_t*>(smem);
-  const double* A = reinterpret_cast<const double*>(smem + a.mask_bytes);   // A[i * np + j]
+  const uint64_t* colmask = rowmask + np;                                      // binary pack
+  const double* A = reinterpret_cast<const double*>(smem + a.mask_bytes);   // A[i * np + j] (general pack)
   const double* AT = A + (size_t)n * np;                                       // AT[j * np + i]
   double* dwarp = reinterpret_cast<double*>(smem + a.pack_bytes);
-  double* slots = dwarp + (kMcBlock / 32) * 128;
+  double* slots = dwarp + (kMcBlock / 32) * kMcWarpDoubles;
   uint64_t* bar = reinterpret_cast<uint64_t*>(slots + (kMcBlock / 32) * 3);
   const bool staged = stage_to_smem(smem, a.pack, a.pack_bytes, bar, a.err);
 
   const int lane = threadIdx.x & 31;
-  double* dr = dwarp + (threadIdx.x >> 5) * 128;
+  double* dr = dwarp + (threadIdx.x >> 5) * kMcWarpDoubles;
   double* dc = dr + 64;
+  double* prefix = dc + 64;                               // running sums of the column choice
+  int* pcol = reinterpret_cast<int*>(prefix + 64);        // their columns
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   double s = 0, s2 = 0, zeros = 0;
@@ -171,8 +180,6 @@ __global__ void __launch_bounds__(kMcBlock) scaling_kernel(McArgs a) {
         const unsigned key = min_row_key(rowmask, n, colext, rowext, lane);
         const int row = (int)(key & 0xffu);
         if (it % a.y == 0) {
-          // only the rows/columns still in the submatrix take part; both
-          // passes walk them in ascending order (the CPU restatement's order)
           const uint64_t full = n == 64 ? ~0ull : ((1ull << n) - 1);
           const uint64_t rows_left = ~rowext & full, cols_left = ~colext & full;
           const int j0 = lane, j1 = lane + 32;
@@ -181,12 +188,28 @@ __global__ void __launch_bounds__(kMcBlock) scaling_kernel(McArgs a) {
           for (int k = 0; k < a.z; k++) {
             // column pass: lane owns columns lane, lane + 32
             double cs0 = 0.0, cs1 = 0.0;
-            for (uint64_t m = rows_left; m; m &= m - 1) {
-              const int i = __ffsll((long long)m) - 1;
-              const double d = dr[i];
-              const double* Ai = A + i * np;
-              if (c0) cs0 = __dadd_rn(cs0, __dmul_rn(d, Ai[j0]));
-              if (c1) cs1 = __dadd_rn(cs1, __dmul_rn(d, Ai[j1]));
+            if (kBinary) {
+              const uint64_t m0 = c0 ? (colmask[j0] & rows_left) : 0ull;
+              const uint64_t m1 = c1 ? (colmask[j1] & rows_left) : 0ull;
+              for (int i0 = 0; i0 < n; i0 += 8) {
+                const uint32_t b0 = (uint32_t)(m0 >> i0) & 0xFFu, b1 = (uint32_t)(m1 >> i0) & 0xFFu;
+#pragma unroll
+                for (int u = 0; u < 8; u += 2) {
+                  const double2 d = *reinterpret_cast<const double2*>(dr + i0 + u);
+                  if (b0 & (1u << u)) cs0 = __dadd_rn(cs0, d.x);
+                  if (b1 & (1u << u)) cs1 = __dadd_rn(cs1, d.x);
+                  if (b0 & (2u << u)) cs0 = __dadd_rn(cs0, d.y);
+                  if (b1 & (2u << u)) cs1 = __dadd_rn(cs1, d.y);
+                }
+              }
+            } else {
+              for (uint64_t m = rows_left; m; m &= m - 1) {
+                const int i = __ffsll((long long)m) - 1;
+                const double d = dr[i];
+                const double* Ai = A + i * np;
+                if (c0) cs0 = __dadd_rn(cs0, __dmul_rn(d, Ai[j0]));
+                if (c1) cs1 = __dadd_rn(cs1, __dmul_rn(d, Ai[j1]));
+              }
             }
             bool fail = (c0 && cs0 == 0.0) || (c1 && cs1 == 0.0);
             if (__any_sync(0xffffffffu, fail)) {
@@ -196,14 +219,30 @@ __global__ void __launch_bounds__(kMcBlock) scaling_kernel(McArgs a) {
             if (c0) dc[j0] = __drcp_rn(cs0);
             if (c1) dc[j1] = __drcp_rn(cs1);
             __syncwarp();
-            // row pass: lane owns rows lane, lane + 32 (reads the transposed copy)
+            // row pass: lane owns rows lane, lane + 32
             double rs0 = 0.0, rs1 = 0.0;
-            for (uint64_t m = cols_left; m; m &= m - 1) {
-              const int j = __ffsll((long long)m) - 1;
-              const double d = dc[j];
-              const double* ATj = AT + j * np;
-              if (r0) rs0 = __dadd_rn(rs0, __dmul_rn(ATj[j0], d));
-              if (r1) rs1 = __dadd_rn(rs1, __dmul_rn(ATj[j1], d));
+            if (kBinary) {
+              const uint64_t m0 = r0 ? (rowmask[j0] & cols_left) : 0ull;
+              const uint64_t m1 = r1 ? (rowmask[j1] & cols_left) : 0ull;
+              for (int i0 = 0; i0 < n; i0 += 8) {
+                const uint32_t b0 = (uint32_t)(m0 >> i0) & 0xFFu, b1 = (uint32_t)(m1 >> i0) & 0xFFu;
+#pragma unroll
+                for (int u = 0; u < 8; u += 2) {
+                  const double2 d = *reinterpret_cast<const double2*>(dc + i0 + u);
+                  if (b0 & (1u << u)) rs0 = __dadd_rn(rs0, d.x);
+                  if (b1 & (1u << u)) rs1 = __dadd_rn(rs1, d.x);
+                  if (b0 & (2u << u)) rs0 = __dadd_rn(rs0, d.y);
+                  if (b1 & (2u << u)) rs1 = __dadd_rn(rs1, d.y);
+                }
+              }
+            } else {
+              for (uint64_t m = cols_left; m; m &= m - 1) {
+                const int j = __ffsll((long long)m) - 1;
+                const double d = dc[j];
+                const double* ATj = AT + j * np;
+                if (r0) rs0 = __dadd_rn(rs0, __dmul_rn(ATj[j0], d));
+                if (r1) rs1 = __dadd_rn(rs1, __dmul_rn(ATj[j1], d));
+              }
             }
             fail = (r0 && rs0 == 0.0) || (r1 && rs1 == 0.0);
             if (__any_sync(0xffffffffu, fail)) {
@@ -216,27 +255,34 @@ __global__ void __launch_bounds__(kMcBlock) scaling_kernel(McArgs a) {
           }
           if (!ok) break;
         }
+        // column choice: running sums in ascending column order (recorded),
+        // the first one above u * sum (one ballot), the last column if none
         const uint64_t avail = rowmask[row] & ~colext;
         const double drow = dr[row];
         double sum = 0.0;
-        for (uint64_t m = avail; m; m &= m - 1) sum = __dadd_rn(sum, __dmul_rn(drow, dc[__ffsll((long long)m) - 1]));
+        int cnt = 0;
+        for (uint64_t m = avail; m; m &= m - 1, cnt++) {
+          const int j = __ffsll((long long)m) - 1;
+          sum = __dadd_rn(sum, __dmul_rn(drow, dc[j]));
+          if (lane == 0) {
+            prefix[cnt] = sum;
+            pcol[cnt] = j;
+          }
+        }
         if (sum == 0.0) {
           ok = false;
           break;
         }
+        __syncwarp();
         const u32x4 rnd = philox_step(a.seed, t, (uint32_t)it, kTagScaling);
         const double u = __dmul_rn(__dadd_rn(__dmul_rn((double)(rnd.x >> 5), 67108864.0), (double)(rnd.y >> 6)),
                                    1.0 / 9007199254740992.0);
         const double target = __dmul_rn(u, sum);
-        double run = 0.0, sp = 0.0;
-        int col = -1;
-        for (uint64_t m = avail; m; m &= m - 1) {
-          const int j = __ffsll((long long)m) - 1;
-          sp = __dmul_rn(drow, dc[j]);
-          run = __dadd_rn(run, sp);
-          col = j;
-          if (target < run) break;
-        }
+        const unsigned lo = __ballot_sync(0xffffffffu, lane < cnt && target < prefix[lane]);
+        const unsigned hi = __ballot_sync(0xffffffffu, lane + 32 < cnt && target < prefix[lane + 32]);
+        const int pick = lo ? __ffs(lo) - 1 : (hi ? 32 + __ffs(hi) - 1 : cnt - 1);
+        const int col = pcol[pick];
+        const double sp = __dmul_rn(drow, dc[col]);
         w.mul(__double2float_rn(__ddiv_rn(sum, sp)));
         colext |= 1ull << col;
         rowext |= 1ull << row;
@@ -253,6 +299,16 @@ __global__ void __launch_bounds__(kMcBlock) scaling_kernel(McArgs a) {
     }
   }
   finish3(s, s2, zeros, slots, a);
+}
+
+__global__ void __launch_bounds__(kMcBlock) scaling_kernel(McArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  scaling_trials<false>(a, smem);
+}
+
+__global__ void __launch_bounds__(kMcBlock) scaling_kernel_binary(McArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  scaling_trials<true>(a, smem);
 }
 
 }  // namespace perm

@@ -28,6 +28,17 @@ def test_scaling_trials_bit_identical(engine, orc, n, y, z):
     np.testing.assert_array_equal(e.trial_values, want)
 
 
+@pytest.mark.parametrize("n", [9, 33, 64])
+def test_scaling_trials_bit_identical_weighted(engine, orc, n):
+    """Entries other than 0/1 take the general scaling kernel (Sinkhorn sums
+    over the values); 0/1 matrices take the mask kernel: both match the oracle
+    bit for bit."""
+    rng = np.random.default_rng(300 + n)
+    A = bernoulli(rng, n, 0.5) * rng.integers(1, 4, (n, n))
+    e = engine.scaling(A, 500, 3, 4, seed=11, keep_trials=True)
+    np.testing.assert_array_equal(e.trial_values, orc.scaling_trials(A, 3, 4, 11, 0, 500))
+
+
 def test_estimates_within_standard_error(engine, orc):
     rng = np.random.default_rng(5)
     A = bernoulli(rng, 16, 0.5)

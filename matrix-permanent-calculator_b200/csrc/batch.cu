@@ -16,6 +16,7 @@
 
 #include "batch.h"
 #include "ryser_dense.cuh"
+#include "ryser_dense_int.cuh"
 
 namespace perm {
 
@@ -76,6 +77,62 @@ __device__ __noinline__ void walk_range(const double* col, int np, const double*
   abs_sum += ((fabs(t1) + fabs(t2)) + (fabs(t3) + fabs(t4))) + ((fabs(t5) + fabs(t6)) + fabs(t7));
 }
 
+// The same walk with y = 2x in int32 (ryser_dense_int.cuh): for integer
+// matrices whose product groups of G rows provably fit in int32.  Terms are
+// y-products (2^N times the x-products).
+template <int N, int G>
+__device__ __noinline__ void walk_range_int(const int* col, int np4, const int* y0s, uint64_t s, uint64_t e,
+                                            Acc& acc, double& abs_sum) {
+  int y[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) y[j] = y0s[j];
+  const uint64_t g = s ^ (s >> 1);
+#pragma unroll 1
+  for (int k = 0; k < N - 1; k++) {
+    if ((g >> k) & 1) {
+#pragma unroll
+      for (int j = 0; j < N; j++) y[j] += col[k * np4 + j];
+    }
+  }
+  {
+    const double p0 = group_product<N, G>(y);
+    acc.add(p0);
+    abs_sum += fabs(p0);
+  }
+  const int* c0 = col;
+  const int* c1 = col + np4;
+  const int* c2 = col + 2 * np4;
+  const uint64_t groups = (e - s) >> 3;
+  uint64_t base = s;
+#pragma unroll 1
+  for (uint64_t gi = 0; gi + 1 < groups; gi++, base += 8) {
+    const int s4 = ((base >> 3) & 1) ? -1 : 1;
+    const uint64_t i8 = base + 8;
+    const int k8 = __ffsll((long long)i8) - 1;
+    const int s8 = ((i8 >> (k8 + 1)) & 1) ? -1 : 1;
+    double t1 = istep<N, G, +1>(y, c0, 0);
+    double t2 = istep<N, G, +1>(y, c1, 0);
+    double t3 = istep<N, G, -1>(y, c0, 0);
+    double t4 = istep<N, G, 0>(y, c2, s4);
+    double t5 = istep<N, G, +1>(y, c0, 0);
+    double t6 = istep<N, G, -1>(y, c1, 0);
+    double t7 = istep<N, G, -1>(y, c0, 0);
+    double t8 = istep<N, G, 0>(y, col + k8 * np4, s8);
+    acc.add(((t2 - t1) + (t4 - t3)) + ((t6 - t5) + (t8 - t7)));
+    abs_sum += ((fabs(t1) + fabs(t2)) + (fabs(t3) + fabs(t4))) + ((fabs(t5) + fabs(t6)) + (fabs(t7) + fabs(t8)));
+  }
+  const int s4 = ((base >> 3) & 1) ? -1 : 1;
+  double t1 = istep<N, G, +1>(y, c0, 0);
+  double t2 = istep<N, G, +1>(y, c1, 0);
+  double t3 = istep<N, G, -1>(y, c0, 0);
+  double t4 = istep<N, G, 0>(y, c2, s4);
+  double t5 = istep<N, G, +1>(y, c0, 0);
+  double t6 = istep<N, G, -1>(y, c1, 0);
+  double t7 = istep<N, G, -1>(y, c0, 0);
+  acc.add(((t2 - t1) + (t4 - t3)) + ((t6 - t5) - t7));
+  abs_sum += ((fabs(t1) + fabs(t2)) + (fabs(t3) + fabs(t4))) + ((fabs(t5) + fabs(t6)) + fabs(t7));
+}
+
 // Orders below 9 have fewer than 256 Gray indices: lane 0 walks them all.
 __device__ void walk_small(const double* col, int np, const double* x0s, int n, Acc& acc, double& abs_sum) {
   double x[8];
@@ -111,6 +168,24 @@ __device__ __forceinline__ void walk_dispatch(int n, const double* col, int np, 
   }
 }
 
+__device__ __forceinline__ void walk_dispatch_int(int n, int g, const int* col, int np4, const int* y0s, uint64_t s,
+                                                  uint64_t e, Acc& acc, double& abs_sum) {
+  switch (n * 8 + g) {
+#define PERM_BATCH_ICASE(N) \
+  case N * 8 + 5: walk_range_int<N, 5>(col, np4, y0s, s, e, acc, abs_sum); break; \
+  case N * 8 + 6: walk_range_int<N, 6>(col, np4, y0s, s, e, acc, abs_sum); break;
+    PERM_BATCH_ICASE(9) PERM_BATCH_ICASE(10) PERM_BATCH_ICASE(11) PERM_BATCH_ICASE(12) PERM_BATCH_ICASE(13)
+    PERM_BATCH_ICASE(14) PERM_BATCH_ICASE(15) PERM_BATCH_ICASE(16) PERM_BATCH_ICASE(17) PERM_BATCH_ICASE(18)
+    PERM_BATCH_ICASE(19) PERM_BATCH_ICASE(20) PERM_BATCH_ICASE(21) PERM_BATCH_ICASE(22) PERM_BATCH_ICASE(23)
+    PERM_BATCH_ICASE(24) PERM_BATCH_ICASE(25) PERM_BATCH_ICASE(26) PERM_BATCH_ICASE(27) PERM_BATCH_ICASE(28)
+    PERM_BATCH_ICASE(29) PERM_BATCH_ICASE(30) PERM_BATCH_ICASE(31) PERM_BATCH_ICASE(32) PERM_BATCH_ICASE(33)
+    PERM_BATCH_ICASE(34) PERM_BATCH_ICASE(35) PERM_BATCH_ICASE(36) PERM_BATCH_ICASE(37) PERM_BATCH_ICASE(38)
+    PERM_BATCH_ICASE(39) PERM_BATCH_ICASE(40)
+#undef PERM_BATCH_ICASE
+    default: break;
+  }
+}
+
 __device__ __forceinline__ int find_matrix(const BatchMatrix* mats, int count, uint64_t tile) {
   int lo = 0, hi = count - 1;
   while (lo < hi) {  // last matrix with first_tile <= tile
@@ -138,16 +213,24 @@ __global__ void __launch_bounds__(kBatchBlock) batch_kernel(BatchArgs a) {
     const int mi = find_matrix(a.mats, a.count, t);
     const BatchMatrix M = a.mats[mi];
     const int n = M.n, np = (n + 1) & ~1;
+    const int np4 = (n + 3) & ~3;
     if (mi != cached) {
       __syncwarp();
-      const double* src = a.operands + M.offset;
-      for (int idx = lane; idx < n * np; idx += 32) slot[idx] = src[idx];
-      __syncwarp();
-      double* x0 = slot + n * np;
-      for (int j = lane; j < n; j += 32) {
-        double rs = 0.0;
-        for (int k = 0; k < n; k++) rs += slot[k * np + j];
-        x0[j] = slot[(n - 1) * np + j] - rs * 0.5;
+      if (M.g) {
+        // int32 image: doubled columns then y0, (n + 1) np4 words
+        const int* src = reinterpret_cast<const int*>(a.operands + M.offset);
+        int* dst = reinterpret_cast<int*>(slot);
+        for (int idx = lane; idx < (n + 1) * np4; idx += 32) dst[idx] = src[idx];
+      } else {
+        const double* src = a.operands + M.offset;
+        for (int idx = lane; idx < n * np; idx += 32) slot[idx] = src[idx];
+        __syncwarp();
+        double* x0 = slot + n * np;
+        for (int j = lane; j < n; j += 32) {
+          double rs = 0.0;
+          for (int k = 0; k < n; k++) rs += slot[k * np + j];
+          x0[j] = slot[(n - 1) * np + j] - rs * 0.5;
+        }
       }
       __syncwarp();
       cached = mi;
@@ -161,7 +244,12 @@ __global__ void __launch_bounds__(kBatchBlock) batch_kernel(BatchArgs a) {
       const uint64_t q = t - M.first_tile;
       const uint64_t L = 1ull << M.m;
       const uint64_t s = (q * 32 + lane) * L;
-      walk_dispatch(n, slot, np, x0, s, s + L, acc, abs_sum);
+      if (M.g) {
+        const int* ci = reinterpret_cast<const int*>(slot);
+        walk_dispatch_int(n, M.g, ci, np4, ci + n * np4, s, s + L, acc, abs_sum);
+      } else {
+        walk_dispatch(n, slot, np, x0, s, s + L, acc, abs_sum);
+      }
     }
     dd v = acc.value();
 #pragma unroll
@@ -195,10 +283,12 @@ __global__ void __launch_bounds__(kBatchBlock) batch_kernel(BatchArgs a) {
         sa += __shfl_down_sync(0xffffffffu, sa, d);
       }
       if (lane == 0) {
-        const double f = (n & 1) ? 2.0 : -2.0;
+        // y-products carry 2^n (exact power-of-two rescaling)
+        const double scale = M.g ? ldexp(1.0, -n) : 1.0;
+        const double f = ((n & 1) ? 2.0 : -2.0) * scale;
         a.results[3 * M.index] = s.hi * f;
         a.results[3 * M.index + 1] = s.lo * f;
-        a.results[3 * M.index + 2] = sa * 2.0;
+        a.results[3 * M.index + 2] = sa * 2.0 * scale;
         a.mat_done[mi] = 0u;
       }
     }

@@ -19,6 +19,9 @@ struct BatchMatrix {
   int n;                // order
   int m;                // lane range = 2^m Gray indices (unused below order 9)
   int index;            // position in the caller's batch
+  int g;                // 0: FP64 X (column-major doubles, stride np); 5 or 6: int32 X
+                        // with product groups of g rows (doubled int columns, stride
+                        // np4 = n rounded up to 4, then y0) -- orders >= 9 only
 };
 
 struct BatchArgs {

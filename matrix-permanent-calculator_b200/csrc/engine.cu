@@ -1401,6 +1401,7 @@ struct perm_batch {
   unsigned long long* d_next = nullptr;
   double* d_results = nullptr;
   double* h_results = nullptr;  // pinned: (hi, lo, sum |term|) per matrix
+  std::vector<int> groups;       // per matrix: 0 = FP64 X, else the int32-X group size
   std::vector<int> orders;       // host copies for double-double reruns
   std::vector<uint64_t> offsets;
   std::vector<double> values;
@@ -1444,6 +1445,14 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
     const int np = (n + 1) & ~1;
     M.offset = img;
     img += (uint64_t)n * np;
+    // int32 X for integer matrices whose groups of 5 or 6 rows fit in int32
+    // (every 0/1 matrix up to order 35); FP64 X otherwise
+    M.g = 0;
+    if (n >= 9) {
+      std::vector<double> a(values + src_off[i], values + src_off[i] + (size_t)n * n);
+      const int G = int_group_size(a, n);
+      if (G >= 5) M.g = G;
+    }
   }
   // queue order: most Gray work first (longest-processing-time scheduling)
   std::vector<int> order(count);
@@ -1461,13 +1470,30 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
     const int n = mats[i].n, np = (n + 1) & ~1;
     const double* a = values + src_off[i];
     double* dst = image.data() + mats[i].offset;
-    for (int k = 0; k < n; k++)
-      for (int j = 0; j < np; j++) dst[(size_t)k * np + j] = j < n ? a[(size_t)j * n + k] : 0.0;
+    if (mats[i].g) {
+      // doubled int columns (stride np4), then y0 = 2 a[j][n-1] - rowsum_j;
+      // (n + 1) np4 words fit in the n np doubles reserved for the matrix
+      const int np4 = (n + 3) & ~3;
+      int* di = reinterpret_cast<int*>(dst);
+      for (int k = 0; k < n; k++)
+        for (int j = 0; j < np4; j++) di[(size_t)k * np4 + j] = j < n ? 2 * (int)a[(size_t)j * n + k] : 0;
+      for (int j = 0; j < np4; j++) {
+        long long rs = 0;
+        if (j < n)
+          for (int k = 0; k < n; k++) rs += (long long)a[(size_t)j * n + k];
+        di[(size_t)n * np4 + j] = j < n ? (int)(2 * (long long)a[(size_t)j * n + n - 1] - rs) : 0;
+      }
+    } else {
+      for (int k = 0; k < n; k++)
+        for (int j = 0; j < np; j++) dst[(size_t)k * np + j] = j < n ? a[(size_t)j * n + k] : 0.0;
+    }
   }
   perm_batch* b = new perm_batch();
   b->count = count;
   b->total_tiles = tiles;
   b->orders.assign(orders, orders + count);
+  b->groups.resize(count);
+  for (int i = 0; i < count; i++) b->groups[i] = mats[i].g;
   b->offsets = src_off;
   b->values.assign(values, values + off);
   cudaError_t e;
@@ -1566,17 +1592,20 @@ extern "C" int perm_batch_run_ex(perm_ctx* ctx, perm_batch* b, double* results, 
     const int n = b->orders[i];
     const double v = b->h_results[3 * i] + b->h_results[3 * i + 1];
     const double sa = b->h_results[3 * i + 2];
-    double est = v != 0.0 ? (2.0 * n + 16.0) * u * sa / std::fabs(v) : (sa > 0 ? INFINITY : 0.0);
+    const int G = b->groups[i];
+    const double rounds = G ? std::ceil((double)n / G) : 2.0 * n;  // roundings per term
+    double est = v != 0.0 ? (rounds + 16.0) * u * sa / std::fabs(v) : (sa > 0 ? INFINITY : 0.0);
     if (ctx->rel_target > 0 && est > ctx->rel_target && n >= 2) {
       const double* mat = b->values.data() + b->offsets[i];
+      const int kernel = G ? PERM_KERNEL_DENSE_INT : PERM_KERNEL_DENSE;
       DenseOperand op;
-      if ((rc = build_operand(ctx, mat, n, PERM_F64, PERM_KERNEL_DENSE, &op))) return rc;
+      if ((rc = build_operand(ctx, mat, n, PERM_F64, kernel, &op))) return rc;
       perm_result r{};
       r.hi = b->h_results[3 * i];
       r.lo = b->h_results[3 * i + 1];
       r.value = v;
       r.n = n;
-      r.kernel = PERM_KERNEL_DENSE;
+      r.kernel = kernel;
       if ((rc = refine_result(ctx, mat, n, PERM_F64, op, true, &r))) return rc;
       if (results) {
         results[2 * i] = r.hi;

@@ -101,3 +101,38 @@ def test_batch_error_estimates_and_reruns(engine, orc, pb):
     finally:
         engine.set_rel_target(1e-10)
         b.free()
+
+
+def test_integer_matrices_take_int32_x_exactly(engine, orc):
+    """0/1 and small-integer matrices (groups of 5-6 rows fit in int32) walk
+    y = 2x in int32 inside the batch; larger entries stay in FP64 X.  All
+    agree with the exact oracle, including integer permanents above 2^53."""
+    rng = np.random.default_rng(77)
+    mats = []
+    for n in (9, 12, 17, 22, 26):
+        mats.append((rng.random((n, n)) < 0.5).astype(np.float64))
+    for n in (10, 16, 24):
+        mats.append(rng.integers(-2, 3, (n, n)).astype(np.float64))
+    mats.append(rng.integers(0, 200, (14, 14)).astype(np.float64))  # groups do not fit: FP64 X
+    b = engine.batch(mats)
+    try:
+        vals, est, _, _ = b.run_ex()
+    finally:
+        b.free()
+    for A, v, e in zip(mats, vals, est):
+        exact = orc.perm_exact_int(A)[0]
+        if exact == 0:
+            assert abs(v) <= 1e-9
+        else:
+            assert abs(v - exact) <= max(1e-10, e) * abs(exact), (A.shape[0], v, exact, e)
+
+
+def test_order_35_binary_in_batch_matches_single_kernel(engine, pb):
+    """Groups of 6 rows still fit at order 35 (35^6 < 2^31): the batch's int32
+    walk against the single-matrix int32-X kernel (the CPU oracle is too slow
+    at this order)."""
+    rng = np.random.default_rng(78)
+    A = (rng.random((35, 35)) < 0.5).astype(np.float64)
+    vals, _ = engine.batch_exact([A])
+    single = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT).value
+    assert abs(vals[0] - single) <= 1e-12 * abs(single)

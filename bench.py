@@ -374,7 +374,7 @@ def main():
             "rel_diff_vs_headline": abs(fr.value - perm_value) / abs(perm_value)}
         line["secondary"]["reference_gpu_p4_same_box"] = reference_gpu(A)
         line["secondary"]["batched_8192_n12_28"] = batched_secondary(pb, eng)
-        line["secondary"]["serving_poisson_2000_per_s"] = serving_secondary(pb)
+        line["secondary"]["serving_poisson_2000_per_s"] = serving_secondary(pb, baseline=True)
         line["secondary"]["serving_poisson_40_per_s"] = serving_secondary(pb, requests=120, rate=40.0)
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -512,10 +512,12 @@ def batched_secondary(pb, eng, count=8192):
             "timing": "CUDA events around the graph launch (queue reset + kernel + 128 KB readback)"}
 
 
-def serving_secondary(pb, requests=400, rate=2000.0, slots=4, seed=5555):
+def serving_secondary(pb, requests=400, rate=2000.0, slots=4, seed=5555, baseline=False):
     """Poisson arrivals mixing exact (n ~ U[16,34], U(0,1], d=0.5) and
     approximate (binary n ~ U[40,64], d=0.5, Rasmussen or scaling y=4 z=5,
-    2e5 trials) requests through the request loop."""
+    2e5 trials) requests through the request loop; with `baseline`, the same
+    requests also run one call at a time on one context (the same accuracy
+    policy) for the one-launch-per-request comparison."""
     import threading
 
     rng = np.random.default_rng(seed)
@@ -555,11 +557,26 @@ def serving_secondary(pb, requests=400, rate=2000.0, slots=4, seed=5555):
     first = min(r["t_submit_ms"] for r in resps)
     last = max(r["t_done_ms"] for r in resps)
     dev = sum(r["device_ms"] for r in resps)
-    return {"requests": requests, "offered_rate_per_s": rate, "slots": slots, "ok": ok,
-            "perms_per_s": requests / ((last - first) * 1e-3), "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "mean_device_ms_per_request": dev / requests,
-            "errors": errors,
-            "wall_s": wall}
+    out = {"requests": requests, "offered_rate_per_s": rate, "slots": slots, "ok": ok,
+           "perms_per_s": requests / ((last - first) * 1e-3), "p50_ms": float(np.percentile(lat, 50)),
+           "p99_ms": float(np.percentile(lat, 99)), "mean_device_ms_per_request": dev / requests,
+           "errors": errors,
+           "wall_s": wall}
+    if baseline:
+        eng = pb.Engine(0)
+        t0 = time.perf_counter()
+        for k, A, kw in reqs:
+            if k == pb.PERM_REQ_EXACT_DENSE:
+                eng.exact_dense(A)
+            elif k == pb.PERM_REQ_RASMUSSEN:
+                eng.rasmussen(A, kw["trials"], seed=kw["seed"])
+            else:
+                eng.scaling(A, kw["trials"], 4, 5, seed=kw["seed"])
+        seq = time.perf_counter() - t0
+        eng.close()
+        out["one_call_per_request"] = {"wall_s": seq, "perms_per_s": requests / seq,
+                                       "served_speedup": (requests / ((last - first) * 1e-3)) / (requests / seq)}
+    return out
 
 
 def secondary(pb, eng):

@@ -104,6 +104,13 @@ int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int
  * covers for order n.  Host only (no device): depends on (n, shard, nshards)
  * alone, so ranks on different devices always partition [0, 2^(n-1)). */
 int perm_shard_range(int n, int shard, int nshards, uint64_t* first, uint64_t* last);
+/* The whole-walk value (io->hi, io->lo, io->kernel_ms) assembled from all
+ * shards of perm_exact_dense_shard, given the error estimate and the
+ * context's accuracy policy of perm_exact_dense (see perm_ctx_set_rel_target):
+ * io is updated in place, its kernel_ms grows by any cross-check or
+ * double-double launch.  No counterpart in the reference (which checks no
+ * accuracy). */
+int perm_exact_dense_refine(perm_ctx* ctx, const void* mat, int n, int dtype, perm_result* io);
 
 /* SkipPer on CRS (rptrs, cols, rvals) + CCS (cptrs, rows, cvals) of an n x n
  * matrix, 1 <= n <= 64; only the stored entries are used (x0 from the CRS row

@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
-    "perm_exact_dense_resident", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target",
+    "perm_exact_dense_resident", "perm_exact_dense_refine", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target",
     "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
@@ -121,6 +121,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_matrix_create_dense": (i, [_P, _P, i, i, ctypes.POINTER(_P)]),
         "perm_matrix_destroy": (None, [_P, _P]),
         "perm_exact_dense_resident": (i, [_P, _P, ctypes.POINTER(PermResult)]),
+        "perm_exact_dense_refine": (i, [_P, _P, i, i, ctypes.POINTER(PermResult)]),
         "perm_exact_dense_tc_rounds": (i, [_P, _P, i, i, u64, u64, ctypes.POINTER(PermResult)]),
         "perm_approx_rasmussen": (i, [_P, _P, i, i, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
         "perm_approx_scaling": (i, [_P, _P, i, i, i64, i, i, u64, _P, ctypes.POINTER(PermEstimate)]),
@@ -247,6 +248,15 @@ class Engine:
                                                      ctypes.byref(r)))
         else:
             self._check(self.lib.perm_exact_dense(self.ctx, _ptr(a), a.shape[0], dt, ctypes.byref(r)))
+        return _exact(r)
+
+    def refine_dense(self, mat, hi: float, lo: float, kernel_ms: float = 0.0) -> ExactResult:
+        """Accuracy policy and error estimate for a whole-walk value assembled
+        from shards (perm_exact_dense_refine)."""
+        a, dt = _as_matrix(mat)
+        r = PermResult()
+        r.hi, r.lo, r.kernel_ms = hi, lo, kernel_ms
+        self._check(self.lib.perm_exact_dense_refine(self.ctx, _ptr(a), a.shape[0], dt, ctypes.byref(r)))
         return _exact(r)
 
     def exact_dense_shard(self, mat, shard: int, nshards: int, variant: int = 0) -> ExactResult:

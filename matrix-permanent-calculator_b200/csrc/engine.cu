@@ -851,6 +851,23 @@ extern "C" int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dt
   return refine_result(ctx, mat, n, dtype, op, variant == 0 && ctx->rel_target > 0, out);
 }
 
+extern "C" int perm_exact_dense_refine(perm_ctx* ctx, const void* mat, int n, int dtype, perm_result* io) {
+  int rc = check_dense_args(ctx, mat, n, dtype, io);
+  if (rc) return rc;
+  DenseOperand op;
+  if ((rc = build_operand(ctx, mat, n, dtype, 0, &op))) return rc;
+  if (op.variant == PERM_KERNEL_DENSE_TC) op.variant = PERM_KERNEL_DENSE_INT;  // what the shards ran
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  io->value = io->hi + io->lo;
+  io->n = n;
+  io->kernel = op.variant;
+  io->steps = io->total_steps = std::ldexp(1.0, n - 1);
+  io->abs_term_sum = io->rel_error_estimate = 0;
+  if (ctx->rel_target < 0) return PERM_OK;
+  return refine_result(ctx, mat, n, dtype, op, ctx->rel_target > 0, io);
+}
+
 extern "C" int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int shard,
                                       int nshards, perm_result* out) {
   return perm_exact_dense_ex(ctx, mat, n, dtype, 0, shard, nshards, out);

@@ -14,7 +14,9 @@
 //  * Exact requests whose Gray walk exceeds `slice_steps` run as several
 //    shard launches (perm_exact_dense_shard) so that one large permanent does
 //    not hold the whole GPU for tens of milliseconds while small requests
-//    wait; shard results are added in double-double.
+//    wait; shard results are added in double-double and the sum gets the
+//    context's accuracy policy (perm_exact_dense_refine), like an unsliced
+//    request.
 //  * Every request gets a status; a failing request (bad size, CUDA error)
 //    fails alone.
 #include <cuda_runtime.h>
@@ -140,6 +142,20 @@ void run_job(perm_server* s, perm_ctx* ctx, Job* j) {
         r.lo = lo - (r.hi - hi);
         r.device_ms = dev;
         r.kernel = pr.kernel;
+        if (rc == PERM_OK && shards > 1) {
+          // the single-shard call applied the accuracy policy itself; a
+          // sliced request gets it on the assembled value
+          pr.hi = r.hi;
+          pr.lo = r.lo;
+          pr.kernel_ms = dev;
+          rc = perm_exact_dense_refine(ctx, a, q.n, PERM_F64, &pr);
+          if (rc == PERM_OK) {
+            r.hi = pr.hi;
+            r.lo = pr.lo;
+            r.device_ms = pr.kernel_ms;
+            r.kernel = pr.kernel;
+          }
+        }
       }
       r.value = r.hi + r.lo;
       r.std_error = 0;

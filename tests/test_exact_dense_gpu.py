@@ -416,3 +416,17 @@ def test_tc_kernel_resident_and_shards(engine, pb):
     parts = [engine.exact_dense_shard(A, s, 3, variant=pb.PERM_KERNEL_DENSE_TC) for s in range(3)]
     assert all(p.kernel == pb.PERM_KERNEL_DENSE_INT for p in parts)
     assert rel_err(pb.dd_sum([(p.hi, p.lo) for p in parts])[0], whole) < 1e-12
+
+
+def test_refine_assembled_shards(engine, pb):
+    """perm_exact_dense_refine gives a value assembled from shards the same
+    estimate and policy as a whole call: within 1e-10 of double-double."""
+    rng = np.random.default_rng(92)
+    A = 1.0 - rng.random((29, 29))
+    parts = [engine.exact_dense_shard(A, s, 4) for s in range(4)]
+    hi, lo = pb.dd_sum([(p.hi, p.lo) for p in parts])
+    r = engine.refine_dense(A, hi, lo, sum(p.kernel_ms for p in parts))
+    d = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_DD).value
+    assert abs(r.value - d) <= 1e-10 * abs(d)
+    assert 0 < r.rel_error_estimate <= 1e-10
+    assert r.kernel_ms >= sum(p.kernel_ms for p in parts)

@@ -573,6 +573,61 @@ def distributed_exact_dense(mat, group=None, engine: Engine | None = None, shard
     return dd_sum((float(g[0]), float(g[1])) for g in gathered)
 
 
+_queue_calls = 0
+
+
+def distributed_exact_dense_dynamic(mat, chunks: int | None = None, group=None, engine: Engine | None = None,
+                                    shard_fn=None, store=None, claims_out: list | None = None
+                                    ) -> tuple[float, float]:
+    """Exact permanent of one matrix over all ranks with a dynamic chunk queue
+    (the reference's hybrid multi-GPU chunk queue, gpu_exact_dense.cu:777-904,
+    restated over torch.distributed ranks instead of host threads).
+
+    The Gray walk is cut into `chunks` device-independent shards
+    (perm_shard_range; default 8 per rank).  Each rank repeatedly claims the
+    next chunk from an atomic counter in the process group's key-value store
+    (`store`, default: the group's rendezvous store) and runs it on its own
+    GPU, so faster or less loaded GPUs take more chunks.  One all-reduce of a
+    chunks x 3 table (claimed flag, hi, lo; each row written by exactly one
+    rank, so the sum is exact) gives every rank all partials, which are added
+    in chunk order (double-double): the result does not depend on who ran
+    what.  `shard_fn(mat, chunk, chunks) -> (hi, lo)` replaces the device
+    call (host-logic tests without a GPU); `claims_out` receives this rank's
+    chunk ids."""
+    import torch
+    import torch.distributed as dist
+
+    global _queue_calls
+    world = dist.get_world_size(group)
+    chunks = chunks or 8 * world
+    if store is None:
+        store = dist.distributed_c10d._get_default_store()
+    key = f"perm_b200_queue_{_queue_calls}"  # every rank makes the same calls in the same order
+    _queue_calls += 1
+    eng = None if shard_fn is not None else (engine or default_engine())
+    table = torch.zeros((chunks, 3), dtype=torch.float64)
+    while True:
+        c = int(store.add(key, 1)) - 1
+        if c >= chunks:
+            break
+        if shard_fn is None:
+            r = eng.exact_dense_shard(mat, c, chunks)
+            hi, lo = r.hi, r.lo
+        else:
+            hi, lo = shard_fn(mat, c, chunks)
+        table[c, 0], table[c, 1], table[c, 2] = 1.0, hi, lo
+        if claims_out is not None:
+            claims_out.append(c)
+    backend = dist.get_backend(group)
+    if backend == "nccl":
+        table = table.to(f"cuda:{torch.cuda.current_device()}")
+    dist.all_reduce(table, op=dist.ReduceOp.SUM, group=group)
+    table = table.cpu()
+    if not bool((table[:, 0] == 1.0).all()):
+        raise PermError(PERM_EINVAL, "chunk queue: a chunk was not computed exactly once")
+    return dd_sum((float(table[c, 1]), float(table[c, 2])) for c in range(chunks))
+
+
 # ---- reference-named entry points (argument meaning as in the reference) ------
 _default_engine: Engine | None = None
 

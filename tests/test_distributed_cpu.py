@@ -77,3 +77,60 @@ def test_gloo_two_ranks_recombine(pb, orc, tmp_path, n):
     for r in range(2):
         hi, lo = np.load(f"{out}.{r}.npy")
         assert abs((hi + lo) - want) <= 1e-14 * abs(want)
+
+
+def _rank_dynamic(rank, world, port, store_port, A, out_path):
+    import sys
+    import time
+    from datetime import timedelta
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    sys.path.insert(0, str(root / "tests"))
+    sys.path.insert(0, str(root / "oracle"))
+    import torch.distributed as dist
+    from conftest import load_package
+    from oracle import Oracle
+
+    pb = load_package()
+    orc = Oracle()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    store = dist.TCPStore("127.0.0.1", store_port, world, rank == 0, timeout=timedelta(seconds=60))
+    n = A.shape[0]
+    factor = 2.0 if n & 1 else -2.0
+
+    def shard_fn(mat, c, chunks):  # CPU stand-in; rank 0 is made slower
+        if rank == 0:
+            time.sleep(0.05)
+        a, b = pb.shard_range(n, c, chunks)
+        hi, lo = orc.ryser_dd_range(mat, a, b, threads=1)
+        return hi * factor, lo * factor
+
+    claims = []
+    hi, lo = pb.distributed_exact_dense_dynamic(A, chunks=24, shard_fn=shard_fn, store=store, claims_out=claims)
+    # a second call uses a fresh queue
+    hi2, lo2 = pb.distributed_exact_dense_dynamic(A, chunks=5, shard_fn=shard_fn, store=store)
+    dist.barrier()
+    dist.destroy_process_group()
+    np.save(f"{out_path}.{rank}.npy", np.array([hi, lo, len(claims), hi2, lo2]))
+
+
+def test_gloo_dynamic_chunk_queue(pb, orc, tmp_path):
+    """Two gloo ranks share a chunk queue: every chunk runs exactly once, the
+    slower rank claims fewer chunks, and both ranks get the same permanent
+    (independent of who ran what)."""
+    rng = np.random.default_rng(5)
+    A = rng.random((15, 15))
+    port, store_port = _free_port(), _free_port()
+    out = str(tmp_path / "dyn")
+    mp.start_processes(_rank_dynamic, args=(2, port, store_port, A, out), nprocs=2, join=True,
+                       start_method="spawn")
+    want = sum(orc.perm_dd(A))
+    r0, r1 = np.load(f"{out}.0.npy"), np.load(f"{out}.1.npy")
+    for r in (r0, r1):
+        assert abs((r[0] + r[1]) - want) <= 1e-14 * abs(want)
+        assert abs((r[3] + r[4]) - want) <= 1e-14 * abs(want)
+    assert r0[0] == r1[0] and r0[1] == r1[1]
+    assert r0[2] + r1[2] == 24 and r1[2] > r0[2]

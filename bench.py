@@ -626,7 +626,9 @@ def secondary(pb, eng):
     t = time.perf_counter()
     f = eng.scaling(C, 200000, 4, 5, seed=2)
     f_wall = time.perf_counter() - t
-    out["mc_n64_binary_2e5_trials"] = {"rasmussen_ms": e.kernel_ms, "rasmussen_call_s": e_wall,
+    out["mc_n64_binary_2e5_trials"] = {"rasmussen_trials_per_s": 200000 / (e.kernel_ms * 1e-3),
+                                       "scaling_trials_per_s": 200000 / (f.kernel_ms * 1e-3),
+                                       "rasmussen_ms": e.kernel_ms, "rasmussen_call_s": e_wall,
                                        "rasmussen_mean": e.mean, "rasmussen_rel_se": e.std_error / e.mean,
                                        "scaling_ms": f.kernel_ms, "scaling_call_s": f_wall, "scaling_mean": f.mean,
                                        "scaling_rel_se": f.std_error / f.mean}

@@ -616,6 +616,8 @@ static int dense_launch(perm_ctx* ctx, const DenseOperand& op, const void* d_ima
     args.colA = static_cast<const double*>(d_image);
     args.np = (n + 1) & ~1;
     args.m = p.m;
+    // re-anchor X every >= 2^11 Gray steps (orders <= kAnchorMaxN)
+    args.seg_blocks = p.m >= 11 ? 1 : (1ull << (11 - p.m));
     args.block0 = p.block0;
     args.nblocks = p.nblocks;
     args.partials = ctx->partials;

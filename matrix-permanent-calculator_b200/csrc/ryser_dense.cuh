@@ -34,7 +34,16 @@ struct DenseArgs {
   unsigned* ticket;    // zero-initialised completion counter
   double* out;         // out[0], out[1] = permanent as (hi, lo)
   int* err;            // set to 1 if the shared-memory staging timed out
+  uint64_t seg_blocks; // orders <= kAnchorMaxN: X is recomputed from x0 every seg_blocks
+                       // aligned blocks (0: once per thread range)
 };
+
+// Orders up to which the FP64-X walk re-anchors X (recomputes it from x0) at
+// every segment: the rounding errors of the X updates then accumulate over at
+// most one segment (>= 2^11 steps) instead of a whole thread range (up to
+// 2^25 steps), which is what dominates the FP64-X error on real matrices.
+// Above this order the extra code makes the compiler spill inside the walk.
+constexpr int kAnchorMaxN = 35;
 
 __device__ __forceinline__ double2 lds2(const double* p) {
   double2 v;
@@ -87,6 +96,39 @@ __device__ __forceinline__ double step(double (&x)[N], const double* col, double
   if (N == 2) return p0 * p1;
   if (N == 3) return (p0 * p1) * p2;
   return (p0 * p1) * (p2 * p3);
+}
+
+// X for Gray index i recomputed from x0 (volatile shared loads: nothing is
+// hoisted into registers across the walk)
+template <int N>
+__device__ __forceinline__ void anchor_x(double (&x)[N], const double* x0, const double* sA, int np, uint64_t i) {
+  const uint64_t g = i ^ (i >> 1);
+#pragma unroll
+  for (int j = 0; j < N; j += 2) {
+    if (j + 1 < N) {
+      const double2 v = lds2(x0 + j);
+      x[j] = v.x;
+      x[j + 1] = v.y;
+    } else {
+      x[j] = lds1(x0 + j);
+    }
+  }
+#pragma unroll 1
+  for (int k = 0; k < N - 1; k++) {
+    if ((g >> k) & 1) {
+      const double* c = sA + k * np;
+#pragma unroll
+      for (int j = 0; j < N; j += 2) {
+        if (j + 1 < N) {
+          const double2 v = lds2(c + j);
+          x[j] += v.x;
+          x[j + 1] += v.y;
+        } else {
+          x[j] += lds1(c + j);
+        }
+      }
+    }
+  }
 }
 
 template <int N>
@@ -155,6 +197,49 @@ __global__ void __launch_bounds__(128) ryser_dense_kernel(DenseArgs args) {
         for (int j = 0; j < N; j++) x[j] = fma(s, sA[k * np + j], x[j]);
         double p = prod_only<N>(x);
         acc.add((i & 1) ? -p : p);
+      }
+    }
+  } else if (N <= kAnchorMaxN && b1 > b0) {
+    // segments of seg_blocks aligned blocks, each from a freshly computed X
+    const uint64_t K = args.seg_blocks ? args.seg_blocks : b1 - b0;
+    const double* c0 = sA;
+    const double* c1 = sA + np;
+    const double* c2 = sA + 2 * np;
+#pragma unroll 1
+    for (uint64_t blk = b0; blk < b1; blk += K) {
+      const uint64_t nb = b1 - blk < K ? b1 - blk : K;
+      const uint64_t s0 = (args.block0 + blk) << args.m;
+      double x[N];
+      anchor_x<N>(x, sX0, sA, np, s0);
+      acc.add(prod_only<N>(x));  // index s0 is even: sign +
+      const uint64_t groups = (nb << args.m) >> 3;
+      uint64_t base = s0;
+#pragma unroll 1
+      for (uint64_t gi = 0; gi + 1 < groups; gi++, base += 8) {
+        const double s4 = ((base >> 3) & 1) ? -1.0 : 1.0;
+        const uint64_t i8 = base + 8;
+        const int k8 = __ffsll((long long)i8) - 1;
+        const double s8 = ((i8 >> (k8 + 1)) & 1) ? -1.0 : 1.0;
+        double t1 = step<N, +1>(x, c0, 0.0);
+        double t2 = step<N, +1>(x, c1, 0.0);
+        double t3 = step<N, -1>(x, c0, 0.0);
+        double t4 = step<N, 0>(x, c2, s4);
+        double t5 = step<N, +1>(x, c0, 0.0);
+        double t6 = step<N, -1>(x, c1, 0.0);
+        double t7 = step<N, -1>(x, c0, 0.0);
+        double t8 = step<N, 0>(x, sA + k8 * np, s8);
+        acc.add(((t2 - t1) + (t4 - t3)) + ((t6 - t5) + (t8 - t7)));
+      }
+      {  // last group of the segment: seven steps (the next index starts the next segment)
+        const double s4 = ((base >> 3) & 1) ? -1.0 : 1.0;
+        double t1 = step<N, +1>(x, c0, 0.0);
+        double t2 = step<N, +1>(x, c1, 0.0);
+        double t3 = step<N, -1>(x, c0, 0.0);
+        double t4 = step<N, 0>(x, c2, s4);
+        double t5 = step<N, +1>(x, c0, 0.0);
+        double t6 = step<N, -1>(x, c1, 0.0);
+        double t7 = step<N, -1>(x, c0, 0.0);
+        acc.add(((t2 - t1) + (t4 - t3)) + ((t6 - t5) - t7));
       }
     }
   } else if (b1 > b0) {

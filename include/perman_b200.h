@@ -51,6 +51,8 @@ extern "C" {
 #define PERM_KERNEL_DENSE_DD 4  /* double-double Gray-code Ryser (orders <= 40) */
 #define PERM_KERNEL_DENSE_TC 5  /* tensor-core row sums (kind::i8) + int32 products:
                                    integer matrices, |a| <= 63, orders 16..64 */
+#define PERM_KERNEL_DENSE_SPLIT 6 /* split-X Gray-code Ryser: exact coarse row sums
+                                     plus a small remainder, orders 4..40 */
 
 /* Limits of this build. */
 #define PERM_MAX_EXACT_N 64  /* Gray indices are 64-bit                 */

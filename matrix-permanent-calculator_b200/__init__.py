@@ -31,6 +31,7 @@ PERM_OK, PERM_EINVAL, PERM_ECUDA, PERM_ENOMEM, PERM_EUNSUPPORTED, PERM_ETIMEOUT,
 PERM_F64, PERM_F32, PERM_I32 = 0, 1, 2
 PERM_KERNEL_DENSE, PERM_KERNEL_SKIPPER, PERM_KERNEL_DENSE_INT, PERM_KERNEL_DENSE_DD = 1, 2, 3, 4
 PERM_KERNEL_DENSE_TC = 5
+PERM_KERNEL_DENSE_SPLIT = 6
 MAX_EXACT_N = 64
 MAX_MC_N = 64
 MAX_MC_SPARSE_N = 2047
@@ -240,7 +241,8 @@ class Engine:
     # ---- exact ----
     def exact_dense(self, mat, variant: int = 0) -> ExactResult:
         """Dense Ryser; variant 0 = automatic, PERM_KERNEL_DENSE = FP64 X, PERM_KERNEL_DENSE_INT = int32 X,
-        PERM_KERNEL_DENSE_TC = tensor-core row sums, PERM_KERNEL_DENSE_DD = double-double."""
+        PERM_KERNEL_DENSE_TC = tensor-core row sums, PERM_KERNEL_DENSE_DD = double-double,
+        PERM_KERNEL_DENSE_SPLIT = split X (exact coarse row sums, orders 4..40)."""
         a, dt = _as_matrix(mat)
         r = PermResult()
         if variant:

@@ -35,6 +35,7 @@
 #include "perman_common.cuh"
 #include "ryser_dense.cuh"
 #include "ryser_dense_dd.cuh"
+#include "ryser_dense_split.cuh"
 #include "ryser_dense_tc.cuh"
 #include "ryser_dense_int.cuh"
 #include "skipper.h"
@@ -52,6 +53,7 @@ const void* dense_int_kernel_g5(int n);
 const void* dense_int_kernel_g6(int n);
 
 const void* dense_dd_kernel(int n);
+const void* dense_split_kernel(int n);
 
 const void* dense_tc_kernel_g3(int n);
 const void* dense_tc_kernel_g4(int n);
@@ -186,11 +188,12 @@ struct perm_ctx {
   size_t h_stage_cap = 0;
   double* d_trials = nullptr;
   size_t d_trials_cap = 0;
-  int dense_occ[12][PERM_MAX_EXACT_N + 1] = {};  // [0]: FP64-X, [G]: int32-X, [7]: dd, [8 + G - 3]: tensor core
+  int dense_occ[13][PERM_MAX_EXACT_N + 1] = {};  // [0]: FP64-X, [G]: int32-X, [7]: dd, [8 + G - 3]: tensor core, [12]: split X
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
-  double* d_est = nullptr;                       // sample-kernel accumulator
+  double* d_est = nullptr;                       // sample-kernel / split-walk moment accumulator
+  double split_m1 = 0, split_m2 = 0;             // last split-X walk: sum |term|, sum term^2
   int batch_occ = 0;
   std::string err;
   std::mutex mu;
@@ -436,12 +439,65 @@ static bool tc_eligible(const std::vector<double>& a, int n) {
   return true;
 }
 
+// Split-X operand (ryser_dense_split.cuh): every entry a = ah + al with ah on
+// the grid 2^-q, q chosen so that partial row sums of coarse parts stay below
+// 2^(52 - q) and are exact in FP64; x0 likewise, from its double-double value.
+// Image: [ah column-major, stride np][al][x0h][x0l].
+static int build_split_operand(perm_ctx* ctx, const std::vector<double>& a, int n, DenseOperand* op) {
+  if (n < 4 || n > 40) return fail(ctx, PERM_EUNSUPPORTED, "split-X kernel covers orders 4..40 (got %d)", n);
+  double rowabs = 0.0;
+  for (int j = 0; j < n; j++) {
+    double r = 0.0;
+    for (int k = 0; k < n; k++) r += std::fabs(a[(size_t)j * n + k]);
+    rowabs = std::max(rowabs, r);
+  }
+  if (!(rowabs > 0.0) || !std::isfinite(rowabs)) rowabs = 1.0;
+  const int E = (int)std::ceil(std::log2(2.0 * rowabs * (1.0 + 1e-12) + 1.0));  // |coarse sums| < 2^E
+  const int q = 51 - E;
+  auto coarse = [q](double v) { return std::ldexp(std::nearbyint(std::ldexp(v, q)), -q); };
+  const int np = (n + 1) & ~1;
+  op->n = n;
+  op->variant = PERM_KERNEL_DENSE_SPLIT;
+  op->group = 0;
+  op->image.assign(sizeof(double) * (2 * (size_t)n * np + 2 * (size_t)np), 0);
+  double* img = reinterpret_cast<double*>(op->image.data());
+  double* H = img;
+  double* L = img + (size_t)n * np;
+  double* X0h = L + (size_t)n * np;
+  double* X0l = X0h + np;
+  for (int k = 0; k < n; k++)
+    for (int j = 0; j < n; j++) {
+      const double v = a[(size_t)j * n + k], h = coarse(v);
+      H[(size_t)k * np + j] = h;
+      L[(size_t)k * np + j] = v - h;  // exact
+    }
+  for (int j = 0; j < n; j++) {
+    // x0 = a[j][n-1] - rowsum_j / 2 in double-double
+    double hi = 0.0, lo = 0.0;
+    for (int k = 0; k < n; k++) {
+      const double v = a[(size_t)j * n + k], sum = hi + v, bb = sum - hi;
+      lo += (hi - (sum - bb)) + (v - bb);
+      hi = sum;
+    }
+    hi *= -0.5;
+    lo *= -0.5;
+    const double v = a[(size_t)j * n + n - 1], sum = hi + v, bb = sum - hi;
+    lo += (hi - (sum - bb)) + (v - bb);
+    hi = sum;
+    const double h = coarse(hi);
+    X0h[j] = h;
+    X0l[j] = (hi - h) + lo;
+  }
+  return PERM_OK;
+}
+
 static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, DenseOperand* op) {
   std::vector<double> a((size_t)n * n);
   for (size_t i = 0; i < a.size(); i++) a[i] = elem(mat, dtype, i);
   op->n = n;
   const int pref = variant == 0 && n <= PERM_MAX_EXACT_N ? ctx->dense_pref[n] : 0;
   const bool prefer_fp64 = pref == PERM_KERNEL_DENSE;
+  if (variant == PERM_KERNEL_DENSE_SPLIT) return build_split_operand(ctx, a, n, op);
   int G = (variant == PERM_KERNEL_DENSE || variant == PERM_KERNEL_DENSE_DD || prefer_fp64) ? 0 : int_group_size(a, n);
   if (variant == PERM_KERNEL_DENSE_INT && G == 0)
     return fail(ctx, PERM_EUNSUPPORTED,
@@ -488,6 +544,7 @@ static const void* operand_kernel(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
+  if (op.variant == PERM_KERNEL_DENSE_SPLIT) return dense_split_kernel(op.n);
   return dense_kernel(op.n);
 }
 static int operand_threads(const DenseOperand& op) { return op.variant == PERM_KERNEL_DENSE_TC ? kTcThreads : 128; }
@@ -495,6 +552,7 @@ static size_t operand_smem(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_smem_bytes(op.n);
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_smem_bytes(op.n);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_smem_bytes(op.n);
+  if (op.variant == PERM_KERNEL_DENSE_SPLIT) return dense_split_smem_bytes(op.n);
   return dense_smem_bytes(op.n);
 }
 
@@ -535,7 +593,8 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
   if (!fn) return fail(ctx, PERM_EUNSUPPORTED, "dense exact order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
   int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? op.group
                                  : op.variant == PERM_KERNEL_DENSE_DD ? 7
-                                 : op.variant == PERM_KERNEL_DENSE_TC ? 8 + op.group - 3 : 0][n];
+                                 : op.variant == PERM_KERNEL_DENSE_TC ? 8 + op.group - 3
+                                 : op.variant == PERM_KERNEL_DENSE_SPLIT ? 12 : 0][n];
   if (!occ_slot) {
     int rc = allow_smem(ctx, fn, operand_smem(op));
     if (rc) return rc;
@@ -596,6 +655,21 @@ static int dense_launch(perm_ctx* ctx, const DenseOperand& op, const void* d_ima
     void* kargs[] = {&args};
     CU(ctx, cudaLaunchKernel(operand_kernel(op), dim3(p.grid), dim3(kTcThreads), kargs, operand_smem(op),
                              ctx->stream));
+  } else if (op.variant == PERM_KERNEL_DENSE_SPLIT) {
+    DenseSplitArgs args;
+    args.img = static_cast<const double*>(d_image);
+    args.np = (n + 1) & ~1;
+    args.m = p.m;
+    args.block0 = p.block0;
+    args.nblocks = p.nblocks;
+    args.partials = ctx->partials;
+    args.ticket = ctx->ticket;
+    args.out = ctx->d_out;
+    args.sums = ctx->d_est;
+    args.err = ctx->d_err;
+    void* kargs[] = {&args};
+    CU(ctx, cudaMemsetAsync(ctx->d_est, 0, 2 * sizeof(double), ctx->stream));
+    CU(ctx, cudaLaunchKernel(operand_kernel(op), dim3(p.grid), dim3(128), kargs, operand_smem(op), ctx->stream));
   } else if (op.variant == PERM_KERNEL_DENSE_INT) {
     DenseIntArgs args;
     const int np4 = (n + 3) & ~3;
@@ -632,8 +706,14 @@ static int dense_launch(perm_ctx* ctx, const DenseOperand& op, const void* d_ima
 }
 
 static int dense_collect(perm_ctx* ctx, const DenseOperand& op, const DensePlan& p, perm_result* out) {
+  if (op.variant == PERM_KERNEL_DENSE_SPLIT)
+    CU(ctx, cudaMemcpyAsync(ctx->h_out + 12, ctx->d_est, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   int rc = finish_and_read(ctx, 2);
   if (rc != PERM_OK) return rc;
+  if (op.variant == PERM_KERNEL_DENSE_SPLIT) {
+    ctx->split_m1 = ctx->h_out[12] * 2.0;  // |factor| = 2
+    ctx->split_m2 = ctx->h_out[13] * 4.0;
+  }
   float ms = 0;
   CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   const int n = op.n;
@@ -660,7 +740,7 @@ static int check_dense_args(perm_ctx* ctx, const void* mat, int n, int dtype, co
 
 static int check_variant(perm_ctx* ctx, int variant) {
   if (variant != 0 && variant != PERM_KERNEL_DENSE && variant != PERM_KERNEL_DENSE_INT &&
-      variant != PERM_KERNEL_DENSE_DD && variant != PERM_KERNEL_DENSE_TC)
+      variant != PERM_KERNEL_DENSE_DD && variant != PERM_KERNEL_DENSE_TC && variant != PERM_KERNEL_DENSE_SPLIT)
     return fail(ctx, PERM_EINVAL, "unknown dense kernel variant %d", variant);
   return PERM_OK;
 }
@@ -678,8 +758,33 @@ static int check_variant(perm_ctx* ctx, int variant) {
 //    so it is only used together with an independent second evaluation;
 //  * double-double: (4n + 32) u^2 S1 / |perm|.
 struct ErrEstimate {
-  double s1 = 0, worst = 0, random = 0;
+  double s1 = 0, s2 = 0, worst = 0, random = 0;
 };
+
+// bounds of `variant`'s rounding error from the sampled sums of |term| and term^2
+static void error_bounds(int variant, int group, int n, double value, ErrEstimate* e) {
+  const double u = std::ldexp(1.0, -53);
+  const double av = std::fabs(value), s1 = e->s1, s2 = e->s2;
+  if (av == 0.0) {
+    e->worst = e->random = s1 > 0 ? INFINITY : 0.0;
+    return;
+  }
+  if (variant == PERM_KERNEL_DENSE_DD) {
+    e->worst = e->random = (4.0 * n + 32.0) * u * u * s1 / av;
+  } else if (variant == PERM_KERNEL_DENSE_SPLIT) {
+    // exact coarse X: one combine per entry and n - 1 product roundings, each
+    // a function of the subset alone, so independent from term to term
+    e->worst = (2.0 * n + 16.0) * u * s1 / av;
+    e->random = 4.0 * u * std::sqrt(2.0 * n / 3.0) * std::sqrt(s2) / av;
+  } else if (variant == PERM_KERNEL_DENSE_INT || variant == PERM_KERNEL_DENSE_TC) {
+    const double groups = std::ceil((double)n / group);
+    e->worst = (groups + 16.0) * u * s1 / av;
+    e->random = 4.0 * u * std::sqrt(std::max(1.0, groups - 1.0) / 3.0) * std::sqrt(s2) / av;
+  } else {
+    e->worst = (2.0 * n + 16.0) * u * s1 / av;
+    e->random = 4.0 * u * std::sqrt(2.0 * n / 3.0) * std::sqrt(s2) / av;
+  }
+}
 
 static int estimate_error(perm_ctx* ctx, const void* d_col_fp64, int n, const DenseOperand& op, double value,
                           ErrEstimate* e) {
@@ -695,25 +800,9 @@ static int estimate_error(perm_ctx* ctx, const void* d_col_fp64, int n, const De
   CU(ctx, cudaMemcpyAsync(ctx->h_out + 12, ctx->d_est, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CU(ctx, cudaStreamSynchronize(ctx->stream));
   const double scale = (double)total / (double)samples;
-  const double s1 = ctx->h_out[12] * scale * 2.0;       // |factor| = 2
-  const double s2 = ctx->h_out[13] * scale * 4.0;
-  const double u = std::ldexp(1.0, -53);
-  const double av = std::fabs(value);
-  e->s1 = s1;
-  if (av == 0.0) {
-    e->worst = e->random = s1 > 0 ? INFINITY : 0.0;
-    return PERM_OK;
-  }
-  if (op.variant == PERM_KERNEL_DENSE_DD) {
-    e->worst = e->random = (4.0 * n + 32.0) * u * u * s1 / av;
-  } else if (op.variant == PERM_KERNEL_DENSE_INT || op.variant == PERM_KERNEL_DENSE_TC) {
-    const double groups = std::ceil((double)n / op.group);
-    e->worst = (groups + 16.0) * u * s1 / av;
-    e->random = 4.0 * u * std::sqrt(std::max(1.0, groups - 1.0) / 3.0) * std::sqrt(s2) / av;
-  } else {
-    e->worst = (2.0 * n + 16.0) * u * s1 / av;
-    e->random = 4.0 * u * std::sqrt(2.0 * n / 3.0) * std::sqrt(s2) / av;
-  }
+  e->s1 = ctx->h_out[12] * scale * 2.0;  // |factor| = 2
+  e->s2 = ctx->h_out[13] * scale * 4.0;
+  error_bounds(op.variant, op.group, n, value, e);
   return PERM_OK;
 }
 
@@ -774,7 +863,11 @@ static bool has_perfect_matching(const void* mat, int n, int dtype) {
 //     matrices, so B's roundings are independent of A's.  Keep when
 //     max(independent-rounding estimate, 16 |perm(A) - perm(B)/3| / |perm(A)|)
 //     meets the target;
-//  4. otherwise recompute in double-double (orders <= 40).
+//  4. the same cross-check with the split-X kernel on A and B (orders 4..40),
+//     whose per-term roundings are independent;
+//  5. otherwise recompute in double-double (orders <= 40).
+// Steps 3 and 4 are skipped when their independent-rounding estimate alone
+// misses the target.
 // Context lock held.
 static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const DenseOperand& op, bool policy,
                          perm_result* out) {
@@ -784,25 +877,33 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
     out->abs_term_sum = out->rel_error_estimate = 0.0;
     return PERM_OK;
   }
-  // the estimate samples an FP64 column image; an int32 operand is replaced by one
+  // the estimate samples an FP64 column image; an int32 or split operand is replaced by one
   DenseOperand f;
   const DenseOperand* fp = &op;
-  if (op.variant == PERM_KERNEL_DENSE_INT || op.variant == PERM_KERNEL_DENSE_TC) {
+  if (op.variant == PERM_KERNEL_DENSE_INT || op.variant == PERM_KERNEL_DENSE_TC ||
+      op.variant == PERM_KERNEL_DENSE_SPLIT) {
     if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE, &f))) return rc;
     fp = &f;
   }
   if ((rc = stage_operand(ctx, *fp))) return rc;
   ErrEstimate e;
   if ((rc = estimate_error(ctx, ctx->d_stage, n, op, out->value, &e))) return rc;
+  if (op.variant == PERM_KERNEL_DENSE_SPLIT && out->steps == out->total_steps) {
+    // the split walk summed its own |terms| and terms^2: exact moments
+    e.s1 = ctx->split_m1;
+    e.s2 = ctx->split_m2;
+    error_bounds(op.variant, 0, n, out->value, &e);
+  }
   out->abs_term_sum = e.s1;
   out->rel_error_estimate = e.worst;
   const double target = ctx->rel_target;
   if (!policy || e.worst <= target || op.variant == PERM_KERNEL_DENSE_DD) return PERM_OK;
-  if (out->value != 0.0) {
-    std::vector<double> b((size_t)n * n);
-    for (int i2 = 0; i2 < n; i2++)
-      for (int j2 = 0; j2 < n; j2++)
-        b[(size_t)i2 * n + j2] = elem(mat, dtype, (size_t)j2 * n + i2) * (i2 == 0 ? 3.0 : 1.0);
+  std::vector<double> b((size_t)n * n);
+  for (int i2 = 0; i2 < n; i2++)
+    for (int j2 = 0; j2 < n; j2++)
+      b[(size_t)i2 * n + j2] = elem(mat, dtype, (size_t)j2 * n + i2) * (i2 == 0 ? 3.0 : 1.0);
+  // the cross-check's estimate is at least the independent-rounding one
+  if (out->value != 0.0 && e.random <= target) {
     DenseOperand t;
     perm_result rt;
     if ((rc = build_operand(ctx, b.data(), n, PERM_F64, 0, &t))) return rc;
@@ -813,6 +914,35 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
     if (est <= target) {
       out->rel_error_estimate = est;
       return PERM_OK;
+    }
+  }
+  // split-X walks of A and B: independent per-term roundings; A's walk also
+  // returns the exact moments of its terms, and B runs only if the estimate
+  // from those can meet the target
+  if (n >= 4 && n <= 40 && out->value != 0.0) {
+    DenseOperand sa, sb;
+    perm_result ra, rb;
+    if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE_SPLIT, &sa))) return rc;
+    if ((rc = run_whole(ctx, sa, &ra))) return rc;
+    out->kernel_ms += ra.kernel_ms;
+    ErrEstimate es;
+    es.s1 = ctx->split_m1;
+    es.s2 = ctx->split_m2;
+    error_bounds(PERM_KERNEL_DENSE_SPLIT, 0, n, ra.value, &es);
+    if (ra.value != 0.0 && es.random <= target) {
+      if ((rc = build_operand(ctx, b.data(), n, PERM_F64, PERM_KERNEL_DENSE_SPLIT, &sb))) return rc;
+      if ((rc = run_whole(ctx, sb, &rb))) return rc;
+      out->kernel_ms += rb.kernel_ms;
+      const double diff = std::fabs(ra.value - rb.value / 3.0) / std::fabs(ra.value);
+      const double est = std::max(es.random, 16.0 * diff);
+      if (est <= target) {
+        const double ms = out->kernel_ms;
+        *out = ra;
+        out->kernel_ms = ms;
+        out->abs_term_sum = es.s1;
+        out->rel_error_estimate = est;
+        return PERM_OK;
+      }
     }
   }
   if (n > 40) return PERM_OK;  // no double-double kernel above order 40: keep the bound

@@ -265,7 +265,7 @@ def test_fp64_error_grows_and_double_double_fixes_it(engine, pb):
         if auto.kernel == pb.PERM_KERNEL_DENSE_DD:
             assert auto.value == d.value
         else:
-            assert auto.kernel == pb.PERM_KERNEL_DENSE
+            assert auto.kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_SPLIT)
             assert abs(auto.value - d.value) / abs(d.value) <= auto.rel_error_estimate <= 1e-10
 
 
@@ -430,3 +430,96 @@ def test_refine_assembled_shards(engine, pb):
     assert abs(r.value - d) <= 1e-10 * abs(d)
     assert 0 < r.rel_error_estimate <= 1e-10
     assert r.kernel_ms >= sum(p.kernel_ms for p in parts)
+
+
+# ---- split-X kernel ---------------------------------------------------------------------
+
+@pytest.mark.parametrize("n", [4, 5, 9, 12, 19, 24])
+def test_split_kernel_vs_oracle(engine, orc, pb, n):
+    rng = np.random.default_rng(950 + n)
+    for kind in ("real", "signed", "wide"):
+        if kind == "real":
+            A = 1.0 - rng.random((n, n))
+        elif kind == "signed":
+            A = rng.standard_normal((n, n))
+        else:  # entries over many binades: the small ones live mostly in the remainder part;
+            # Ryser's terms cancel heavily here, so only the estimate is checked
+            A = rng.random((n, n)) * np.exp2(rng.integers(-30, 4, (n, n)))
+        r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SPLIT)
+        assert r.kernel == pb.PERM_KERNEL_DENSE_SPLIT
+        hi, lo = orc.perm_dd(A)
+        actual = abs(r.value - hi - lo) / abs(hi)
+        assert 0 < r.rel_error_estimate and actual <= r.rel_error_estimate, (kind, actual, r.rel_error_estimate)
+        if kind == "real":
+            assert actual <= 1e-13, (kind, actual)
+
+
+def test_split_kernel_integer_and_binary_inputs(engine, orc, pb):
+    rng = np.random.default_rng(960)
+    for A in (bernoulli(rng, 21, 0.5), rng.integers(-3, 4, (18, 18)).astype(float), np.ones((13, 13))):
+        r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SPLIT)
+        exact = orc.perm_exact_int(A)[0]
+        assert abs(r.value - exact) <= max(r.rel_error_estimate * abs(exact), 2.0 ** -52 * abs(exact))
+
+
+@pytest.mark.parametrize("n", [30, 34])
+def test_split_kernel_vs_double_double(engine, pb, n):
+    """Positive real matrices, where the FP64-X walk's correlated roundings
+    reach 1e-10..1e-9: the split-X result stays far inside the target."""
+    rng = np.random.default_rng(970 + n)
+    A = 1.0 - rng.random((n, n))
+    s = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SPLIT)
+    d = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_DD)
+    actual = abs(s.value - d.value) / abs(d.value)
+    assert actual <= 1e-11, actual
+    assert actual <= s.rel_error_estimate
+
+
+def test_split_kernel_shards_and_resident(engine, pb):
+    rng = np.random.default_rng(980)
+    A = 1.0 - rng.random((25, 25))
+    whole = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SPLIT)
+    parts = [engine.exact_dense_shard(A, s, 5, variant=pb.PERM_KERNEL_DENSE_SPLIT) for s in range(5)]
+    assert all(p.kernel == pb.PERM_KERNEL_DENSE_SPLIT for p in parts)
+    assert sum(p.steps for p in parts) == 2.0 ** 24
+    assert rel_err(pb.dd_sum([(p.hi, p.lo) for p in parts])[0], whole.value) < 1e-13
+    res = engine.upload_dense(A, variant=pb.PERM_KERNEL_DENSE_SPLIT)
+    try:
+        assert res.run().value == whole.value
+    finally:
+        res.free()
+
+
+def test_split_kernel_order_limits(engine, pb):
+    for n in (3, 41):
+        with pytest.raises(pb.PermError) as ei:
+            engine.exact_dense(np.ones((n, n)), variant=pb.PERM_KERNEL_DENSE_SPLIT)
+        assert ei.value.status == pb.PERM_EUNSUPPORTED
+
+
+@pytest.mark.parametrize("n", [31, 33])
+def test_policy_split_stage_meets_the_target(engine, pb, n):
+    """Where the FP64-X cross-check fails, the split-X stage settles most
+    positive real requests without the double-double rerun; whichever kernel
+    the policy ends on, the value is within 1e-10 of double-double."""
+    rng = np.random.default_rng(990 + n)
+    A = 1.0 - rng.random((n, n))
+    d = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_DD)
+    auto = engine.exact_dense(A)
+    assert auto.kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_SPLIT, pb.PERM_KERNEL_DENSE_DD)
+    assert abs(auto.value - d.value) <= 1e-10 * abs(d.value)
+    assert auto.rel_error_estimate <= 1e-10
+
+
+def test_split_kernel_exact_term_moments(engine, pb):
+    """The split walk sums |term| over its own terms: abs_term_sum is the exact
+    sum of |2 prod_j x_j(S)| over all 2^(n-1) subsets S (numpy, order 13)."""
+    n = 13
+    rng = np.random.default_rng(995)
+    A = rng.standard_normal((n, n))
+    x0 = A[:, n - 1] - A.sum(axis=1) / 2
+    S = ((np.arange(2 ** (n - 1))[:, None] >> np.arange(n - 1)) & 1).astype(float)
+    X = x0[None, :] + S @ A[:, : n - 1].T
+    want = 2.0 * np.abs(np.prod(X, axis=1)).sum()
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SPLIT)
+    assert rel_err(r.abs_term_sum, want) < 1e-12, (r.abs_term_sum, want)

@@ -83,13 +83,13 @@ def test_reference_signature_skipper(pb):
 
 def test_automatic_choice(engine, pb):
     """Real values never give exact zeros, so a register kernel runs (FP64 X,
-    or double-double when the cancellation check asks for it); sparse binary
+    or split X / double-double when the accuracy policy asks for it); sparse binary
     matrices mostly vanish, so SkipPer runs."""
     rng = np.random.default_rng(31)
     A = bernoulli(rng, 26, 0.2) * (1.0 - rng.random((26, 26)))
     c = pb.compress(2, A)
     r = engine.exact_sparse(c["n"], c["rptrs"], c["cols"], c["rvals"], c["cptrs"], c["rows"], c["cvals"])
-    assert r.kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_DD)
+    assert r.kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_SPLIT, pb.PERM_KERNEL_DENSE_DD)
     s = engine.exact_sparse(c["n"], c["rptrs"], c["cols"], c["rvals"], c["cptrs"], c["rows"], c["cvals"],
                             variant=pb.PERM_KERNEL_SKIPPER)
     assert rel_err(r.value, s.value) < TOL

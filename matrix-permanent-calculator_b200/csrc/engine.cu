@@ -89,12 +89,26 @@ static const void* dense_kernel(int n) {
   return nullptr;
 }
 
-// Estimates of sum_i |term(i)| and sum_i term(i)^2 from `samples` Gray
-// indices spread over the walk (index s * stride mod 2^(n-1), stride odd):
-// each thread builds x(i) from scratch in FP64; out[0] and out[1] receive the
-// sample sums of |prod x_j| and of its square.
-__global__ void __launch_bounds__(256) ryser_abs_sample_kernel(const double* colA, int n, int np, uint64_t samples,
-                                                                uint64_t stride, double* out) {
+// Estimates of sum_S |term(S)| and sum_S term(S)^2 over the 2^(n-1) column
+// subsets S of the walk, stratified by |S|: class k holds C(n-1, k) subsets
+// and gets `per_class` threads.  A class no larger than that is enumerated
+// exactly (the r-th k-subset in colex order, by unranking); a
+// larger one is sampled uniformly (Floyd's k-subset algorithm on a
+// splitmix64 stream) and each sample weighted C(n-1, k) / per_class.  Term
+// magnitudes depend strongly on |S| (|S| = 0 is the all-minus subset, often
+// the largest term), so a plain uniform sample of Gray indices either misses
+// the heavy classes or, hitting one, overstates the sums by 2^(n-1)/samples.
+// Each thread builds x(S) from scratch in FP64; out[0] and out[1] receive
+// the weighted sums of |prod x_j| and of its square.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t& state) {
+  uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void __launch_bounds__(256) ryser_abs_sample_kernel(const double* colA, int n, int np, int per_class,
+                                                                uint64_t seed, double* out) {
   __shared__ double sA[64 * 64];
   __shared__ double x0[64];
   __shared__ double red[8], red2[8];
@@ -107,21 +121,54 @@ __global__ void __launch_bounds__(256) ryser_abs_sample_kernel(const double* col
     x0[j] = sA[(n - 1) * np + j] - rs * 0.5;
   }
   __syncthreads();
-  const uint64_t mask = (n >= 2) ? ((1ull << (n - 1)) - 1) : 0;
+  const int m = n - 1;
   double local = 0.0, local2 = 0.0;
-  for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < samples;
-       s += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t i = (s * stride) & mask;
-    const uint64_t g = i ^ (i >> 1);
-    double p = 1.0;
-    for (int j = 0; j < n; j++) {
-      double xj = x0[j];
-      for (int k = 0; k < n - 1; k++)
-        if ((g >> k) & 1) xj += sA[k * np + j];
-      p *= xj;
+  const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = (int)(s / (uint64_t)per_class);
+  const uint64_t r = s % (uint64_t)per_class;
+  if (k <= m) {
+    double c = 1.0;  // C(m, k)
+    for (int t = 1; t <= k; t++) c = c * (double)(m - k + t) / (double)t;
+    uint64_t g = 0;
+    double w = 0.0;
+    if (c <= (double)per_class) {
+      if ((double)r < c) {
+        // colex unranking: the largest element i is the largest with
+        // C(i, kk) <= rank; cb tracks C(i, kk) down the loop (small exact integers)
+        double cb = (k <= m - 1) ? c * (double)(m - k) / (double)m : 0.0;  // C(m - 1, k)
+        uint64_t rank = r;
+        int kk = k;
+        for (int i = m - 1; i >= 0 && kk > 0; i--) {
+          if ((double)rank >= cb) {
+            rank -= (uint64_t)cb;
+            g |= 1ull << i;
+            if (i > 0) cb = cb * (double)kk / (double)i;
+            kk--;
+          } else if (i > 0) {
+            cb = cb * (double)(i - kk) / (double)i;
+          }
+        }
+        w = 1.0;
+      }
+    } else {
+      uint64_t st = seed ^ (s * 0xD1B54A32D192ED03ull);
+      for (int j = m - k; j < m; j++) {
+        const uint32_t t = (uint32_t)(((splitmix64(st) >> 32) * (uint64_t)(j + 1)) >> 32);
+        g |= ((g >> t) & 1) ? (1ull << j) : (1ull << t);
+      }
+      w = c / (double)per_class;
     }
-    local += fabs(p);
-    local2 += p * p;
+    if (w > 0.0) {
+      double p = 1.0;
+      for (int j = 0; j < n; j++) {
+        double xj = x0[j];
+        for (int kk = 0; kk < m; kk++)
+          if ((g >> kk) & 1) xj += sA[kk * np + j];
+        p *= xj;
+      }
+      local = w * fabs(p);
+      local2 = w * p * p;
+    }
   }
   for (int d = 16; d >= 1; d >>= 1) {
     local += __shfl_down_sync(0xffffffffu, local, d);
@@ -757,6 +804,8 @@ static int check_variant(perm_ctx* ctx, int variant) {
 //    sqrt(S2) / |perm|.  Not a bound -- terms with equal values round alike --
 //    so it is only used together with an independent second evaluation;
 //  * double-double: (4n + 32) u^2 S1 / |perm|.
+constexpr int kSamplesPerClass = 8192;  // term-moment sample: threads per subset-size class
+
 struct ErrEstimate {
   double s1 = 0, s2 = 0, worst = 0, random = 0;
 };
@@ -791,17 +840,16 @@ static int estimate_error(perm_ctx* ctx, const void* d_col_fp64, int n, const De
   *e = ErrEstimate();
   if (n < 2) return PERM_OK;
   const int np = (n + 1) & ~1;
-  const uint64_t total = 1ull << (n - 1);
-  const uint64_t samples = std::min<uint64_t>(total, 65536);
+  const int per_class = kSamplesPerClass;
+  const uint64_t threads = (uint64_t)n * per_class;  // classes |S| = 0 .. n-1
   CU(ctx, cudaMemsetAsync(ctx->d_est, 0, 2 * sizeof(double), ctx->stream));
-  ryser_abs_sample_kernel<<<(unsigned)((samples + 255) / 256), 256, 0, ctx->stream>>>(
-      static_cast<const double*>(d_col_fp64), n, np, samples, 0x9E3779B97F4A7C15ull | 1ull, ctx->d_est);
+  ryser_abs_sample_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, ctx->stream>>>(
+      static_cast<const double*>(d_col_fp64), n, np, per_class, 0x243F6A8885A308D3ull, ctx->d_est);
   CU(ctx, cudaGetLastError());
   CU(ctx, cudaMemcpyAsync(ctx->h_out + 12, ctx->d_est, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CU(ctx, cudaStreamSynchronize(ctx->stream));
-  const double scale = (double)total / (double)samples;
-  e->s1 = ctx->h_out[12] * scale * 2.0;  // |factor| = 2
-  e->s2 = ctx->h_out[13] * scale * 4.0;
+  e->s1 = ctx->h_out[12] * 2.0;  // |factor| = 2
+  e->s2 = ctx->h_out[13] * 4.0;
   error_bounds(op.variant, op.group, n, value, e);
   return PERM_OK;
 }
@@ -918,8 +966,10 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
   }
   // split-X walks of A and B: independent per-term roundings; A's walk also
   // returns the exact moments of its terms, and B runs only if the estimate
-  // from those can meet the target
-  if (n >= 4 && n <= 40 && out->value != 0.0) {
+  // from those can meet the target.  Not after an int32-X first pass: its
+  // ceil(n/G) roundings per term are already fewer than split X's 2n - 1.
+  if (n >= 4 && n <= 40 && out->value != 0.0 && op.variant != PERM_KERNEL_DENSE_INT &&
+      op.variant != PERM_KERNEL_DENSE_TC) {
     DenseOperand sa, sb;
     perm_result ra, rb;
     if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE_SPLIT, &sa))) return rc;

@@ -196,8 +196,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--order", type=int, default=N_ORDER, help="matrix order (profiling runs use a smaller one)")
-    ap.add_argument("--variant", choices=["auto", "fp64", "int", "tc"], default="auto",
-                    help="dense kernel: automatic, FP64-X, int32-X or tensor-core row sums")
+    ap.add_argument("--variant", choices=["auto", "fp64", "int", "tc", "split"], default="auto",
+                    help="dense kernel: automatic, FP64-X, int32-X, tensor-core row sums or split X")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -220,9 +220,14 @@ def main():
     A = make_matrix(rank, args.order)
     n = A.shape[0]
     variant = {"auto": 0, "fp64": pb.PERM_KERNEL_DENSE, "int": pb.PERM_KERNEL_DENSE_INT,
-               "tc": pb.PERM_KERNEL_DENSE_TC}[args.variant]
+               "tc": pb.PERM_KERNEL_DENSE_TC, "split": pb.PERM_KERNEL_DENSE_SPLIT}[args.variant]
     total_steps = 2.0 ** (n - 1)
     ops_per_step = 2.0 * n  # n X-updates + n multiplies per Gray step (algorithmic)
+    ops_text = f"2n = {int(ops_per_step)} FP64 ops per Gray step x 2^{n - 1} steps"
+    if variant == pb.PERM_KERNEL_DENSE_SPLIT:
+        # coarse and remainder X updates, a combine per entry, n - 1 multiplies
+        ops_per_step = 4.0 * n - 1.0
+        ops_text = f"4n - 1 = {int(ops_per_step)} FP64 ops per split-X Gray step x 2^{n - 1} steps"
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")  # 256 MB > L2
 
     peak_ops, _ = eng.fp64_peak()
@@ -300,7 +305,7 @@ def main():
 
     mean_ms = statistics.mean(kernel_ms)
     achieved = total_steps * ops_per_step / (mean_ms * 1e-3)
-    kname = {1: "fp64x", 3: "int32x", 5: "tc"}.get(r.kernel, "")
+    kname = {1: "fp64x", 3: "int32x", 5: "tc", 6: "splitx"}.get(r.kernel, "")
     prof_rec = load_profile(kname, n)
     traffic = prof_rec.get("dram_bytes_per_launch") if prof_rec else None
 
@@ -322,7 +327,7 @@ def main():
                      "frac": achieved / peak_ops, "traffic": traffic,
                      "peak_source": "measured this run: perm_fp64_peak (independent DFMA chains), "
                                     "1 op = 1 lane DADD/DMUL/DFMA",
-                     "algorithmic": f"2n = {int(ops_per_step)} FP64 ops per Gray step x 2^{n - 1} steps"},
+                     "algorithmic": ops_text},
         "gpu_launches": args.steps * 1 + args.steps * 1,
         "wall_s_timed": wall,
     }

@@ -910,9 +910,10 @@ static bool has_perfect_matching(const void* mat, int n, int dtype) {
 //     changes every product's significand, even for symmetric or constant
 //     matrices, so B's roundings are independent of A's.  Keep when
 //     max(independent-rounding estimate, 16 |perm(A) - perm(B)/3| / |perm(A)|)
-//     meets the target;
-//  4. the same cross-check with the split-X kernel on A and B (orders 4..40),
-//     whose per-term roundings are independent;
+//     meets the target (B walked with split X when the FP64-X bound is far
+//     above the target);
+//  4. the same cross-check with the split-X kernel on A and B (orders 4..40,
+//     after an FP64-X first pass), whose per-term roundings are independent;
 //  5. otherwise recompute in double-double (orders <= 40).
 // Steps 3 and 4 are skipped when their independent-rounding estimate alone
 // misses the target.
@@ -950,11 +951,21 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
   for (int i2 = 0; i2 < n; i2++)
     for (int j2 = 0; j2 < n; j2++)
       b[(size_t)i2 * n + j2] = elem(mat, dtype, (size_t)j2 * n + i2) * (i2 == 0 ? 3.0 : 1.0);
+  // Split X (orders 4..40) after an FP64-X first pass; an int32-X one has
+  // ceil(n/G) roundings per term, already fewer than split X's 2n - 1.
+  const bool split_ok = n >= 4 && n <= 40 && op.variant != PERM_KERNEL_DENSE_INT &&
+                        op.variant != PERM_KERNEL_DENSE_TC;
+  // An FP64-X bound well above the target rarely passes an FP64-X
+  // cross-check (its correlated X roundings give errors near the bound), so
+  // B is then walked with split X at once, and reused for the split stage.
+  const bool b_split = split_ok && e.worst > 8.0 * target;
+  perm_result rb;
+  bool have_rb = false;
   // the cross-check's estimate is at least the independent-rounding one
   if (out->value != 0.0 && e.random <= target) {
     DenseOperand t;
     perm_result rt;
-    if ((rc = build_operand(ctx, b.data(), n, PERM_F64, 0, &t))) return rc;
+    if ((rc = build_operand(ctx, b.data(), n, PERM_F64, b_split ? PERM_KERNEL_DENSE_SPLIT : 0, &t))) return rc;
     if ((rc = run_whole(ctx, t, &rt))) return rc;
     out->kernel_ms += rt.kernel_ms;
     const double diff = std::fabs(out->value - rt.value / 3.0) / std::fabs(out->value);
@@ -963,15 +974,17 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
       out->rel_error_estimate = est;
       return PERM_OK;
     }
+    if (b_split) {
+      rb = rt;
+      have_rb = true;
+    }
   }
   // split-X walks of A and B: independent per-term roundings; A's walk also
   // returns the exact moments of its terms, and B runs only if the estimate
-  // from those can meet the target.  Not after an int32-X first pass: its
-  // ceil(n/G) roundings per term are already fewer than split X's 2n - 1.
-  if (n >= 4 && n <= 40 && out->value != 0.0 && op.variant != PERM_KERNEL_DENSE_INT &&
-      op.variant != PERM_KERNEL_DENSE_TC) {
+  // from those can meet the target
+  if (split_ok && out->value != 0.0) {
     DenseOperand sa, sb;
-    perm_result ra, rb;
+    perm_result ra;
     if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE_SPLIT, &sa))) return rc;
     if ((rc = run_whole(ctx, sa, &ra))) return rc;
     out->kernel_ms += ra.kernel_ms;
@@ -980,9 +993,11 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
     es.s2 = ctx->split_m2;
     error_bounds(PERM_KERNEL_DENSE_SPLIT, 0, n, ra.value, &es);
     if (ra.value != 0.0 && es.random <= target) {
-      if ((rc = build_operand(ctx, b.data(), n, PERM_F64, PERM_KERNEL_DENSE_SPLIT, &sb))) return rc;
-      if ((rc = run_whole(ctx, sb, &rb))) return rc;
-      out->kernel_ms += rb.kernel_ms;
+      if (!have_rb) {
+        if ((rc = build_operand(ctx, b.data(), n, PERM_F64, PERM_KERNEL_DENSE_SPLIT, &sb))) return rc;
+        if ((rc = run_whole(ctx, sb, &rb))) return rc;
+        out->kernel_ms += rb.kernel_ms;
+      }
       const double diff = std::fabs(ra.value - rb.value / 3.0) / std::fabs(ra.value);
       const double est = std::max(es.random, 16.0 * diff);
       if (est <= target) {

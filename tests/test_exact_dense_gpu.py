@@ -196,7 +196,7 @@ def test_int_kernel_shards(engine, pb):
 def test_dense_autotune_sets_the_automatic_choice(pb):
     with pb.Engine(0) as eng:
         table = eng.dense_autotune(8, 22)
-        assert set(table.values()) <= {pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_INT}
+        assert set(table.values()) <= {pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_INT, pb.PERM_KERNEL_DENSE_TC}
         rng = np.random.default_rng(1)
         for n, k in table.items():
             A = bernoulli(rng, n, 0.5)

@@ -108,8 +108,12 @@ __host__ __device__ inline size_t dense_split_smem_bytes(int n) {
   return sizeof(double) * (2 * (size_t)n * np + 2 * np) + 32 * sizeof(dd) + 16;
 }
 
+// CTAs per SM by order: the two X vectors fit 128 registers up to order 23
+// (4 CTAs) and 168 up to order 34 (3 CTAs; without the hint ptxas picked a
+// 166-register schedule at order 34 that ran 25% slower); above, 2 CTAs of
+// up to 255 registers.
 template <int N>
-__global__ void __launch_bounds__(128) ryser_dense_split_kernel(DenseSplitArgs args) {
+__global__ void __launch_bounds__(128, (N <= 23 ? 4 : N <= 34 ? 3 : 1)) ryser_dense_split_kernel(DenseSplitArgs args) {
   static_assert(N >= 4, "orders below 4 use the other kernels");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* sH = reinterpret_cast<double*>(smem_raw);  // whole image, staged once

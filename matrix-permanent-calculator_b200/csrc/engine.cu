@@ -487,21 +487,22 @@ static bool tc_eligible(const std::vector<double>& a, int n) {
 }
 
 // Split-X operand (ryser_dense_split.cuh): every entry a = ah + al with ah on
-// the grid 2^-q, q chosen so that partial row sums of coarse parts stay below
-// 2^(52 - q) and are exact in FP64; x0 likewise, from its double-double value.
+// its row's grid 2^-q_j, q_j chosen so that partial row sums of coarse parts
+// are exact in FP64 (rows scale independently: x_j only sums row j); x0
+// likewise, from its double-double value.
 // Image: [ah column-major, stride np][al][x0h][x0l].
 static int build_split_operand(perm_ctx* ctx, const std::vector<double>& a, int n, DenseOperand* op) {
   if (n < 4 || n > 40) return fail(ctx, PERM_EUNSUPPORTED, "split-X kernel covers orders 4..40 (got %d)", n);
-  double rowabs = 0.0;
+  // per row: grid 2^-q_j with 2^(51 - q_j) > 4 sum_k |a_jk|, so every partial
+  // sum of coarse parts (at most 1.5x the row's absolute sum plus n half
+  // grid steps) is an integer multiple of 2^-q_j below 2^51 of them
+  std::vector<int> q(n, 0);
   for (int j = 0; j < n; j++) {
     double r = 0.0;
     for (int k = 0; k < n; k++) r += std::fabs(a[(size_t)j * n + k]);
-    rowabs = std::max(rowabs, r);
+    if (r > 0.0 && std::isfinite(r)) q[j] = std::min(1000, std::max(-1000, 51 - (std::ilogb(2.0 * r) + 2)));
   }
-  if (!(rowabs > 0.0) || !std::isfinite(rowabs)) rowabs = 1.0;
-  const int E = (int)std::ceil(std::log2(2.0 * rowabs * (1.0 + 1e-12) + 1.0));  // |coarse sums| < 2^E
-  const int q = 51 - E;
-  auto coarse = [q](double v) { return std::ldexp(std::nearbyint(std::ldexp(v, q)), -q); };
+  auto coarse = [&q](double v, int j) { return std::ldexp(std::nearbyint(std::ldexp(v, q[j])), -q[j]); };
   const int np = (n + 1) & ~1;
   op->n = n;
   op->variant = PERM_KERNEL_DENSE_SPLIT;
@@ -514,7 +515,7 @@ static int build_split_operand(perm_ctx* ctx, const std::vector<double>& a, int 
   double* X0l = X0h + np;
   for (int k = 0; k < n; k++)
     for (int j = 0; j < n; j++) {
-      const double v = a[(size_t)j * n + k], h = coarse(v);
+      const double v = a[(size_t)j * n + k], h = coarse(v, j);
       H[(size_t)k * np + j] = h;
       L[(size_t)k * np + j] = v - h;  // exact
     }
@@ -531,7 +532,7 @@ static int build_split_operand(perm_ctx* ctx, const std::vector<double>& a, int 
     const double v = a[(size_t)j * n + n - 1], sum = hi + v, bb = sum - hi;
     lo += (hi - (sum - bb)) + (v - bb);
     hi = sum;
-    const double h = coarse(hi);
+    const double h = coarse(hi, j);
     X0h[j] = h;
     X0l[j] = (hi - h) + lo;
   }

@@ -454,6 +454,17 @@ def test_split_kernel_vs_oracle(engine, orc, pb, n):
             assert actual <= 1e-13, (kind, actual)
 
 
+def test_split_kernel_rows_of_different_scales(engine, orc, pb):
+    """Each row gets its own coarse grid: rows scaled over 10 orders of
+    magnitude keep the split result at the unscaled matrix's accuracy."""
+    n = 22
+    rng = np.random.default_rng(961)
+    A = (1.0 - rng.random((n, n))) * (7.3 ** (np.arange(n) % 11 - 5.0))[:, None]
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SPLIT)
+    hi, lo = orc.perm_dd(A)
+    assert abs(r.value - hi - lo) / abs(hi) <= 1e-13
+
+
 def test_split_kernel_integer_and_binary_inputs(engine, orc, pb):
     rng = np.random.default_rng(960)
     for A in (bernoulli(rng, 21, 0.5), rng.integers(-3, 4, (18, 18)).astype(float), np.ones((13, 13))):

@@ -140,15 +140,19 @@ int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, const int* cols
 int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard, int nshards,
                         perm_result* out);
 /* Whole-walk dense results carry rel_error_estimate, a worst-case bound
- * formed from sum |term| over 65536 sampled Gray terms.  With variant 0 and a
- * context target (default 1e-10; <= 0 disables the policy; < 0 also skips
- * the estimate):
+ * formed from sum |term|, estimated by a sample of Ryser terms stratified by
+ * subset size (exact for the split-X kernel, whose walk sums its own terms).
+ * With variant 0 and a context target (default 1e-10; <= 0 disables the
+ * policy; < 0 also skips the estimate):
  *  - a zero pattern without a perfect matching returns exactly 0;
  *  - a result whose bound exceeds the target is cross-checked against
  *    B = A^T with its first row times 3 (perm(B) = 3 perm(A), independent
  *    roundings) and kept when max(4-sigma independent-rounding estimate from
  *    sum term^2, 16 |perm(A) - perm(B)/3| / |perm(A)|) meets the target, which
  *    then is the reported estimate;
+ *  - after an FP64-X first pass (orders 4..40) the same check runs on split-X
+ *    walks of A and B, returning the split-X value (kernel
+ *    PERM_KERNEL_DENSE_SPLIT) when it passes;
  *  - otherwise it is recomputed by the double-double kernel (orders <= 40).
  * kernel_ms covers every launch.  PERM_KERNEL_DENSE_DD forces that kernel. */
 int perm_ctx_set_rel_target(perm_ctx* ctx, double rel_target);

@@ -54,3 +54,21 @@ def test_no_device_fails_loudly(pb):
 def test_missing_library_raises(pb, tmp_path):
     with pytest.raises(pb.PermError):
         pb.load_library(tmp_path / "nope.so")
+
+
+def test_header_constants_match_the_binding(pb):
+    """Every PERM_* integer #define in the header has the same value in the
+    Python binding (status codes, dtypes, kernel ids, request kinds)."""
+    text = (ROOT / "include" / "perman_b200.h").read_text()
+    defines = dict(re.findall(r"^#define\s+(PERM_\w+)\s+(-?\d+)\b", text, flags=re.M))
+    assert "PERM_KERNEL_DENSE_SPLIT" in defines and "PERM_KERNEL_DENSE_TC" in defines
+    checked = 0
+    for name, value in defines.items():
+        if name.startswith("PERM_MAX") or not hasattr(pb, name):
+            continue
+        assert getattr(pb, name) == int(value), (name, getattr(pb, name), value)
+        checked += 1
+    assert checked >= 10
+    for name in defines:
+        if name.startswith(("PERM_KERNEL_", "PERM_E", "PERM_F", "PERM_I", "PERM_REQ_")):
+            assert hasattr(pb, name), name

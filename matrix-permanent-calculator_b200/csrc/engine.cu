@@ -794,10 +794,12 @@ static int check_variant(perm_ctx* ctx, int variant) {
 }
 
 // Error estimate of a whole-walk result.  The sample kernel estimates
-// S1 = sum_i |term(i)| and S2 = sum_i term(i)^2 from 65536 Gray indices
-// spread over the walk; with unit roundoff u = 2^-53 and r roundings per term
-// (FP64 X: n x updates and n - 1 products, r ~ 2n; int32 X: x and the group
-// products are exact, r = ceil(n/G) - 1 FP64 products):
+// S1 = sum_i |term(i)| and S2 = sum_i term(i)^2 from terms stratified by
+// subset size (the split-X walk sums both exactly); with unit roundoff
+// u = 2^-53 and r roundings per term (FP64 X: n x updates and n - 1
+// products, r ~ 2n; split X: n combines and n - 1 products, r ~ 2n, each a
+// function of the subset alone; int32 X: x and the group products are exact,
+// r = ceil(n/G) - 1 FP64 products):
 //  * worst: every rounding of every term in the same direction,
 //    (r + 16) u S1 / |perm|;
 //  * random: four standard deviations of the sum when roundings are

@@ -500,7 +500,7 @@ static int build_split_operand(perm_ctx* ctx, const std::vector<double>& a, int 
   for (int j = 0; j < n; j++) {
     double r = 0.0;
     for (int k = 0; k < n; k++) r += std::fabs(a[(size_t)j * n + k]);
-    if (r > 0.0 && std::isfinite(r)) q[j] = std::min(1000, std::max(-1000, 51 - (std::ilogb(2.0 * r) + 2)));
+    if (r > 0.0 && std::isfinite(r)) q[j] = std::min(1000, std::max(-1000, 51 - (std::ilogb(r) + 3)));
   }
   auto coarse = [&q](double v, int j) { return std::ldexp(std::nearbyint(std::ldexp(v, q[j])), -q[j]); };
   const int np = (n + 1) & ~1;

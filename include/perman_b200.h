@@ -188,6 +188,12 @@ int perm_exact_dense_tc_rounds(perm_ctx* ctx, const void* mat, int n, int dtype,
  * buffer `d_out` of two doubles that receives (hi, lo); everything else lives
  * in one static device array (~96 KB per GPU that loads this library, held
  * until the process exits).  No cudaMalloc or cudaFree is called.
+ *  - the computation is perm_exact_dense_ex's FP64-X kernel (PERM_KERNEL_DENSE)
+ *    with the same launch decomposition and X re-anchoring, so its value
+ *    equals that call's to the last bit on the same device; unlike
+ *    perm_exact_dense it returns no error estimate and applies no accuracy
+ *    policy (no int32-X, split-X or double-double pass), so on matrices with
+ *    heavy cancellation its error is that of one FP64-X walk;
  *  - orders 1..64; larger orders return PERM_EUNSUPPORTED (the array holds one
  *    64 x 64 operand and partials for 4096 CTAs), null pointers PERM_EINVAL;
  *  - runs asynchronously on `stream` (a cudaStream_t, NULL = default stream);
@@ -234,7 +240,9 @@ int perm_batch_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* m_out);
  * admitted when a slot is idle and its device-memory need fits the budget
  * (0 = half the free device memory).  Exact requests longer than
  * `slice_steps` Gray indices (0 = 2^31) run as several shard launches so small
- * requests interleave.  The request's matrix is copied at submit. */
+ * requests interleave.  The request's matrix is copied at submit.  A request
+ * that does not fit the remaining budget may be passed by later, smaller ones
+ * at most 8 times; then admission waits for it. */
 #define PERM_REQ_EXACT_DENSE 0
 #define PERM_REQ_EXACT_SPARSE 1
 #define PERM_REQ_RASMUSSEN 2
@@ -263,6 +271,10 @@ int perm_server_submit(perm_server* s, const perm_request* req, uint64_t* ticket
 int perm_server_wait(perm_server* s, uint64_t ticket, int timeout_ms, perm_response* out);
 /* out5 = submitted, completed, in flight, queued, device bytes in use. */
 int perm_server_stats(perm_server* s, double* out5);
+/* Finishes the requests already running, ends every queued one with status
+ * PERM_EINVAL ("server destroyed before the request ran"), lets threads
+ * blocked in perm_server_wait return with their response, then frees the
+ * server.  No other call on `s` may start once destroy has begun. */
 void perm_server_destroy(perm_server* s);
 
 /* ---- Monte-Carlo estimates of the permanent of the 0/1 pattern -------------- */

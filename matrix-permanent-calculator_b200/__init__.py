@@ -575,7 +575,10 @@ def distributed_exact_dense(mat, group=None, engine: Engine | None = None, shard
     return dd_sum((float(g[0]), float(g[1])) for g in gathered)
 
 
-_queue_calls = 0
+# calls of distributed_exact_dense_dynamic so far, per process group (keyed
+# by its sorted global ranks): every member makes the same calls in the same
+# order, so (group, call number) names one queue on all of them
+_queue_calls: dict[tuple[int, ...], int] = {}
 
 
 def distributed_exact_dense_dynamic(mat, chunks: int | None = None, group=None, engine: Engine | None = None,
@@ -599,13 +602,16 @@ def distributed_exact_dense_dynamic(mat, chunks: int | None = None, group=None, 
     import torch
     import torch.distributed as dist
 
-    global _queue_calls
     world = dist.get_world_size(group)
     chunks = chunks or 8 * world
     if store is None:
         store = dist.distributed_c10d._get_default_store()
-    key = f"perm_b200_queue_{_queue_calls}"  # every rank makes the same calls in the same order
-    _queue_calls += 1
+    members = tuple(sorted(dist.get_process_group_ranks(group if group is not None else dist.group.WORLD)))
+    call = _queue_calls.get(members, 0)
+    _queue_calls[members] = call + 1
+    # the key names the group and the call, so concurrent subgroups and later
+    # world calls never share a counter
+    key = f"perm_b200_queue_{'-'.join(map(str, members))}_{call}"
     eng = None if shard_fn is not None else (engine or default_engine())
     table = torch.zeros((chunks, 3), dtype=torch.float64)
     while True:

@@ -491,8 +491,22 @@ static bool tc_eligible(const std::vector<double>& a, int n) {
 // are exact in FP64 (rows scale independently: x_j only sums row j); x0
 // likewise, from its double-double value.
 // Image: [ah column-major, stride np][al][x0h][x0l].
+// Rows whose absolute sum reaches 2^1020 are outside the split: their coarse
+// grid 2^-q_j would be coarser than 2^971, and a coarse part rounded up to
+// the top of that grid can overflow to infinity.
+static bool split_rows_ok(const std::vector<double>& a, int n) {
+  for (int j = 0; j < n; j++) {
+    double r = 0.0;
+    for (int k = 0; k < n; k++) r += std::fabs(a[(size_t)j * n + k]);
+    if (!std::isfinite(r) || (r > 0.0 && std::ilogb(r) >= 1020)) return false;
+  }
+  return true;
+}
+
 static int build_split_operand(perm_ctx* ctx, const std::vector<double>& a, int n, DenseOperand* op) {
   if (n < 4 || n > 40) return fail(ctx, PERM_EUNSUPPORTED, "split-X kernel covers orders 4..40 (got %d)", n);
+  if (!split_rows_ok(a, n))
+    return fail(ctx, PERM_EUNSUPPORTED, "split-X kernel needs row absolute sums below 2^1020");
   // per row: grid 2^-q_j with 2^(51 - q_j) > 4 sum_k |a_jk|, so every partial
   // sum of coarse parts (at most 1.5x the row's absolute sum plus n half
   // grid steps) is an integer multiple of 2^-q_j below 2^51 of them
@@ -500,7 +514,7 @@ static int build_split_operand(perm_ctx* ctx, const std::vector<double>& a, int 
   for (int j = 0; j < n; j++) {
     double r = 0.0;
     for (int k = 0; k < n; k++) r += std::fabs(a[(size_t)j * n + k]);
-    if (r > 0.0 && std::isfinite(r)) q[j] = std::min(1000, std::max(-1000, 51 - (std::ilogb(r) + 3)));
+    if (r > 0.0) q[j] = std::min(1000, std::max(-1000, 51 - (std::ilogb(r) + 3)));
   }
   auto coarse = [&q](double v, int j) { return std::ldexp(std::nearbyint(std::ldexp(v, q[j])), -q[j]); };
   const int np = (n + 1) & ~1;
@@ -956,8 +970,10 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
       b[(size_t)i2 * n + j2] = elem(mat, dtype, (size_t)j2 * n + i2) * (i2 == 0 ? 3.0 : 1.0);
   // Split X (orders 4..40) after an FP64-X first pass; an int32-X one has
   // ceil(n/G) roundings per term, already fewer than split X's 2n - 1.
+  std::vector<double> av((size_t)n * n);
+  for (size_t i = 0; i < av.size(); i++) av[i] = elem(mat, dtype, i);
   const bool split_ok = n >= 4 && n <= 40 && op.variant != PERM_KERNEL_DENSE_INT &&
-                        op.variant != PERM_KERNEL_DENSE_TC;
+                        op.variant != PERM_KERNEL_DENSE_TC && split_rows_ok(av, n) && split_rows_ok(b, n);
   // An FP64-X bound well above the target rarely passes an FP64-X
   // cross-check (its correlated X roundings give errors near the bound), so
   // B is then walked with split X at once, and reused for the split stage.

@@ -158,7 +158,7 @@ extern "C" int perm_exact_dense_noalloc(const double* d_mat, int n, double* d_ou
   args.ticket = &su.scratch->ticket;
   args.out = d_out;
   args.err = &su.scratch->err;
-  args.seg_blocks = 0;  // one X per thread range (no re-anchoring)
+  args.seg_blocks = 0;
   int grid = 1;
   if (n < 4) {
     args.m = 0;
@@ -176,6 +176,9 @@ extern "C" int perm_exact_dense_noalloc(const double* d_mat, int n, double* d_ou
     args.m = m;
     args.block0 = 0;
     args.nblocks = blocks;
+    // X re-anchored every >= 2^11 Gray steps (orders <= kAnchorMaxN), as in
+    // perm_exact_dense's FP64-X launches: same rounding behaviour
+    args.seg_blocks = m >= 11 ? 1 : (1ull << (11 - m));
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   noalloc_prepare<<<1, 256, 0, st>>>(d_mat, n, np);

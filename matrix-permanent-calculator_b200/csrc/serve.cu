@@ -9,8 +9,10 @@
 //  * Admission: a request is admitted when a slot is idle and its device
 //    memory need (operand image + per-trial buffers) fits in the remaining
 //    budget; requests that arrive while others run are admitted as slots and
-//    memory free up (FIFO, with smaller requests allowed to pass a blocked
-//    head when they fit -- no starvation because the head is retried first).
+//    memory free up (FIFO; a request that does not fit may be passed by
+//    later ones that do, at most kMaxPasses times, after which nothing passes
+//    it until enough memory frees up -- so a large request cannot starve
+//    behind a steady stream of small ones).
 //  * Exact requests whose Gray walk exceeds `slice_steps` run as several
 //    shard launches (perm_exact_dense_shard) so that one large permanent does
 //    not hold the whole GPU for tens of milliseconds while small requests
@@ -48,7 +50,12 @@ struct Job {
   Clock::time_point t_submit;
   perm_response resp{};
   bool done = false;
+  int passes = 0;  // times a later job was admitted ahead of this one
 };
+
+// How often a pending job that does not fit the memory budget may be passed
+// by later jobs before admission stops at it.
+constexpr int kMaxPasses = 8;
 
 size_t request_bytes(const perm_request& r) {
   const size_t n = (size_t)std::max(r.n, 1);
@@ -82,6 +89,7 @@ struct perm_server {
   uint64_t next_ticket = 1;
   uint64_t submitted = 0, completed = 0, in_flight = 0;
   bool stop = false;
+  int waiters = 0;  // threads inside perm_server_wait
   std::vector<std::thread> workers;
   std::vector<perm_ctx*> ctxs;
 };
@@ -94,16 +102,20 @@ double ms_since(const perm_server* s, Clock::time_point t) {
 
 // Pick the next job this worker may run (caller holds the lock): the oldest
 // pending job whose memory need fits the remaining budget; a job larger than
-// the whole budget runs alone once nothing else holds memory.
+// the whole budget runs alone once nothing else holds memory.  Jobs that are
+// passed over are counted, and one passed kMaxPasses times blocks every job
+// behind it until it fits.
 Job* take_admissible(perm_server* s) {
   for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
     Job* j = *it;
     if (s->in_use + j->bytes <= s->budget || s->in_use == 0) {
+      for (auto p = s->pending.begin(); p != it; ++p) (*p)->passes++;
       s->pending.erase(it);
       s->in_use += j->bytes;
       s->in_flight++;
       return j;
     }
+    if (j->passes >= kMaxPasses) return nullptr;
   }
   return nullptr;
 }
@@ -272,12 +284,17 @@ extern "C" int perm_server_wait(perm_server* s, uint64_t ticket, int timeout_ms,
   if (it == s->jobs.end()) return PERM_EINVAL;
   Job* j = it->second;
   auto ready = [&] { return j->done; };
+  s->waiters++;
+  bool got = true;
   if (timeout_ms < 0)
     s->cv_done.wait(lock, ready);
-  else if (!s->cv_done.wait_for(lock, std::chrono::milliseconds(timeout_ms), ready))
-    return PERM_ETIMEOUT;
+  else
+    got = s->cv_done.wait_for(lock, std::chrono::milliseconds(timeout_ms), ready);
+  s->waiters--;
+  if (s->stop) s->cv_done.notify_all();  // perm_server_destroy waits for the last waiter
+  if (!got) return PERM_ETIMEOUT;
   *out = j->resp;
-  s->jobs.erase(it);
+  s->jobs.erase(ticket);
   delete j;
   return PERM_OK;
 }
@@ -301,6 +318,19 @@ extern "C" void perm_server_destroy(perm_server* s) {
   }
   s->cv_work.notify_all();
   for (auto& t : s->workers) t.join();
+  {
+    // requests that never ran end with an error, and threads blocked in
+    // perm_server_wait collect their response before anything is freed
+    std::unique_lock<std::mutex> lock(s->mu);
+    for (Job* j : s->pending) {
+      j->resp.status = PERM_EINVAL;
+      snprintf(j->resp.message, sizeof j->resp.message, "server destroyed before the request ran");
+      j->done = true;
+    }
+    s->pending.clear();
+    s->cv_done.notify_all();
+    s->cv_done.wait(lock, [&] { return s->waiters == 0; });
+  }
   for (perm_ctx* c : s->ctxs) perm_ctx_destroy(c);
   for (auto& kv : s->jobs) delete kv.second;
   delete s;

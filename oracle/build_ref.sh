@@ -8,8 +8,9 @@
 # (Makefile:2) plus -include cstdint (util.h uses INT8_MAX without <cstdint>)
 # and an sm_100a target.
 set -euo pipefail
-REF=${REF_SRC:-/root/reference}
 HERE="$(cd "$(dirname "$0")" && pwd)"
+# $REF_SRC, else a `reference` directory beside this repository
+REF=${REF_SRC:-$HERE/../../reference}
 OUT="$HERE/_ref"
 if [ ! -f "$REF/main.cu" ]; then
   echo "reference sources not found at $REF; keeping prebuilt $OUT" >&2

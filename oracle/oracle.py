@@ -29,9 +29,15 @@ def build_oracle() -> Path:
     return ORACLE_SO
 
 
+def reference_sources() -> Path:
+    """Where the reference's sources are read from: $REF_SRC, else a
+    `reference` directory beside this repository."""
+    return Path(os.environ.get("REF_SRC", HERE.parents[1] / "reference"))
+
+
 def build_reference() -> Path | None:
     """Compile the reference into oracle/_ref when its sources are present."""
-    if not Path(os.environ.get("REF_SRC", "/root/reference"), "main.cu").exists():
+    if not (reference_sources() / "main.cu").exists():
         return REF_SO if REF_SO.exists() else None
     if not REF_SO.exists():
         subprocess.run([str(HERE / "build_ref.sh")], check=True, capture_output=True)

@@ -13,7 +13,8 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 PKG_DIR = ROOT / "matrix-permanent-calculator_b200"
 GOLDEN = ROOT / "tests" / "golden" / "golden.json"
-REF_SRC = Path(os.environ.get("REF_SRC", "/root/reference"))
+# reference sources: $REF_SRC, else a `reference` directory beside this repository
+REF_SRC = Path(os.environ.get("REF_SRC", ROOT.parent / "reference"))
 
 sys.path.insert(0, str(ROOT / "oracle"))
 

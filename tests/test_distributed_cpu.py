@@ -134,3 +134,56 @@ def test_gloo_dynamic_chunk_queue(pb, orc, tmp_path):
         assert abs((r[3] + r[4]) - want) <= 1e-14 * abs(want)
     assert r0[0] == r1[0] and r0[1] == r1[1]
     assert r0[2] + r1[2] == 24 and r1[2] > r0[2]
+
+
+def _rank_subgroup_then_world(rank, world, port, store_port, A, out_path):
+    import sys
+    from datetime import timedelta
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    sys.path.insert(0, str(root / "tests"))
+    sys.path.insert(0, str(root / "oracle"))
+    import torch.distributed as dist
+    from conftest import load_package
+    from oracle import Oracle
+
+    pb = load_package()
+    orc = Oracle()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    store = dist.TCPStore("127.0.0.1", store_port, world, rank == 0, timeout=timedelta(seconds=60))
+    n = A.shape[0]
+    factor = 2.0 if n & 1 else -2.0
+
+    def shard_fn(mat, c, chunks):
+        a, b = pb.shard_range(n, c, chunks)
+        hi, lo = orc.ryser_dd_range(mat, a, b, threads=1)
+        return hi * factor, lo * factor
+
+    # two disjoint subgroups run their own queues at the same time, then the
+    # world group runs one: no queue is shared, every chunk runs exactly once
+    g01, g23 = dist.new_group([0, 1]), dist.new_group([2, 3])
+    mine = g01 if rank < 2 else g23
+    sub = pb.distributed_exact_dense_dynamic(A, chunks=6, group=mine, shard_fn=shard_fn, store=store)
+    whole = pb.distributed_exact_dense_dynamic(A, chunks=8, shard_fn=shard_fn, store=store)
+    dist.barrier()
+    dist.destroy_process_group()
+    np.save(f"{out_path}.{rank}.npy", np.array([sub[0], sub[1], whole[0], whole[1]]))
+
+
+def test_gloo_dynamic_queue_subgroups_then_world(pb, orc, tmp_path):
+    """The queue's store key names the process group: two subgroups of a
+    4-rank job and then the world group each drain a queue of their own."""
+    rng = np.random.default_rng(9)
+    A = rng.random((13, 13))
+    port, store_port = _free_port(), _free_port()
+    out = str(tmp_path / "sub")
+    mp.start_processes(_rank_subgroup_then_world, args=(4, port, store_port, A, out), nprocs=4, join=True,
+                       start_method="spawn")
+    want = sum(orc.perm_dd(A))
+    for r in range(4):
+        v = np.load(f"{out}.{r}.npy")
+        assert abs((v[0] + v[1]) - want) <= 1e-14 * abs(want)
+        assert abs((v[2] + v[3]) - want) <= 1e-14 * abs(want)

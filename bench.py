@@ -2,8 +2,12 @@
 
 One step = one whole exact permanent (2^39 Gray steps x 2n FP64 operations)
 of a seeded synthetic matrix that is already resident in device memory;
-`value` is Ryser Gray steps per second over all ranks (weak scaling: every
-rank computes its own matrix).  `e2e` is the same metric through the C-ABI
+`value` is Ryser Gray steps per second.  With N ranks (torchrun, one GPU
+each) the one matrix is sharded: rank r walks Gray-range shard r of N
+(perm_exact_dense_resident_shard) and the 16-byte (hi, lo) partials are
+all-gathered over NCCL and added in double-double (strong scaling; at N=1
+the step is the whole walk).  A weak-scaling secondary (every rank its own
+matrix) is kept beside it.  `e2e` is the same metric through the C-ABI
 call with a host matrix (host->device copy and result readback inside the
 timed region).  `roofline` relates the kernel's algorithmic FP64 operations to
 the FP64 peak measured live on the same chip; `cpu_baseline` is the
@@ -16,6 +20,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import hashlib
 import importlib.util
 import json
 import math
@@ -177,14 +182,97 @@ def run_reference_arm(args):
     return 0
 
 
-def load_profile(kernel: str, n: int) -> dict | None:
-    """ncu figures of one launch of `kernel` at order n (profiles/), if recorded."""
+# Sources whose text determines each profiled kernel's instruction stream:
+# a recorded ncu count is only valid for the same template instance compiled
+# from the same text.
+KERNEL_SOURCES = {
+    "int32x": ["ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
+    "fp64x": ["ryser_dense.cuh", "perman_common.cuh"],
+    "int32x_dd": ["ryser_dense_intc.cuh", "ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
+}
+
+
+def source_sha16(kname: str) -> str | None:
+    files = KERNEL_SOURCES.get(kname)
+    if not files:
+        return None
+    h = hashlib.sha256()
+    for f in files:
+        h.update((PKG / "csrc" / f).read_bytes())
+    return h.hexdigest()[:16]
+
+
+def int_group_size(A: np.ndarray) -> int:
+    """The int32-X kernels' product-group size for an integer matrix: the
+    largest G in {6,5,4,3} with prod(row absolute sums) < 2^31 over every run
+    of G consecutive rows (the engine's own rule, restated to name the
+    template instance that runs)."""
+    n = A.shape[0]
+    rows = np.maximum(np.abs(A).sum(axis=1).astype(float), 1.0)
+    for g in (6, 5, 4, 3):
+        if all(np.prod(rows[j:j + g]) < 2.0 ** 31 for j in range(0, n, g)):
+            return g
+    return 0
+
+
+def kernel_template(kname: str, A: np.ndarray) -> str:
+    n = A.shape[0]
+    if kname == "int32x":
+        return f"ryser_dense_int_kernel<{n}, {int_group_size(A)}>"
+    if kname == "int32x_dd":
+        return f"ryser_dense_intc_kernel<{n}, {int_group_size(A)}>"
+    if kname == "fp64x":
+        return f"ryser_dense_kernel<{n}>"
+    return kname
+
+
+def load_profile(kname: str, A: np.ndarray) -> tuple[dict | None, str | None]:
+    """ncu figures of one launch of this kernel's template instance (profiles/),
+    and why they do not apply (None when they do): recorded for another
+    instance, or for other source text than this checkout's."""
     prof = ROOT / "profiles" / "ryser_dense_n40_issue.json"
     try:
-        rec = json.loads(prof.read_text()).get(kernel)
+        rec = json.loads(prof.read_text()).get(kname)
     except Exception:
-        return None
-    return rec if rec and rec.get("n") == n else None
+        return None, "no profile record"
+    if not rec:
+        return None, "no profile record"
+    want = kernel_template(kname, A)
+    if rec.get("kernel") != want:
+        return None, f"profile recorded for {rec.get('kernel')}, this run launches {want}"
+    sha = source_sha16(kname)
+    if rec.get("source_sha16") != sha:
+        return rec, f"kernel sources changed since the profile (recorded {rec.get('source_sha16')}, now {sha})"
+    return rec, None
+
+
+def sharded_step(pb, shard_fn, rank: int, world: int, dist=None, device=None):
+    """One step of the sharded workload: this rank's Gray-range shard of the
+    one matrix (shard_fn(rank, world) -> (hi, lo, device ms)), then the
+    16-byte all-gather of every rank's (hi, lo), added in rank order in
+    double-double.  Returns ((hi, lo), device ms of the step on this rank:
+    the shard's kernel plus the all-gather)."""
+    hi, lo, ms = shard_fn(rank, world)
+    parts = [(hi, lo)]
+    if dist is not None and world > 1:
+        import torch
+
+        dev = f"cuda:{device}" if device is not None else "cpu"
+        t = torch.tensor([hi, lo], dtype=torch.float64, device=dev)
+        gathered = [torch.zeros_like(t) for _ in range(world)]
+        if device is not None:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dist.all_gather(gathered, t)
+            e1.record()
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        else:
+            t0 = time.perf_counter()
+            dist.all_gather(gathered, t)
+            ms += (time.perf_counter() - t0) * 1e3
+        parts = [(float(g[0]), float(g[1])) for g in gathered]
+    return pb.dd_sum(parts), ms
 
 
 def main():
@@ -196,8 +284,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--order", type=int, default=N_ORDER, help="matrix order (profiling runs use a smaller one)")
-    ap.add_argument("--variant", choices=["auto", "fp64", "int", "tc", "split"], default="auto",
-                    help="dense kernel: automatic, FP64-X, int32-X, tensor-core row sums or split X")
+    ap.add_argument("--variant", choices=["auto", "fp64", "int", "tc", "split", "intdd"], default="auto",
+                    help="dense kernel: automatic, FP64-X, int32-X, tensor-core row sums, split X or the "
+                         "certified int32-X walk (double-double products and sum)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -217,10 +306,11 @@ def main():
     torch.cuda.set_device(device)
     pb = load_pkg()
     eng = pb.Engine(device)
-    A = make_matrix(rank, args.order)
+    A = make_matrix(0, args.order)  # the one matrix every rank shards
     n = A.shape[0]
     variant = {"auto": 0, "fp64": pb.PERM_KERNEL_DENSE, "int": pb.PERM_KERNEL_DENSE_INT,
-               "tc": pb.PERM_KERNEL_DENSE_TC, "split": pb.PERM_KERNEL_DENSE_SPLIT}[args.variant]
+               "tc": pb.PERM_KERNEL_DENSE_TC, "split": pb.PERM_KERNEL_DENSE_SPLIT,
+               "intdd": pb.PERM_KERNEL_DENSE_INT_DD}[args.variant]
     total_steps = 2.0 ** (n - 1)
     ops_per_step = 2.0 * n  # n X-updates + n multiplies per Gray step (algorithmic)
     ops_text = f"2n = {int(ops_per_step)} FP64 ops per Gray step x 2^{n - 1} steps"
@@ -233,39 +323,55 @@ def main():
     peak_ops, _ = eng.fp64_peak()
     peak_ops = max(peak_ops, eng.fp64_peak()[0])
     res = eng.upload_dense(A, variant=variant)
+    if world > 1 and variant == pb.PERM_KERNEL_DENSE_TC:
+        raise SystemExit("the tensor-core kernel runs whole walks only; use --variant int for sharded runs")
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize(device)
 
+    def resident_shard(r_, w_):
+        rr = res.run_shard(r_, w_)
+        resident_shard.last = rr
+        return rr.hi, rr.lo, rr.kernel_ms
+
     for _ in range(args.warmup):
-        res.run()
+        sharded_step(pb, resident_shard, rank, world, dist, device)
         flush_l2(flush)
     barrier()
-    kernel_ms = []
+    kernel_ms, step_ms = [], []
     t0 = time.perf_counter()
     with Clocks(device) as clk:
         for _ in range(args.steps):
             flush_l2(flush)
             torch.cuda.synchronize(device)
-            r = res.run()
-            kernel_ms.append(r.kernel_ms)
+            (hi, lo), ms = sharded_step(pb, resident_shard, rank, world, dist, device)
+            kernel_ms.append(resident_shard.last.kernel_ms)
+            step_ms.append(ms)
     barrier()
     wall = time.perf_counter() - t0
-    dev_s = sum(kernel_ms) * 1e-3
+    r = resident_shard.last
+    dev_s = sum(step_ms) * 1e-3
     if dist is not None:
         t = torch.tensor([dev_s], device=f"cuda:{device}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_s = float(t.item())
-    value = world * args.steps * total_steps / dev_s
-    perm_value = r.value
+    value = args.steps * total_steps / dev_s
+    perm_value = hi + lo
 
-    # end to end through the reference-signature C entry point with a host
-    # int32 matrix (gpu_perman64_xshared_coalescing_mshared_int: upload, walk,
-    # double-double result back; one evaluation, like the reference)
+    # end to end through the public C ABI with a host matrix: at N=1 the
+    # reference-signature entry point gpu_perman64_xshared_coalescing_mshared_int
+    # (upload, walk, double-double result back; one evaluation, like the
+    # reference); at N>1 distributed_exact_dense (each rank uploads the host
+    # matrix, walks its shard, the 16-byte partials are all-gathered)
     os.environ["PERM_DEVICE"] = str(device)
-    if variant == 0:
+    plain = pb.Engine(device)
+    plain.set_rel_target(-1.0)
+    if world > 1:
+        e2e_call = lambda: sum(pb.distributed_exact_dense(A, engine=plain))  # noqa: E731
+        e2e_path = "distributed_exact_dense(): perm_exact_dense_shard() C ABI per rank with a host matrix + all-gather"
+    elif variant == 0:
         shim = eng.lib.gpu_perman64_xshared_coalescing_mshared_int
         shim.restype = ctypes.c_double
         shim.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -273,8 +379,6 @@ def main():
         e2e_call = lambda: shim(A32.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n, 2048, 256)  # noqa: E731
         e2e_path = "gpu_perman64_xshared_coalescing_mshared_int() C ABI (reference signature), host int32 matrix"
     else:
-        plain = pb.Engine(device)
-        plain.set_rel_target(-1.0)
         e2e_call = lambda: plain.exact_dense(A, variant=variant).value  # noqa: E731
         e2e_path = "perm_exact_dense_ex() C ABI with a forced kernel, host matrix"
     e2e_ms = []
@@ -290,37 +394,57 @@ def main():
         t = torch.tensor([e2e_s], device=f"cuda:{device}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    assert v2 == perm_value, (v2, perm_value)  # same kernel, deterministic reduction
+    assert v2 == perm_value, (v2, perm_value)  # same shards, deterministic reductions
 
-    # the same call through perm_exact_dense with the accuracy policy
-    # (target 1e-10): estimate, cross-check and, if needed, double-double
+    # weak scaling beside it: every rank its own matrix, one whole walk
+    weak = None
+    if world > 1:
+        W = eng.upload_dense(make_matrix(rank, args.order), variant=variant)
+        W.run()
+        barrier()
+        wms = W.run().kernel_ms
+        W.free()
+        t = torch.tensor([wms * 1e-3], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        weak = {"value": world * total_steps / float(t.item()), "unit": "steps/s",
+                "ms_max_over_ranks": float(t.item()) * 1e3,
+                "config": f"{world} ranks, one whole n={n} walk each (rank r: seed {SEED} + 1000 r)"}
+        barrier()
+
+    # the same matrix through perm_exact_dense with the accuracy policy
+    # (target 1e-10): the certified walk for integer matrices
     policy = None
-    if not args.no_secondary:
+    if not args.no_secondary and rank == 0:
         t = time.perf_counter()
         rp = eng.exact_dense(A, variant=variant)
-        policy = {"ms": (time.perf_counter() - t) * 1e3, "kernel_ms": rp.kernel_ms, "kernel": rp.kernel,
+        pms = (time.perf_counter() - t) * 1e3
+        policy = {"ms": pms, "kernel_ms": rp.kernel_ms, "kernel": rp.kernel,
                   "rel_error_estimate": rp.rel_error_estimate,
-                  "rel_diff_vs_single_evaluation": abs(rp.value - perm_value) / abs(perm_value)}
+                  "rel_diff_vs_single_evaluation": abs(rp.value - perm_value) / abs(perm_value),
+                  "ratio_vs_single_evaluation_e2e": pms / (e2e_s * 1e3 / args.steps), "value": rp.value}
     barrier()
 
     mean_ms = statistics.mean(kernel_ms)
-    achieved = total_steps * ops_per_step / (mean_ms * 1e-3)
-    kname = {1: "fp64x", 3: "int32x", 5: "tc", 6: "splitx"}.get(r.kernel, "")
-    prof_rec = load_profile(kname, n)
-    traffic = prof_rec.get("dram_bytes_per_launch") if prof_rec else None
+    achieved = (total_steps / world) * ops_per_step / (mean_ms * 1e-3)
+    kname = {1: "fp64x", 3: "int32x", 5: "tc", 6: "splitx", 7: "int32x_dd"}.get(r.kernel, "")
+    prof_rec, prof_stale = load_profile(kname, A)
+    traffic = prof_rec.get("dram_bytes_per_launch") if prof_rec and not prof_stale else None
 
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, resident in HBM)",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, resident in HBM)",
         "config": {"workload": WORKLOAD.replace("n=40", f"n={n}"), "n": n, "density": DENSITY,
                    "values": "U{1,2,3,4}",
-                   "gray_steps_per_permanent": total_steps, "parallelism": f"{world} rank(s), one matrix each",
+                   "gray_steps_per_permanent": total_steps,
+                   "parallelism": (f"{world} ranks: Gray-range shards of one matrix, 16-byte NCCL all-gather"
+                                   if world > 1 else "1 rank, the whole walk"),
                    "l2": "256 MB buffer written between steps (operand is 12.8 KB; compute-bound)",
-                   "timing": "CUDA events around each kernel on the engine stream; max over ranks"},
-        "result": {"permanent": perm_value, "rank0_matrix_seed": SEED},
-        "e2e": {"value": world * args.steps * total_steps / e2e_s, "unit": "steps/s",
-                "h2d_bytes_per_step": int(4 * n * n), "d2h_bytes_per_step": 16,
+                   "timing": "CUDA events around each shard kernel (engine stream) and the all-gather; "
+                             "max over ranks"},
+        "result": {"permanent": perm_value, "matrix_seed": SEED},
+        "e2e": {"value": args.steps * total_steps / e2e_s, "unit": "steps/s",
+                "h2d_bytes_per_step": int(4 * n * n) * world, "d2h_bytes_per_step": 16 * world,
                 "ms_per_step": e2e_s * 1e3 / args.steps, "path": e2e_path, "launches_per_call": 1},
         "e2e_with_accuracy_policy": policy,
         "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "TFLOP/s",
@@ -331,8 +455,10 @@ def main():
         "gpu_launches": args.steps * 1 + args.steps * 1,
         "wall_s_timed": wall,
     }
+    if weak:
+        line["weak_scaling"] = weak
     line["clocks"] = clk.summary()
-    if kname in ("int32x", "tc"):
+    if kname in ("int32x", "tc", "int32x_dd"):
         # The integer and tensor-core kernels do not run the FP64-X algorithm:
         # their binding resource is instruction issue (one warp instruction per
         # cycle per SM sub-partition).  achieved = the kernel's warp
@@ -345,18 +471,23 @@ def main():
         sms = torch.cuda.get_device_properties(device).multi_processor_count
         peak_issue = 4.0 * sms * sm_mhz * 1e6
         inst = prof_rec.get("warp_inst_per_launch") if prof_rec else None
+        if inst and world > 1:
+            inst = inst / world  # a shard walks 1/world of the Gray range
         ach = inst / (mean_ms * 1e-3) if inst else None
         line["roofline"] = {"bound": "issue", "achieved": ach / 1e12 if ach else None,
                             "peak": peak_issue / 1e12, "unit": "Twarp-inst/s",
                             "frac": ach / peak_issue if ach else None, "traffic": traffic,
                             "peak_source": f"4 warp instructions / cycle / SM x {sms} SMs x "
                                            f"{sm_mhz:.0f} MHz (median sampled SM clock)",
-                            "algorithmic": "smsp__inst_executed.sum of one launch of this kernel and order (ncu, "
-                                           "profiles/ryser_dense_n40_issue.json)",
+                            "algorithmic": "smsp__inst_executed.sum of one launch of "
+                                           f"{kernel_template(kname, A)} (ncu, profiles/ryser_dense_n40_issue.json)",
                             "fp64_equivalent": fp64_equiv}
-
+        if prof_stale:
+            line["roofline"]["frac_stale"] = True
+            line["roofline"]["stale_reason"] = prof_stale
     line["config"]["kernel"] = {1: "FP64-X register kernel", 3: "int32-X register kernel",
-                                5: "tensor-core row sums (tcgen05 kind::i8) + int32 products"}.get(r.kernel, r.kernel)
+                                5: "tensor-core row sums (tcgen05 kind::i8) + int32 products",
+                                7: "int32-X register kernel, double-double products and sum"}.get(r.kernel, r.kernel)
     if rank == 0 and not args.no_secondary:
         line["secondary"] = secondary(pb, eng)
         # the same n=40 matrix through the int32-X and tensor-core kernels
@@ -377,7 +508,9 @@ def main():
             "kernel_ms": fr.kernel_ms, "steps_per_s": total_steps / (fr.kernel_ms * 1e-3),
             "fp64_frac_of_measured_peak": total_steps * ops_per_step / (fr.kernel_ms * 1e-3) / peak_ops,
             "rel_diff_vs_headline": abs(fr.value - perm_value) / abs(perm_value)}
-        line["secondary"]["reference_gpu_p4_same_box"] = reference_gpu(A)
+        line["secondary"]["reference_gpu_same_box"] = reference_gpu(
+            A, mean_ms, line["secondary"]["sparse_n36_d020_real"].get("auto_kernel_ms"),
+            policy["value"] if policy else None)
         line["secondary"]["batched_8192_n12_28"] = batched_secondary(pb, eng)
         line["secondary"]["serving_poisson_2000_per_s"] = serving_secondary(pb, baseline=True)
         line["secondary"]["serving_poisson_40_per_s"] = serving_secondary(pb, requests=120, rate=40.0)
@@ -391,6 +524,7 @@ def main():
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     res.free()
+    plain.close()
     eng.close()
     if dist is not None:
         dist.destroy_process_group()
@@ -399,52 +533,107 @@ def main():
     return 0
 
 
-class _Quiet:
-    """Silence fd 1 (the reference's functions print progress lines)."""
+class _Capture:
+    """Capture fd 1 (the reference's wrappers print their own kernel time,
+    `kernel in <seconds>`, gpu_exact_dense.cu:679-683)."""
 
     def __enter__(self):
+        import tempfile
+
         sys.stdout.flush()
         self.saved = os.dup(1)
-        devnull = os.open(os.devnull, os.O_WRONLY)
-        os.dup2(devnull, 1)
-        os.close(devnull)
+        self.tmp = tempfile.TemporaryFile(mode="w+")
+        os.dup2(self.tmp.fileno(), 1)
+        return self
 
     def __exit__(self, *exc):
         sys.stdout.flush()
         os.dup2(self.saved, 1)
         os.close(self.saved)
+        self.tmp.seek(0)
+        self.text = self.tmp.read()
+        self.tmp.close()
+
+    def kernel_seconds(self):
+        import re
+
+        m = re.findall(r"kernel in ([0-9.eE+-]+)", getattr(self, "text", ""))
+        return float(m[-1]) if m else None
 
 
-def reference_gpu(A40):
-    """The reference's own -p4 kernel (built for sm_100a from its sources) on the
-    same box: the n=30 binary case and a 32-order slice of the headline matrix."""
+def cfg2_matrix():
+    """The sparse exact configuration: n=36, Bernoulli(0.20) mask with no empty
+    row or column, values U(0,1], seed 2026 (tests/golden holds its
+    double-double value)."""
+    rng = np.random.default_rng(2026)
+    while True:
+        mk = rng.random((36, 36)) < 0.2
+        if mk.any(0).all() and mk.any(1).all():
+            break
+    return mk * (1.0 - rng.random((36, 36)))
+
+
+def golden_value(name: str):
     try:
-        import ctypes
+        data = json.loads((ROOT / "tests" / "golden" / "golden.json").read_text())
+        for c in data["cases"]:
+            if c["name"] == name:
+                return c["dd"][0] + c["dd"][1]
+    except Exception:
+        pass
+    return None
 
+
+def reference_gpu(A40, ours_n40_ms, ours_cfg2_ms, certified_n40):
+    """The reference's own GPU kernels (built for sm_100a from its sources) on
+    the same box, kernel against kernel: its wrappers time the kernel alone
+    (launch to cudaDeviceSynchronize, host clock, after a warm-up call that
+    creates the context) and print it; allocation and copies are outside.
+    -p4 (gpu_exact_dense.cu:641) on the headline n=40 matrix and -s -p7
+    (gpu_exact_sparse.cu:1124, skipOrder) on the sparse configuration, each
+    with its error against our certified value / the double-double oracle."""
+    try:
         sys.path.insert(0, str(ROOT / "oracle"))
         from oracle import Reference
 
         ref = Reference()
         out = {}
-        rng = np.random.default_rng(101)
-        while True:
-            m = (rng.random((30, 30)) < 0.5).astype(np.float64)
-            if m.any(0).all() and m.any(1).all():
-                break
-        for name, M in (("n30_binary", m), ("n32_int_slice_of_n40", np.ascontiguousarray(A40[:32, :32], dtype=np.float64))):
-            Mi = np.ascontiguousarray(M, dtype=np.int32)
-            with _Quiet():
-                ref.lib.ref_gpu_dense_mshared_i32(Mi.ctypes.data_as(ctypes.c_void_p), M.shape[0], 2048, 256)
-                t = time.perf_counter()
-                v = ref.lib.ref_gpu_dense_mshared_i32(Mi.ctypes.data_as(ctypes.c_void_p), M.shape[0], 2048, 256)
-                dt = time.perf_counter() - t
-            out[name] = {"seconds_incl_alloc_copy": dt, "steps_per_s": 2.0 ** (M.shape[0] - 1) / dt, "value": v}
+        # warm-up: context creation and module load on a small matrix
+        W = np.ascontiguousarray(np.ones((20, 20)), dtype=np.int32)
+        with _Capture():
+            ref.lib.ref_gpu_dense_mshared_i32(W.ctypes.data_as(ctypes.c_void_p), 20, 2048, 256)
+        Mi = np.ascontiguousarray(A40, dtype=np.int32)
+        with _Capture() as cap:
+            t = time.perf_counter()
+            v = ref.lib.ref_gpu_dense_mshared_i32(Mi.ctypes.data_as(ctypes.c_void_p), Mi.shape[0], 2048, 256)
+            wall = time.perf_counter() - t
+        ks = cap.kernel_seconds()
+        steps = 2.0 ** (Mi.shape[0] - 1)
+        out["p4_dense_n40_headline"] = {
+            "kernel_s": ks, "wall_s_incl_alloc_copy": wall, "steps_per_s": steps / ks if ks else None,
+            "value": v, "rel_error_vs_certified": abs(v - certified_n40) / abs(certified_n40) if certified_n40 else None,
+            "ours_kernel_s": ours_n40_ms * 1e-3,
+            "ours_speedup_kernel_vs_kernel": ks / (ours_n40_ms * 1e-3) if ks else None}
+        B = cfg2_matrix()
+        c = compress_for_reference(B)
+        want = golden_value("cfg2_sparse_real_n36_d020")
+        with _Capture() as cap:
+            t = time.perf_counter()
+            v = ref.lib.ref_gpu_skipper_f64(*c, 36, 2048, 128)
+            wall = time.perf_counter() - t
+        ks = cap.kernel_seconds()
+        out["p7_skipper_cfg2_n36_d020"] = {
+            "kernel_s": ks, "wall_s_incl_alloc_copy": wall, "dense_equivalent_steps_per_s": 2.0 ** 35 / ks if ks else None,
+            "value": v, "rel_error_vs_dd_oracle": abs(v - want) / abs(want) if want else None,
+            "ours_kernel_s": ours_cfg2_ms * 1e-3 if ours_cfg2_ms else None,
+            "ours_speedup_kernel_vs_kernel": ks / (ours_cfg2_ms * 1e-3) if ks and ours_cfg2_ms else None}
+        out["cuda_status_after"] = ref.lib.ref_last_cuda_error().decode()
         # its Monte-Carlo kernels (gpu_approximation_dense.cu:374, :528) on the
         # n=64 binary matrix of the mc_n64 secondary, 2e5 trials each, one call
         rng = np.random.default_rng(55)
         C = np.ascontiguousarray((rng.random((64, 64)) < 0.5).astype(np.float64))
         mc = {}
-        with _Quiet():
+        with _Capture():
             t = time.perf_counter()
             v = ref.lib.ref_gpu_rasmussen_f64(C.ctypes.data_as(ctypes.c_void_p), 64, 200000)
             mc["rasmussen_seconds_incl_alloc_copy"] = time.perf_counter() - t
@@ -459,6 +648,19 @@ def reference_gpu(A40):
         return out
     except Exception as e:  # reported, never fatal
         return {"unavailable": str(e)}
+
+
+def compress_for_reference(B):
+    """skipOrder CRS/CCS (util.h:622) of B as the reference's SkipPer wrapper
+    takes them: (mat, rptrs, cols, cptrs, rows, cvals) pointers, arrays kept
+    alive on the function object."""
+    pb = sys.modules["perman_b200"]
+    c = pb.compress(2, B)
+    arrs = [np.ascontiguousarray(c["mat"], dtype=np.float64), np.ascontiguousarray(c["rptrs"], dtype=np.int32),
+            np.ascontiguousarray(c["cols"], dtype=np.int32), np.ascontiguousarray(c["cptrs"], dtype=np.int32),
+            np.ascontiguousarray(c["rows"], dtype=np.int32), np.ascontiguousarray(c["cvals"], dtype=np.float64)]
+    compress_for_reference.keep = arrs
+    return [a.ctypes.data_as(ctypes.c_void_p) for a in arrs]
 
 
 def batched_secondary(pb, eng, count=8192):

@@ -53,6 +53,14 @@ extern "C" {
                                    integer matrices, |a| <= 63, orders 16..64 */
 #define PERM_KERNEL_DENSE_SPLIT 6 /* split-X Gray-code Ryser: exact coarse row sums
                                      plus a small remainder, orders 4..40 */
+#define PERM_KERNEL_DENSE_INT_DD 7 /* int32-X Gray-code Ryser with double-double
+                                      products and sum: certified error bound for
+                                      integer matrices, orders 8..64 */
+#define PERM_KERNEL_DENSE_SDD 8 /* split X with double-double products and sum
+                                   ("split-dd"): certified error bound for real
+                                   matrices, orders 4..40; sparse matrices whose
+                                   three sparsest columns touch <= 16 rows walk
+                                   only those rows at 7 of 8 steps (orders 12..40) */
 
 /* Limits of this build. */
 #define PERM_MAX_EXACT_N 64  /* Gray indices are 64-bit                 */
@@ -123,9 +131,11 @@ int perm_exact_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols, c
 /* As perm_exact_sparse with an explicit kernel.  variant 0 (what
  * perm_exact_sparse uses) estimates the share of vanishing Gray terms from a
  * fixed sample of 2048 indices and runs SkipPer when at least 75% vanish, the
- * register kernels on the same (CRS) matrix otherwise; PERM_KERNEL_SKIPPER,
- * PERM_KERNEL_DENSE and PERM_KERNEL_DENSE_INT force a kernel.  perm_result.kernel
- * reports which ran. */
+ * register kernels on the same (CRS) matrix otherwise (through
+ * perm_exact_dense_ex's variant 0 and its accuracy policy); PERM_KERNEL_SKIPPER,
+ * PERM_KERNEL_DENSE, PERM_KERNEL_DENSE_INT, PERM_KERNEL_DENSE_TC,
+ * PERM_KERNEL_DENSE_INT_DD and PERM_KERNEL_DENSE_SDD force a kernel.
+ * perm_result.kernel reports which ran. */
 int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, const int* cols, const double* rvals,
                          const int* cptrs, const int* rows, const double* cvals, int variant, perm_result* out);
 
@@ -133,18 +143,28 @@ int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, const int* cols
  * int32-X kernel for integer matrices whose grouped row products provably fit
  * in int32, the FP64-X kernel otherwise; perm_dense_autotune can switch
  * integer inputs to the FP64-X or the tensor-core kernel), PERM_KERNEL_DENSE
- * forces FP64 X, PERM_KERNEL_DENSE_INT forces int32 X and PERM_KERNEL_DENSE_TC
- * the tensor-core kernel (PERM_EUNSUPPORTED where not exact).  The
+ * forces FP64 X, PERM_KERNEL_DENSE_INT forces int32 X, PERM_KERNEL_DENSE_TC
+ * the tensor-core kernel (PERM_EUNSUPPORTED where not exact),
+ * PERM_KERNEL_DENSE_INT_DD and PERM_KERNEL_DENSE_SDD the certified kernels
+ * (integer / real matrices; PERM_EUNSUPPORTED outside their orders).  The
  * tensor-core kernel runs whole walks only: with nshards > 1 its matrices use
  * the int32-X kernel. */
 int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard, int nshards,
                         perm_result* out);
 /* Whole-walk dense results carry rel_error_estimate, a worst-case bound
  * formed from sum |term|, estimated by a sample of Ryser terms stratified by
- * subset size (exact for the split-X kernel, whose walk sums its own terms).
+ * subset size (exact for the split-X and the certified kernels, whose walks
+ * sum their own terms).  The certified kernels' bound is of order
+ * n u^2 sum|term| / |perm| (u = 2^-53): it meets 1e-10 unless the terms
+ * cancel by more than ~1e18.
  * With variant 0 and a context target (default 1e-10; <= 0 disables the
  * policy; < 0 also skips the estimate):
  *  - a zero pattern without a perfect matching returns exactly 0;
+ *  - whole walks of integer matrices whose group products fit in int32 run
+ *    PERM_KERNEL_DENSE_INT_DD at once (about 1.2 int32-X walks), and real
+ *    matrices of order 12..40 whose three sparsest columns touch at most 16
+ *    rows run PERM_KERNEL_DENSE_SDD in its sparse layout: their bound is the
+ *    estimate, no other step runs;
  *  - a result whose bound exceeds the target is cross-checked against
  *    B = A^T with its first row times 3 (perm(B) = 3 perm(A), independent
  *    roundings) and kept when max(4-sigma independent-rounding estimate from
@@ -153,9 +173,34 @@ int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int va
  *  - after an FP64-X first pass (orders 4..40) the same check runs on split-X
  *    walks of A and B, returning the split-X value (kernel
  *    PERM_KERNEL_DENSE_SPLIT) when it passes;
- *  - otherwise it is recomputed by the double-double kernel (orders <= 40).
+ *  - otherwise it is recomputed by a certified kernel: PERM_KERNEL_DENSE_INT_DD
+ *    (integer, orders 8..64, directly after an int32-X first pass),
+ *    PERM_KERNEL_DENSE_SDD (orders 4..40) or the double-double kernel (orders
+ *    <= 40, where neither applies).
  * kernel_ms covers every launch.  PERM_KERNEL_DENSE_DD forces that kernel. */
 int perm_ctx_set_rel_target(perm_ctx* ctx, double rel_target);
+
+/* Failure-injection hook for tests of the bounded device waits.  The next
+ * `launches` launches of the FP64-X dense kernel (PERM_KERNEL_DENSE) or of
+ * the tensor-core kernel (PERM_KERNEL_DENSE_TC) on this context wait on a
+ * barrier that never completes: the FP64-X kernel's operand staging expects
+ * 16 bytes more than it copies (every copy still lands), the tensor-core
+ * kernel's buffer-free barriers expect one arrival more than its consumers
+ * make (its issued MMAs still complete and are drained).  Each bounded wait
+ * gives up after its limit (a fraction of a second), the call returns
+ * PERM_ETIMEOUT with a message naming the wait, nothing is left running on
+ * the device, and the context stays usable.  0 switches it off.  No
+ * counterpart in the reference (which has no device waits to bound). */
+int perm_ctx_inject_wait_timeout(perm_ctx* ctx, int launches);
+
+/* Host only (no device): the layout PERM_KERNEL_DENSE_SDD uses for the
+ * row-major n x n matrix `mat`: the number of inner rows R of the sparse
+ * layout (6, 8, 12 or 16: columns 0..2 after its permutation touch rows
+ * 0..R-1 only, so 7 of 8 Gray steps walk R rows), 0 for the dense layout,
+ * PERM_EUNSUPPORTED where the kernel does not apply (orders outside 4..40,
+ * row absolute sums at or above 2^1020), PERM_EINVAL for bad arguments.
+ * No counterpart in the reference. */
+int perm_sdd_layout(const double* mat, int n);
 
 /* Measures, for orders n_lo..n_hi (within 8..40), which of the int32-X, the
  * FP64-X and (n >= 16) the tensor-core kernel is fastest on this device for
@@ -169,6 +214,12 @@ int perm_matrix_create_dense(perm_ctx* ctx, const void* mat, int n, int dtype, p
 int perm_matrix_create_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, perm_matrix** out);
 void perm_matrix_destroy(perm_ctx* ctx, perm_matrix* m);
 int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, perm_result* out);
+/* Shard `shard` of `nshards` of a resident matrix's walk (the ranges of
+ * perm_exact_dense_shard / perm_shard_range); the tensor-core kernel runs
+ * whole walks only (PERM_EINVAL for nshards > 1).  Replaces the per-device
+ * ranges of gpu_exact_dense.cu:729-752 without a host copy per call. */
+int perm_exact_dense_resident_shard(perm_ctx* ctx, const perm_matrix* m, int shard, int nshards,
+                                    perm_result* out);
 
 /* The tensor-core kernel over rounds [round0, round0 + nrounds) only: the
  * subsets whose columns 9 .. n-2 follow the Gray code of the round index,

@@ -32,6 +32,8 @@ PERM_F64, PERM_F32, PERM_I32 = 0, 1, 2
 PERM_KERNEL_DENSE, PERM_KERNEL_SKIPPER, PERM_KERNEL_DENSE_INT, PERM_KERNEL_DENSE_DD = 1, 2, 3, 4
 PERM_KERNEL_DENSE_TC = 5
 PERM_KERNEL_DENSE_SPLIT = 6
+PERM_KERNEL_DENSE_INT_DD = 7
+PERM_KERNEL_DENSE_SDD = 8
 MAX_EXACT_N = 64
 MAX_MC_N = 64
 MAX_MC_SPARSE_N = 2047
@@ -41,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
-    "perm_exact_dense_resident", "perm_exact_dense_refine", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target",
+    "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
     "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
@@ -116,12 +118,14 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_exact_dense_shard": (i, [_P, _P, i, i, i, i, ctypes.POINTER(PermResult)]),
         "perm_exact_dense_ex": (i, [_P, _P, i, i, i, i, i, ctypes.POINTER(PermResult)]),
         "perm_shard_range": (i, [i, i, i, ctypes.POINTER(u64), ctypes.POINTER(u64)]),
+        "perm_sdd_layout": (i, [_P, i]),
         "perm_matrix_create_dense_ex": (i, [_P, _P, i, i, i, ctypes.POINTER(_P)]),
         "perm_exact_sparse": (i, [_P, i, _P, _P, _P, _P, _P, _P, ctypes.POINTER(PermResult)]),
         "perm_exact_sparse_ex": (i, [_P, i, _P, _P, _P, _P, _P, _P, i, ctypes.POINTER(PermResult)]),
         "perm_matrix_create_dense": (i, [_P, _P, i, i, ctypes.POINTER(_P)]),
         "perm_matrix_destroy": (None, [_P, _P]),
         "perm_exact_dense_resident": (i, [_P, _P, ctypes.POINTER(PermResult)]),
+        "perm_exact_dense_resident_shard": (i, [_P, _P, i, i, ctypes.POINTER(PermResult)]),
         "perm_exact_dense_refine": (i, [_P, _P, i, i, ctypes.POINTER(PermResult)]),
         "perm_exact_dense_tc_rounds": (i, [_P, _P, i, i, u64, u64, ctypes.POINTER(PermResult)]),
         "perm_approx_rasmussen": (i, [_P, _P, i, i, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
@@ -142,6 +146,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_batch_autotune": (i, [_P, i, i, _P]),
         "perm_dense_autotune": (i, [_P, i, i, _P]),
         "perm_ctx_set_rel_target": (i, [_P, d]),
+        "perm_ctx_inject_wait_timeout": (i, [_P, i]),
         "perm_server_create": (i, [i, i, ctypes.c_size_t, u64, ctypes.POINTER(_P)]),
         "perm_server_submit": (i, [_P, ctypes.POINTER(PermRequest), ctypes.POINTER(u64)]),
         "perm_server_wait": (i, [_P, u64, i, ctypes.POINTER(PermResponse)]),
@@ -242,7 +247,9 @@ class Engine:
     def exact_dense(self, mat, variant: int = 0) -> ExactResult:
         """Dense Ryser; variant 0 = automatic, PERM_KERNEL_DENSE = FP64 X, PERM_KERNEL_DENSE_INT = int32 X,
         PERM_KERNEL_DENSE_TC = tensor-core row sums, PERM_KERNEL_DENSE_DD = double-double,
-        PERM_KERNEL_DENSE_SPLIT = split X (exact coarse row sums, orders 4..40)."""
+        PERM_KERNEL_DENSE_SPLIT = split X (exact coarse row sums, orders 4..40),
+        PERM_KERNEL_DENSE_INT_DD / PERM_KERNEL_DENSE_SDD = the certified int32-X /
+        split-dd walks."""
         a, dt = _as_matrix(mat)
         r = PermResult()
         if variant:
@@ -365,6 +372,13 @@ class Engine:
         estimate without the policy, < 0 skips the estimate too."""
         self._check(self.lib.perm_ctx_set_rel_target(self.ctx, target))
 
+    def inject_wait_timeout(self, launches: int = 1):
+        """Failure injection for tests (perm_ctx_inject_wait_timeout): the next
+        `launches` FP64-X or tensor-core dense launches wait on a barrier that
+        never completes, give up after their bounded wait and fail with
+        PERM_ETIMEOUT; the context stays usable."""
+        self._check(self.lib.perm_ctx_inject_wait_timeout(self.ctx, launches))
+
     def dense_autotune(self, n_lo: int, n_hi: int) -> dict:
         """Per order: which register kernel the automatic choice uses for integer inputs."""
         out = np.zeros(n_hi - n_lo + 1, dtype=np.int32)
@@ -419,6 +433,13 @@ class ResidentMatrix:
         r = PermResult()
         self.engine._check(self.engine.lib.perm_exact_dense_resident(self.engine.ctx, self.handle,
                                                                      ctypes.byref(r)))
+        return _exact(r)
+
+    def run_shard(self, shard: int, nshards: int) -> ExactResult:
+        """Shard `shard` of `nshards` of the walk (perm_exact_dense_resident_shard)."""
+        r = PermResult()
+        self.engine._check(self.engine.lib.perm_exact_dense_resident_shard(self.engine.ctx, self.handle, shard,
+                                                                           nshards, ctypes.byref(r)))
         return _exact(r)
 
     def free(self):
@@ -525,6 +546,14 @@ def compress(mode: int, mat) -> dict:
         raise PermError(nnz, "perm_compress failed")
     return {"n": n, "nnz": nnz, "mat": a, "cptrs": cptrs, "rows": rows[:nnz], "cvals": cvals[:nnz],
             "rptrs": rptrs, "cols": cols[:nnz], "rvals": rvals[:nnz]}
+
+
+def sdd_layout(mat) -> int:
+    """Inner rows of the split-dd kernel's sparse layout for this matrix
+    (perm_sdd_layout; host only): 6, 8, 12 or 16, 0 for the dense layout,
+    negative where the kernel does not apply."""
+    a = np.ascontiguousarray(mat, dtype=np.float64)
+    return int(load_library().perm_sdd_layout(_ptr(a), a.shape[0]))
 
 
 def shard_range(n: int, shard: int, nshards: int) -> tuple[int, int]:

@@ -38,6 +38,8 @@
 #include "ryser_dense_split.cuh"
 #include "ryser_dense_tc.cuh"
 #include "ryser_dense_int.cuh"
+#include "ryser_dense_intc.cuh"
+#include "ryser_dense_sdd.cuh"
 #include "skipper.h"
 
 namespace perm {
@@ -54,6 +56,17 @@ const void* dense_int_kernel_g6(int n);
 
 const void* dense_dd_kernel(int n);
 const void* dense_split_kernel(int n);
+
+const void* dense_intc_kernel_g3(int n);
+const void* dense_intc_kernel_g4(int n);
+const void* dense_intc_kernel_g5(int n);
+const void* dense_intc_kernel_g6(int n);
+
+const void* dense_sdd_kernel(int n);
+const void* sparse_sdd_kernel_r6(int n);
+const void* sparse_sdd_kernel_r8(int n);
+const void* sparse_sdd_kernel_r12(int n);
+const void* sparse_sdd_kernel_r16(int n);
 
 const void* dense_tc_kernel_g3(int n);
 const void* dense_tc_kernel_g4(int n);
@@ -76,6 +89,30 @@ static const void* dense_int_kernel(int n, int g) {
     case 4: return dense_int_kernel_g4(n);
     case 5: return dense_int_kernel_g5(n);
     case 6: return dense_int_kernel_g6(n);
+    default: return nullptr;
+  }
+}
+
+static const void* dense_intc_kernel(int n, int g) {
+  switch (g) {
+    case 3: return dense_intc_kernel_g3(n);
+    case 4: return dense_intc_kernel_g4(n);
+    case 5: return dense_intc_kernel_g5(n);
+    case 6: return dense_intc_kernel_g6(n);
+    default: return nullptr;
+  }
+}
+
+// Inner-row counts of the sparse split-dd layout (ryser_sparse_sdd_kernel<N, R>).
+constexpr int kSparseInner[4] = {6, 8, 12, 16};
+
+static const void* sdd_kernel(int n, int inner) {
+  switch (inner) {
+    case 0: return dense_sdd_kernel(n);
+    case 6: return sparse_sdd_kernel_r6(n);
+    case 8: return sparse_sdd_kernel_r8(n);
+    case 12: return sparse_sdd_kernel_r12(n);
+    case 16: return sparse_sdd_kernel_r16(n);
     default: return nullptr;
   }
 }
@@ -235,12 +272,18 @@ struct perm_ctx {
   size_t h_stage_cap = 0;
   double* d_trials = nullptr;
   size_t d_trials_cap = 0;
-  int dense_occ[13][PERM_MAX_EXACT_N + 1] = {};  // [0]: FP64-X, [G]: int32-X, [7]: dd, [8 + G - 3]: tensor core, [12]: split X
+  // occupancy per kernel family and order: [0] FP64-X, [G] int32-X, [7] dd,
+  // [8 + G - 3] tensor core, [12] split X, [13 + G - 3] certified int32-X,
+  // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows
+  int dense_occ[22][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
   double* d_est = nullptr;                       // sample-kernel / split-walk moment accumulator
   double split_m1 = 0, split_m2 = 0;             // last split-X walk: sum |term|, sum term^2
+  double walk_m1 = 0;                            // last certified (int32-X dd or split-dd) walk: sum |term|
+  uint64_t walk_terms_per_thread = 0;            // ... and its longest thread range
+  int inject_timeouts = 0;                       // failure injection: launches left to inject into
   int batch_occ = 0;
   std::string err;
   std::mutex mu;
@@ -437,7 +480,8 @@ static int finish_and_read(perm_ctx* ctx, int nout) {
   if (errflag) {
     cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    return fail(ctx, PERM_ETIMEOUT, "shared-memory staging wait timed out on device %d", ctx->device);
+    return fail(ctx, PERM_ETIMEOUT, "%s wait timed out on device %d",
+                errflag == 3 ? "tensor-core pipeline" : "shared-memory staging", ctx->device);
   }
   return PERM_OK;
 }
@@ -450,6 +494,7 @@ static int finish_and_read(perm_ctx* ctx, int nout) {
 // rounded up to a multiple of 4) for the int32-X kernel.
 struct DenseOperand {
   int n = 0, variant = PERM_KERNEL_DENSE, group = 0;
+  int inner = 0;  // split-dd: rows 0..inner-1 hold the support of columns 0..2 (0: dense layout)
   std::vector<unsigned char> image;
 };
 
@@ -553,6 +598,74 @@ static int build_split_operand(perm_ctx* ctx, const std::vector<double>& a, int 
   return PERM_OK;
 }
 
+// The three columns whose nonzeros lie in the fewest rows (exhaustive over
+// column triples): returns the size of that row set and the columns.
+static int sparsest_column_triple(const std::vector<double>& a, int n, int* c3) {
+  std::vector<uint64_t> sup(n, 0);
+  for (int j = 0; j < n; j++)
+    for (int k = 0; k < n; k++)
+      if (a[(size_t)j * n + k] != 0.0) sup[k] |= 1ull << j;
+  int best = n + 1;
+  for (int c0 = 0; c0 < n; c0++)
+    for (int c1 = c0 + 1; c1 < n; c1++)
+      for (int c2 = c1 + 1; c2 < n; c2++) {
+        const int pc = __builtin_popcountll(sup[c0] | sup[c1] | sup[c2]);
+        if (pc < best) {
+          best = pc;
+          c3[0] = c0;
+          c3[1] = c1;
+          c3[2] = c2;
+        }
+      }
+  return best;
+}
+
+// Inner-row count of the sparse split-dd layout for this matrix (0: dense
+// layout): the smallest kSparseInner entry that holds the rows of the three
+// sparsest columns, for orders 12..40.
+static int sdd_inner_rows(const std::vector<double>& a, int n, int* c3) {
+  if (n < 12 || n > 40) return 0;
+  const int u = sparsest_column_triple(a, n, c3);
+  for (int r : kSparseInner)
+    if (u <= r && r + 4 <= n) return r;
+  return 0;
+}
+
+// Split-dd operand (ryser_dense_sdd.cuh): the split-X image, of the matrix
+// itself (dense layout) or, when three columns have their nonzeros in at
+// most 16 rows, of the matrix with those columns moved to positions 0..2
+// and their rows to the top (the sparse layout; the permanent is invariant
+// under row and column permutations).
+static int build_sdd_operand(perm_ctx* ctx, const std::vector<double>& a, int n, DenseOperand* op) {
+  if (n < 4 || n > 40) return fail(ctx, PERM_EUNSUPPORTED, "split-dd kernel covers orders 4..40 (got %d)", n);
+  int c3[3] = {0, 1, 2};
+  const int inner = sdd_inner_rows(a, n, c3);
+  int rc;
+  if (inner) {
+    std::vector<int> cols = {c3[0], c3[1], c3[2]}, rows;
+    for (int k = 0; k < n; k++)
+      if (k != c3[0] && k != c3[1] && k != c3[2]) cols.push_back(k);
+    std::vector<char> in_union(n, 0);
+    for (int j = 0; j < n; j++)
+      for (int t = 0; t < 3; t++)
+        if (a[(size_t)j * n + c3[t]] != 0.0) in_union[j] = 1;
+    for (int j = 0; j < n; j++)
+      if (in_union[j]) rows.push_back(j);
+    for (int j = 0; j < n; j++)
+      if (!in_union[j]) rows.push_back(j);
+    std::vector<double> p((size_t)n * n);
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < n; k++) p[(size_t)i * n + k] = a[(size_t)rows[i] * n + cols[k]];
+    rc = build_split_operand(ctx, p, n, op);
+  } else {
+    rc = build_split_operand(ctx, a, n, op);
+  }
+  if (rc) return rc;
+  op->variant = PERM_KERNEL_DENSE_SDD;
+  op->inner = inner;
+  return PERM_OK;
+}
+
 static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, DenseOperand* op) {
   std::vector<double> a((size_t)n * n);
   for (size_t i = 0; i < a.size(); i++) a[i] = elem(mat, dtype, i);
@@ -560,10 +673,11 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
   const int pref = variant == 0 && n <= PERM_MAX_EXACT_N ? ctx->dense_pref[n] : 0;
   const bool prefer_fp64 = pref == PERM_KERNEL_DENSE;
   if (variant == PERM_KERNEL_DENSE_SPLIT) return build_split_operand(ctx, a, n, op);
+  if (variant == PERM_KERNEL_DENSE_SDD) return build_sdd_operand(ctx, a, n, op);
   int G = (variant == PERM_KERNEL_DENSE || variant == PERM_KERNEL_DENSE_DD || prefer_fp64) ? 0 : int_group_size(a, n);
-  if (variant == PERM_KERNEL_DENSE_INT && G == 0)
+  if ((variant == PERM_KERNEL_DENSE_INT || variant == PERM_KERNEL_DENSE_INT_DD) && G == 0)
     return fail(ctx, PERM_EUNSUPPORTED,
-                "int32-X kernel needs an integer matrix of order >= 8 whose row products fit in int32");
+                "int32-X kernels need an integer matrix of order >= 8 whose row products fit in int32");
   const bool tc_ok = G && tc_eligible(a, n);
   if (variant == PERM_KERNEL_DENSE_TC && !tc_ok)
     return fail(ctx, PERM_EUNSUPPORTED,
@@ -573,7 +687,8 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
     const int np4 = (n + 3) & ~3;
     op->variant = (variant == PERM_KERNEL_DENSE_TC || (variant == 0 && pref == PERM_KERNEL_DENSE_TC && tc_ok))
                       ? PERM_KERNEL_DENSE_TC
-                      : PERM_KERNEL_DENSE_INT;
+                  : variant == PERM_KERNEL_DENSE_INT_DD ? PERM_KERNEL_DENSE_INT_DD
+                                                        : PERM_KERNEL_DENSE_INT;
     op->group = G;
     op->image.assign(sizeof(int) * (size_t)(n + 1) * np4, 0);
     int* img = reinterpret_cast<int*>(op->image.data());
@@ -604,6 +719,8 @@ struct perm_matrix {
 
 static const void* operand_kernel(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_kernel(op.n, op.group);
+  if (op.variant == PERM_KERNEL_DENSE_INT_DD) return dense_intc_kernel(op.n, op.group);
+  if (op.variant == PERM_KERNEL_DENSE_SDD) return sdd_kernel(op.n, op.inner);
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
   if (op.variant == PERM_KERNEL_DENSE_SPLIT) return dense_split_kernel(op.n);
@@ -611,7 +728,9 @@ static const void* operand_kernel(const DenseOperand& op) {
 }
 static int operand_threads(const DenseOperand& op) { return op.variant == PERM_KERNEL_DENSE_TC ? kTcThreads : 128; }
 static size_t operand_smem(const DenseOperand& op) {
-  if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_smem_bytes(op.n);
+  if (op.variant == PERM_KERNEL_DENSE_INT || op.variant == PERM_KERNEL_DENSE_INT_DD) return dense_int_smem_bytes(op.n);
+  if (op.variant == PERM_KERNEL_DENSE_SDD)
+    return op.inner ? sparse_sdd_smem_bytes(op.n, op.inner, 128) : dense_sdd_smem_bytes(op.n);
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_smem_bytes(op.n);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_smem_bytes(op.n);
   if (op.variant == PERM_KERNEL_DENSE_SPLIT) return dense_split_smem_bytes(op.n);
@@ -642,6 +761,14 @@ static void shard_bounds(int n, int shard, int nshards, uint64_t* first, uint64_
   if (ms_out) *ms_out = ms;
 }
 
+extern "C" int perm_sdd_layout(const double* mat, int n) {
+  if (!mat || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
+  std::vector<double> a(mat, mat + (size_t)n * n);
+  if (n < 4 || n > 40 || !split_rows_ok(a, n)) return PERM_EUNSUPPORTED;
+  int c3[3];
+  return sdd_inner_rows(a, n, c3);
+}
+
 extern "C" int perm_shard_range(int n, int shard, int nshards, uint64_t* first, uint64_t* last) {
   if (n < 1 || n > PERM_MAX_EXACT_N || nshards < 1 || shard < 0 || shard >= nshards || !first || !last)
     return PERM_EINVAL;
@@ -653,10 +780,15 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
   const int n = op.n;
   const void* fn = operand_kernel(op);
   if (!fn) return fail(ctx, PERM_EUNSUPPORTED, "dense exact order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
+  int sparse_slot = 0;
+  for (int i = 0; i < 4; i++)
+    if (op.inner == kSparseInner[i]) sparse_slot = 18 + i;
   int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? op.group
                                  : op.variant == PERM_KERNEL_DENSE_DD ? 7
                                  : op.variant == PERM_KERNEL_DENSE_TC ? 8 + op.group - 3
-                                 : op.variant == PERM_KERNEL_DENSE_SPLIT ? 12 : 0][n];
+                                 : op.variant == PERM_KERNEL_DENSE_SPLIT ? 12
+                                 : op.variant == PERM_KERNEL_DENSE_INT_DD ? 13 + op.group - 3
+                                 : op.variant == PERM_KERNEL_DENSE_SDD ? (op.inner ? sparse_slot : 17) : 0][n];
   if (!occ_slot) {
     int rc = allow_smem(ctx, fn, operand_smem(op));
     if (rc) return rc;
@@ -714,11 +846,44 @@ static int dense_launch(perm_ctx* ctx, const DenseOperand& op, const void* d_ima
     args.ticket = ctx->ticket;
     args.out = ctx->d_out;
     args.err = ctx->d_err;
+    args.inject = ctx->inject_timeouts > 0 ? 1 : 0;
+    if (args.inject) ctx->inject_timeouts--;
     void* kargs[] = {&args};
     CU(ctx, cudaLaunchKernel(operand_kernel(op), dim3(p.grid), dim3(kTcThreads), kargs, operand_smem(op),
                              ctx->stream));
   } else if (op.variant == PERM_KERNEL_DENSE_SPLIT) {
     DenseSplitArgs args;
+    args.img = static_cast<const double*>(d_image);
+    args.np = (n + 1) & ~1;
+    args.m = p.m;
+    args.block0 = p.block0;
+    args.nblocks = p.nblocks;
+    args.partials = ctx->partials;
+    args.ticket = ctx->ticket;
+    args.out = ctx->d_out;
+    args.sums = ctx->d_est;
+    args.err = ctx->d_err;
+    void* kargs[] = {&args};
+    CU(ctx, cudaMemsetAsync(ctx->d_est, 0, 2 * sizeof(double), ctx->stream));
+    CU(ctx, cudaLaunchKernel(operand_kernel(op), dim3(p.grid), dim3(128), kargs, operand_smem(op), ctx->stream));
+  } else if (op.variant == PERM_KERNEL_DENSE_INT_DD) {
+    DenseIntcArgs args;
+    const int np4 = (n + 3) & ~3;
+    args.colI = static_cast<const int*>(d_image);
+    args.np4 = np4;
+    args.m = p.m;
+    args.block0 = p.block0;
+    args.nblocks = p.nblocks;
+    args.partials = ctx->partials;
+    args.ticket = ctx->ticket;
+    args.out = ctx->d_out;
+    args.sums = ctx->d_est;
+    args.err = ctx->d_err;
+    void* kargs[] = {&args};
+    CU(ctx, cudaMemsetAsync(ctx->d_est, 0, 2 * sizeof(double), ctx->stream));
+    CU(ctx, cudaLaunchKernel(operand_kernel(op), dim3(p.grid), dim3(128), kargs, operand_smem(op), ctx->stream));
+  } else if (op.variant == PERM_KERNEL_DENSE_SDD) {
+    DenseSddArgs args;
     args.img = static_cast<const double*>(d_image);
     args.np = (n + 1) & ~1;
     args.m = p.m;
@@ -760,6 +925,8 @@ static int dense_launch(perm_ctx* ctx, const DenseOperand& op, const void* d_ima
     args.ticket = ctx->ticket;
     args.out = ctx->d_out;
     args.err = ctx->d_err;
+    args.inject = ctx->inject_timeouts > 0 && op.variant == PERM_KERNEL_DENSE ? 16u : 0u;
+    if (args.inject) ctx->inject_timeouts--;
     void* kargs[] = {&args};
     CU(ctx, cudaLaunchKernel(operand_kernel(op), dim3(p.grid), dim3(128), kargs, operand_smem(op), ctx->stream));
   }
@@ -768,13 +935,20 @@ static int dense_launch(perm_ctx* ctx, const DenseOperand& op, const void* d_ima
 }
 
 static int dense_collect(perm_ctx* ctx, const DenseOperand& op, const DensePlan& p, perm_result* out) {
-  if (op.variant == PERM_KERNEL_DENSE_SPLIT)
+  const bool sums = op.variant == PERM_KERNEL_DENSE_SPLIT || op.variant == PERM_KERNEL_DENSE_INT_DD ||
+                    op.variant == PERM_KERNEL_DENSE_SDD;
+  if (sums)
     CU(ctx, cudaMemcpyAsync(ctx->h_out + 12, ctx->d_est, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   int rc = finish_and_read(ctx, 2);
   if (rc != PERM_OK) return rc;
   if (op.variant == PERM_KERNEL_DENSE_SPLIT) {
     ctx->split_m1 = ctx->h_out[12] * 2.0;  // |factor| = 2
     ctx->split_m2 = ctx->h_out[13] * 4.0;
+  } else if (sums) {
+    // the int32-X walk's terms are prod y = 2^n prod x (|factor| 2^(1-n))
+    ctx->walk_m1 = ctx->h_out[12] * (op.variant == PERM_KERNEL_DENSE_INT_DD ? std::ldexp(1.0, 1 - op.n) : 2.0);
+    const uint64_t threads = (uint64_t)p.grid * 128;
+    ctx->walk_terms_per_thread = ((p.nblocks + threads - 1) / threads) << p.m;
   }
   float ms = 0;
   CU(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
@@ -802,7 +976,8 @@ static int check_dense_args(perm_ctx* ctx, const void* mat, int n, int dtype, co
 
 static int check_variant(perm_ctx* ctx, int variant) {
   if (variant != 0 && variant != PERM_KERNEL_DENSE && variant != PERM_KERNEL_DENSE_INT &&
-      variant != PERM_KERNEL_DENSE_DD && variant != PERM_KERNEL_DENSE_TC && variant != PERM_KERNEL_DENSE_SPLIT)
+      variant != PERM_KERNEL_DENSE_DD && variant != PERM_KERNEL_DENSE_TC && variant != PERM_KERNEL_DENSE_SPLIT &&
+      variant != PERM_KERNEL_DENSE_INT_DD && variant != PERM_KERNEL_DENSE_SDD)
     return fail(ctx, PERM_EINVAL, "unknown dense kernel variant %d", variant);
   return PERM_OK;
 }
@@ -820,22 +995,36 @@ static int check_variant(perm_ctx* ctx, int variant) {
 //    independent and uniform (variance u^2 / 3 each), 4 u sqrt(r / 3)
 //    sqrt(S2) / |perm|.  Not a bound -- terms with equal values round alike --
 //    so it is only used together with an independent second evaluation;
-//  * double-double: (4n + 32) u^2 S1 / |perm|.
+//  * double-double: (4n + 32) u^2 S1 / |perm|;
+//  * certified walks (int32 X with double-double products, split-dd), whose
+//    S1 is the walk's own exact sum: products of relative error below
+//    ~4u^2 per factor (8 ceil(n/G) or 8n in all), Sum2 of each Gray group of
+//    eight and of the groups of one thread range (256, plus (K/4)^2 for the
+//    low-part sum over K terms per thread), the double-double reductions;
+//    for split-dd also the drift of the remainder row sums xl over K updates
+//    (64 n^2 K).  Plus u for rounding hi + lo to one double.
 constexpr int kSamplesPerClass = 8192;  // term-moment sample: threads per subset-size class
 
 struct ErrEstimate {
   double s1 = 0, s2 = 0, worst = 0, random = 0;
 };
 
-// bounds of `variant`'s rounding error from the sampled sums of |term| and term^2
-static void error_bounds(int variant, int group, int n, double value, ErrEstimate* e) {
+// bounds of `variant`'s rounding error from the sums of |term| and term^2
+// (sampled, or the walk's own); k_terms = the longest thread range of a
+// certified walk
+static void error_bounds(int variant, int group, int n, double value, ErrEstimate* e, uint64_t k_terms = 0) {
   const double u = std::ldexp(1.0, -53);
   const double av = std::fabs(value), s1 = e->s1, s2 = e->s2;
   if (av == 0.0) {
     e->worst = e->random = s1 > 0 ? INFINITY : 0.0;
     return;
   }
-  if (variant == PERM_KERNEL_DENSE_DD) {
+  if (variant == PERM_KERNEL_DENSE_INT_DD || variant == PERM_KERNEL_DENSE_SDD) {
+    const double k = (double)k_terms;
+    const double prod = variant == PERM_KERNEL_DENSE_INT_DD ? 8.0 * std::ceil((double)n / group) : 8.0 * n;
+    const double drift = variant == PERM_KERNEL_DENSE_SDD ? 64.0 * n * n * k : 0.0;
+    e->worst = e->random = (prod + 256.0 + (k / 4) * (k / 4) + drift) * u * u * s1 / av + u;
+  } else if (variant == PERM_KERNEL_DENSE_DD) {
     e->worst = e->random = (4.0 * n + 32.0) * u * u * s1 / av;
   } else if (variant == PERM_KERNEL_DENSE_SPLIT) {
     // exact coarse X: one combine per entry and n - 1 product roundings, each
@@ -868,6 +1057,13 @@ static int estimate_error(perm_ctx* ctx, const void* d_col_fp64, int n, const De
   e->s1 = ctx->h_out[12] * 2.0;  // |factor| = 2
   e->s2 = ctx->h_out[13] * 4.0;
   error_bounds(op.variant, op.group, n, value, e);
+  return PERM_OK;
+}
+
+extern "C" int perm_ctx_inject_wait_timeout(perm_ctx* ctx, int launches) {
+  if (!ctx || launches < 0) return PERM_EINVAL;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->inject_timeouts = launches;
   return PERM_OK;
 }
 
@@ -931,9 +1127,14 @@ static bool has_perfect_matching(const void* mat, int n, int dtype) {
 //     above the target);
 //  4. the same cross-check with the split-X kernel on A and B (orders 4..40,
 //     after an FP64-X first pass), whose per-term roundings are independent;
-//  5. otherwise recompute in double-double (orders <= 40).
+//  5. otherwise recompute with a certified walk: int32 X with double-double
+//     products for integer matrices (orders 8..64), split-dd for the rest
+//     (orders 4..40), double-double where neither applies (orders <= 40).
 // Steps 3 and 4 are skipped when their independent-rounding estimate alone
-// misses the target.
+// misses the target, and after an int32-X first pass (its certified twin
+// costs about 1.2 walks, less than a failed cross-check plus the rerun).
+// A certified walk (int32 X with dd products, split-dd) is its own estimate:
+// its bound uses the exact sum |term| the walk accumulated.
 // Context lock held.
 static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const DenseOperand& op, bool policy,
                          perm_result* out) {
@@ -941,6 +1142,15 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
   if (policy && !has_perfect_matching(mat, n, dtype)) {
     out->value = out->hi = out->lo = 0.0;
     out->abs_term_sum = out->rel_error_estimate = 0.0;
+    return PERM_OK;
+  }
+  if ((op.variant == PERM_KERNEL_DENSE_INT_DD || op.variant == PERM_KERNEL_DENSE_SDD) &&
+      out->steps == out->total_steps) {
+    ErrEstimate c;
+    c.s1 = ctx->walk_m1;
+    error_bounds(op.variant, op.group, n, out->value, &c, ctx->walk_terms_per_thread);
+    out->abs_term_sum = c.s1;
+    out->rel_error_estimate = c.worst;
     return PERM_OK;
   }
   // the estimate samples an FP64 column image; an int32 or split operand is replaced by one
@@ -964,6 +1174,7 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
   out->rel_error_estimate = e.worst;
   const double target = ctx->rel_target;
   if (!policy || e.worst <= target || op.variant == PERM_KERNEL_DENSE_DD) return PERM_OK;
+  const bool int_first = op.variant == PERM_KERNEL_DENSE_INT || op.variant == PERM_KERNEL_DENSE_TC;
   std::vector<double> b((size_t)n * n);
   for (int i2 = 0; i2 < n; i2++)
     for (int j2 = 0; j2 < n; j2++)
@@ -981,7 +1192,7 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
   perm_result rb;
   bool have_rb = false;
   // the cross-check's estimate is at least the independent-rounding one
-  if (out->value != 0.0 && e.random <= target) {
+  if (out->value != 0.0 && e.random <= target && !int_first) {
     DenseOperand t;
     perm_result rt;
     if ((rc = build_operand(ctx, b.data(), n, PERM_F64, b_split ? PERM_KERNEL_DENSE_SPLIT : 0, &t))) return rc;
@@ -1029,16 +1240,44 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
       }
     }
   }
-  if (n > 40) return PERM_OK;  // no double-double kernel above order 40: keep the bound
-  DenseOperand dd_op;
-  if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE_DD, &dd_op))) return rc;
+  int cv = 0;
+  if (int_group_size(av, n) > 0)
+    cv = PERM_KERNEL_DENSE_INT_DD;
+  else if (n >= 4 && n <= 40 && split_rows_ok(av, n))
+    cv = PERM_KERNEL_DENSE_SDD;
+  else if (n <= 40)
+    cv = PERM_KERNEL_DENSE_DD;
+  else
+    return PERM_OK;  // no certified kernel for this matrix: keep the bound
+  DenseOperand c_op;
+  if ((rc = build_operand(ctx, mat, n, dtype, cv, &c_op))) return rc;
   const double first_ms = out->kernel_ms;
-  if ((rc = run_whole(ctx, dd_op, out))) return rc;
+  if ((rc = run_whole(ctx, c_op, out))) return rc;
   out->kernel_ms += first_ms;
-  if ((rc = estimate_error(ctx, ctx->d_stage, n, dd_op, out->value, &e))) return rc;
+  if (cv == PERM_KERNEL_DENSE_DD) {
+    if ((rc = estimate_error(ctx, ctx->d_stage, n, c_op, out->value, &e))) return rc;
+  } else {
+    e.s1 = ctx->walk_m1;
+    error_bounds(cv, c_op.group, n, out->value, &e, ctx->walk_terms_per_thread);
+  }
   out->abs_term_sum = e.s1;
   out->rel_error_estimate = e.worst;
   return PERM_OK;
+}
+
+// With the accuracy policy on, the kernel a whole-walk call starts with
+// when a certified walk is cheap enough to go first: int32 X with
+// double-double products for integer matrices (about 1.2 int32-X walks, its
+// bound needs no sample), split-dd in the sparse layout for real matrices
+// whose three sparsest columns touch at most 16 rows (close to an FP64-X
+// walk in cost).  0: the FP64-X / int32-X walk goes first.
+static int policy_first_kernel(const void* mat, int n, int dtype) {
+  std::vector<double> a((size_t)n * n);
+  for (size_t i = 0; i < a.size(); i++) a[i] = elem(mat, dtype, i);
+  if (int_group_size(a, n) > 0) return PERM_KERNEL_DENSE_INT_DD;
+  int c3[3];
+  if (split_rows_ok(a, n) && sdd_inner_rows(a, n, c3) > 0) return PERM_KERNEL_DENSE_SDD;
+  return 0;
 }
 
 extern "C" int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard,
@@ -1049,7 +1288,8 @@ extern "C" int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dt
   if (nshards < 1 || shard < 0 || shard >= nshards)
     return fail(ctx, PERM_EINVAL, "shard %d of %d", shard, nshards);
   DenseOperand op;
-  if ((rc = build_operand(ctx, mat, n, dtype, variant, &op))) return rc;
+  const int first = variant == 0 && nshards == 1 && ctx->rel_target > 0 ? policy_first_kernel(mat, n, dtype) : 0;
+  if ((rc = build_operand(ctx, mat, n, dtype, first ? first : variant, &op))) return rc;
   // shards are Gray-index ranges of the walking kernels; the tensor-core
   // kernel's operand image is the int32-X one
   if (nshards > 1 && op.variant == PERM_KERNEL_DENSE_TC) op.variant = PERM_KERNEL_DENSE_INT;
@@ -1158,11 +1398,17 @@ extern "C" int perm_exact_dense_tc_rounds(perm_ctx* ctx, const void* mat, int n,
 }
 
 extern "C" int perm_exact_dense_resident(perm_ctx* ctx, const perm_matrix* m, perm_result* out) {
+  return perm_exact_dense_resident_shard(ctx, m, 0, 1, out);
+}
+
+extern "C" int perm_exact_dense_resident_shard(perm_ctx* ctx, const perm_matrix* m, int shard, int nshards,
+                                               perm_result* out) {
   if (!ctx || !m || !out) return ctx ? fail(ctx, PERM_EINVAL, "null argument") : PERM_EINVAL;
+  if (nshards < 1 || shard < 0 || shard >= nshards) return fail(ctx, PERM_EINVAL, "shard %d of %d", shard, nshards);
   std::lock_guard<std::mutex> lock(ctx->mu);
   CU(ctx, cudaSetDevice(ctx->device));
   DensePlan p;
-  int rc = dense_plan(ctx, m->op, 0, 1, &p);
+  int rc = dense_plan(ctx, m->op, shard, nshards, &p);
   if (rc) return rc;
   if ((rc = dense_launch(ctx, m->op, m->d_image, p))) return rc;
   rc = dense_collect(ctx, m->op, p, out);
@@ -1348,7 +1594,8 @@ extern "C" int perm_exact_sparse_ex(perm_ctx* ctx, int n, const int* rptrs, cons
     if (cols[p] < 0 || cols[p] >= n || rows[p] < 0 || rows[p] >= n)
       return fail(ctx, PERM_EINVAL, "index out of range at entry %d", p);
   if (variant != 0 && variant != PERM_KERNEL_SKIPPER && variant != PERM_KERNEL_DENSE &&
-      variant != PERM_KERNEL_DENSE_INT && variant != PERM_KERNEL_DENSE_TC)
+      variant != PERM_KERNEL_DENSE_INT && variant != PERM_KERNEL_DENSE_TC && variant != PERM_KERNEL_DENSE_INT_DD &&
+      variant != PERM_KERNEL_DENSE_SDD)
     return fail(ctx, PERM_EINVAL, "unknown sparse kernel variant %d", variant);
   bool skipper = variant == PERM_KERNEL_SKIPPER;
   if (variant == 0) skipper = n < 8 || zero_term_fraction(n, rptrs, rvals, cptrs, rows, cvals, 2048) >= kSkipperZeroFraction;

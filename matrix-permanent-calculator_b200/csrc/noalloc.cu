@@ -159,6 +159,7 @@ extern "C" int perm_exact_dense_noalloc(const double* d_mat, int n, double* d_ou
   args.out = d_out;
   args.err = &su.scratch->err;
   args.seg_blocks = 0;
+  args.inject = 0;
   int grid = 1;
   if (n < 4) {
     args.m = 0;

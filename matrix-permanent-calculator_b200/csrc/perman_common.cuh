@@ -54,6 +54,14 @@ __device__ __forceinline__ dd dd_shfl_down(dd v, int delta) {
   return v;
 }
 
+// Sum2 step (Ogita, Rump, Oishi: "Accurate sum and dot product", 2005):
+// (s, c) += (th, tl) with the rounding error of the high sum kept in c.
+__device__ __forceinline__ void sum2_add(double& s, double& c, double th, double tl) {
+  const dd r = two_sum(s, th);
+  s = r.hi;
+  c = __dadd_rn(c, __dadd_rn(r.lo, tl));
+}
+
 // Compensated accumulator: running (hi, lo) with TwoSum on every add.
 struct Acc {
   double hi = 0.0, lo = 0.0;
@@ -231,13 +239,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 // Stage `bytes` (multiple of 16) from global to shared with bulk copies.
 // Every thread of the block must call it; returns false (and sets *err) if
-// the completion did not arrive within the spin limit.
+// the completion did not arrive within the spin limit.  `inject_extra` > 0
+// is the failure-injection hook: the barrier then expects that many bytes
+// more than are copied, so its phase never completes although every copy
+// does (nothing stays in flight), and both bounded waits give up.
 __device__ __forceinline__ bool stage_to_smem(void* sdst, const void* gsrc, uint32_t bytes,
-                                              uint64_t* bar, int* err) {
+                                              uint64_t* bar, int* err, uint32_t inject_extra = 0) {
   if (threadIdx.x == 0) mbar_init(bar, 1);
   __syncthreads();
   if (threadIdx.x == 0) {
-    mbar_expect_tx(bar, bytes);
+    mbar_expect_tx(bar, bytes + inject_extra);
     for (uint32_t off = 0; off < bytes; off += kBulkPiece) {
       uint32_t piece = bytes - off < kBulkPiece ? bytes - off : kBulkPiece;
       bulk_g2s((char*)sdst + off, (const char*)gsrc + off, piece, bar);

@@ -36,6 +36,7 @@ struct DenseArgs {
   int* err;            // set to 1 if the shared-memory staging timed out
   uint64_t seg_blocks; // orders <= kAnchorMaxN: X is recomputed from x0 every seg_blocks
                        // aligned blocks (0: once per thread range)
+  uint32_t inject;     // failure injection (tests): staging expects this many extra bytes
 };
 
 // Orders up to which the FP64-X walk re-anchors X (recomputes it from x0) at
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(128) ryser_dense_kernel(DenseArgs args) {
 
   // Stage the matrix (at most 32 KB) once per block with a bulk copy; every
   // warp then reads columns as shared-memory broadcasts.
-  const bool staged = stage_to_smem(sA, args.colA, (uint32_t)(sizeof(double) * N * np), bar, args.err);
+  const bool staged = stage_to_smem(sA, args.colA, (uint32_t)(sizeof(double) * N * np), bar, args.err, args.inject);
   if (threadIdx.x < N) {
     const int j = threadIdx.x;
     double rs = 0.0;

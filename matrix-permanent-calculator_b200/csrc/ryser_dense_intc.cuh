@@ -1,0 +1,217 @@
+// ryser_dense_intc.cuh -- dense exact permanent for integer matrices with a
+// certified error bound: int32 X, double-double products and sum.
+//
+// Same walk, ranges and reductions as ryser_dense_int.cuh (the reference's
+// kernel_xshared_coalescing_mshared, gpu_exact_dense.cu:330-399, restated
+// with y = 2x held in int32).  The int32-X kernel's only roundings are its
+// ceil(n/G) - 1 FP64 products of exact group values and the FP64 sums of
+// terms; its worst-case error bound, (ceil(n/G) + 16) u sum|t| / |perm|,
+// cannot certify 1e-10 once the terms cancel by more than ~4e4 (dense
+// integer matrices of order 40).  Here both roundings are made error-free:
+//  * each group value v_g (an exact int32 product converted exactly to
+//    FP64) enters a double-double product: the first two values of a chain
+//    by TwoProd (h = v0 v1, l = fma(v0, v1, -h), exact), every further value
+//    by h' = h v, l' = fma(l, v, fma(h, v, -h')) (3 operations, relative
+//    error a few u^2); even and odd groups form two chains for
+//    instruction-level parallelism, joined by one double-double product;
+//  * the eight signed terms of a Gray group are summed with TwoSum into a
+//    (hi, lo) pair whose low parts collect every rounding error (Sum2 of
+//    Ogita, Rump and Oishi), and each group is added to the thread total the
+//    same way;
+//  * the walk also sums |hi| of its own terms, so the bound uses the exact
+//    cancellation scale sum|t| instead of a sampled estimate.
+// Per Gray step this adds ~2 ceil(n/G) + 9 FP64 operations to the int32-X
+// step (which is issue-bound with the FP64 pipe mostly idle); the error is
+// below (4 ceil(n/G) + 64) u^2 sum|t| plus the final rounding.
+#pragma once
+#include "ryser_dense_int.cuh"
+
+namespace perm {
+
+struct DenseIntcArgs {
+  const int* colI;  // column-major doubled matrix, then y0 (as DenseIntArgs)
+  int np4;
+  int m;
+  uint64_t block0, nblocks;
+  dd* partials;
+  unsigned* ticket;
+  double* out;
+  double* sums;  // sums[0] += sum |term| over the walked terms (zeroed by the host)
+  int* err;
+};
+
+// y += s * col (compile-time sign when kSign != 0)
+template <int N, int kSign>
+__device__ __forceinline__ void iupdate(int (&y)[N], const int* col, int s) {
+#pragma unroll
+  for (int j = 0; j < N; j += 4) {
+    const int4 v = lds4i(col + j);
+    const int c[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      if (j + t < N) {
+        if (kSign > 0)
+          y[j + t] += c[t];
+        else if (kSign < 0)
+          y[j + t] -= c[t];
+        else
+          y[j + t] += s * c[t];
+      }
+    }
+  }
+}
+
+// Exact group values: v_g = prod of y over rows [gG, gG + G), formed in
+// uint32 (the host proved |v_g| < 2^31) and converted exactly to FP64.
+template <int N, int G>
+__device__ __forceinline__ void group_values(const int (&y)[N], double (&v)[(N + G - 1) / G]) {
+  constexpr int NG = (N + G - 1) / G;
+#pragma unroll
+  for (int g = 0; g < NG; g++) {
+    const int j0 = g * G;
+    uint32_t pr = (uint32_t)y[j0];
+#pragma unroll
+    for (int t = 1; t < G; t++)
+      if (j0 + t < N) pr = pr * (uint32_t)y[j0 + t];
+    v[g] = __int2double_rn((int)pr);
+  }
+}
+
+// Double-double product of v[first], v[first + 2], v[first + 4], ... (an
+// unevaluated pair; the first multiply is an exact TwoProd).
+template <int NG, int kFirst>
+__device__ __forceinline__ dd chain_product(const double (&v)[NG]) {
+  dd p = {v[kFirst], 0.0};
+  if (kFirst + 2 < NG) {
+    p.hi = __dmul_rn(v[kFirst], v[kFirst + 2]);
+    p.lo = __fma_rn(v[kFirst], v[kFirst + 2], -p.hi);
+  }
+#pragma unroll
+  for (int g = kFirst + 4; g < NG; g += 2) {
+    const double h = __dmul_rn(p.hi, v[g]);
+    const double l = __fma_rn(p.hi, v[g], -h);
+    p.lo = __fma_rn(p.lo, v[g], l);
+    p.hi = h;
+  }
+  return p;
+}
+
+template <int N, int G>
+__device__ __forceinline__ dd term_dd(const int (&y)[N]) {
+  constexpr int NG = (N + G - 1) / G;
+  double v[NG];
+  group_values<N, G>(y, v);
+  const dd a = chain_product<NG, 0>(v);
+  if (NG == 1) return a;
+  const dd b = chain_product<NG, 1>(v);
+  // a x b: exact high product and its error, plus both cross terms
+  const double h = __dmul_rn(a.hi, b.hi);
+  double l = __fma_rn(a.hi, b.hi, -h);
+  if (NG > 3) l = __fma_rn(a.hi, b.lo, l);  // b has a low part from three groups on
+  if (NG > 2) l = __fma_rn(a.lo, b.hi, l);  // a has one from three groups on
+  return {h, l};
+}
+
+template <int N, int G>
+__global__ void __launch_bounds__(128, (N <= 36 ? 3 : 2)) ryser_dense_intc_kernel(DenseIntcArgs args) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int np4 = args.np4;
+  int* sC = reinterpret_cast<int*>(smem_raw);  // [N][np4] columns, then y0
+  dd* red = reinterpret_cast<dd*>(sC + (size_t)(N + 1) * np4);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(red + 32);
+  const bool staged = stage_to_smem(sC, args.colI, (uint32_t)(sizeof(int) * (N + 1) * np4), bar, args.err);
+  const int* sY0 = sC + (size_t)N * np4;
+
+  double H = 0.0, L = 0.0, m1 = 0.0;  // thread total (Sum2) and sum |term|
+  const uint64_t TT = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t q = args.nblocks / TT, r = args.nblocks % TT;
+  const uint64_t b0 = q * tid + (r * tid) / TT;
+  const uint64_t b1 = q * (tid + 1) + (r * (tid + 1)) / TT;
+
+  if (staged && b1 > b0) {
+    const uint64_t s0 = (args.block0 + b0) << args.m, e0 = (args.block0 + b1) << args.m;
+    int y[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) y[j] = sY0[j];
+    const uint64_t g = s0 ^ (s0 >> 1);
+#pragma unroll 1
+    for (int k = 0; k < N - 1; k++) {
+      if ((g >> k) & 1) {
+#pragma unroll
+        for (int j = 0; j < N; j++) y[j] += sC[k * np4 + j];
+      }
+    }
+    {
+      const dd t0 = term_dd<N, G>(y);  // index s0 is even: sign +
+      H = t0.hi;
+      L = t0.lo;
+      m1 = fabs(t0.hi);
+    }
+
+    const int* c0 = sC;
+    const int* c1 = sC + np4;
+    const int* c2 = sC + 2 * np4;
+    const uint64_t groups = (e0 - s0) >> 3;
+    uint64_t base = s0;
+    // one group of eight Gray steps, base + 1 .. base + 8 (signs - + - + - + - +);
+    // the eighth flips column k8 >= 3 (kLast: only seven steps)
+    auto group8 = [&](bool kLast) {
+      const int s4 = ((base >> 3) & 1) ? -1 : 1;
+      double gs, gc;
+      iupdate<N, +1>(y, c0, 0);
+      dd t = term_dd<N, G>(y);
+      gs = -t.hi;
+      gc = -t.lo;
+      double ma = fabs(t.hi);
+      iupdate<N, +1>(y, c1, 0);
+      t = term_dd<N, G>(y);
+      sum2_add(gs, gc, t.hi, t.lo);
+      ma += fabs(t.hi);
+      iupdate<N, -1>(y, c0, 0);
+      t = term_dd<N, G>(y);
+      sum2_add(gs, gc, -t.hi, -t.lo);
+      ma += fabs(t.hi);
+      iupdate<N, 0>(y, c2, s4);
+      t = term_dd<N, G>(y);
+      sum2_add(gs, gc, t.hi, t.lo);
+      ma += fabs(t.hi);
+      iupdate<N, +1>(y, c0, 0);
+      t = term_dd<N, G>(y);
+      sum2_add(gs, gc, -t.hi, -t.lo);
+      ma += fabs(t.hi);
+      iupdate<N, -1>(y, c1, 0);
+      t = term_dd<N, G>(y);
+      sum2_add(gs, gc, t.hi, t.lo);
+      ma += fabs(t.hi);
+      iupdate<N, -1>(y, c0, 0);
+      t = term_dd<N, G>(y);
+      sum2_add(gs, gc, -t.hi, -t.lo);
+      ma += fabs(t.hi);
+      if (!kLast) {
+        const uint64_t i8 = base + 8;
+        const int k8 = __ffsll((long long)i8) - 1;
+        const int s8 = ((i8 >> (k8 + 1)) & 1) ? -1 : 1;
+        iupdate<N, 0>(y, sC + k8 * np4, s8);
+        t = term_dd<N, G>(y);
+        sum2_add(gs, gc, t.hi, t.lo);
+        ma += fabs(t.hi);
+      }
+      sum2_add(H, L, gs, gc);
+      m1 += ma;
+    };
+#pragma unroll 1
+    for (uint64_t gi = 0; gi + 1 < groups; gi++, base += 8) group8(false);
+    group8(true);  // last group of the range: index e0 belongs to the next range
+  }
+
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) m1 += __shfl_down_sync(0xffffffffu, m1, d);
+  if ((threadIdx.x & 31) == 0 && m1 > 0.0) atomicAdd(args.sums, m1);
+  const dd mine = two_sum(H, L);
+  const dd bt = block_reduce_dd(mine, red);
+  const double factor = ((N & 1) ? 2.0 : -2.0) * ldexp(1.0, -N);
+  grid_finish_dd(bt, args.partials, args.ticket, args.out, factor, red);
+}
+
+}  // namespace perm

@@ -1,0 +1,372 @@
+// ryser_dense_sdd.cuh -- exact permanent of real matrices with a certified
+// error bound: split X, double-double products and sum ("split-dd").
+//
+// Same Nijenhuis-Wilf Gray walk, aligned thread ranges and reductions as
+// ryser_dense.cuh (the reference's kernel_xshared_coalescing_mshared,
+// gpu_exact_dense.cu:330-399, restated).  The operand is the split-X image
+// (ryser_dense_split.cuh): every entry a = ah + al with ah on its row's grid
+// 2^-q_j, so the coarse row sums xh are EXACT in FP64 and the remainders xl
+// are tiny (|al| <= 2^-(q_j+1)).  The pair (xh_j, xl_j) is therefore an
+// accurate double-double value of x_j for two FP64 additions per update
+// (the double-double kernel's TwoSum update takes seven), and:
+//  * the n-way product is formed in double-double on these pairs: exact high
+//    product and its error from one FMA, both cross terms by FMAs (4
+//    operations per factor, four independent chains);
+//  * terms are summed with TwoSum into a (hi, lo) pair per Gray group of
+//    eight (Sum2 of Ogita, Rump and Oishi) and the groups into the thread
+//    total the same way;
+//  * the walk sums |hi| of its own terms: the error bound uses the exact
+//    cancellation scale sum|t|.
+// About 6n + 10 FP64 operations per Gray step against 11n + 8 for the
+// double-double kernel, with a relative error of order n u^2 sum|t| / |perm|.
+//
+// Two layouts:
+//  * ryser_dense_sdd_kernel<N>: every step updates and multiplies all n
+//    rows (rolled step loop: the two X vectors fill the register file);
+//  * ryser_sparse_sdd_kernel<N, R>: for sparse matrices.  Seven of every
+//    eight Gray steps flip column 0, 1 or 2; the host permutes columns so
+//    these are three columns whose nonzeros lie in few rows, and rows so that
+//    those rows come first (rows 0..R-1).  At those seven steps only rows
+//    0..R-1 change: the kernel updates and multiplies them alone and reuses
+//    the product of rows R..n-1, which it recomputes at the eighth step (the
+//    one that flips a column >= 3).  About (7 (6R + 9) + 6n + 5) / 8
+//    operations per step: 78 instead of 221 for n = 36, R = 8.
+#pragma once
+#include "ryser_dense.cuh"
+
+namespace perm {
+
+struct DenseSddArgs {
+  const double* img;  // [colH: n x np][colL: n x np][x0h: np][x0l: np] (split-X image)
+  int np;
+  int m;
+  uint64_t block0, nblocks;
+  dd* partials;
+  unsigned* ticket;
+  double* out;
+  double* sums;  // sums[0] += sum |term| over the walked terms (zeroed by the host)
+  int* err;
+};
+
+// p *= (xh + xl), both unevaluated pairs: exact high product and its error
+// from one FMA, both cross terms by FMAs (the xl x p.lo term is below u^2).
+__device__ __forceinline__ void pair_mul(dd& p, double xh, double xl) {
+  const double h = __dmul_rn(p.hi, xh);
+  double l = __fma_rn(p.hi, xh, -h);
+  l = __fma_rn(p.hi, xl, l);
+  l = __fma_rn(p.lo, xh, l);
+  p.hi = h;
+  p.lo = l;
+}
+
+// Double-double product of rows [J0, J1) in up to four chains.
+template <int J0, int J1, int N>
+__device__ __forceinline__ dd rows_product(const double (&xh)[N], const double (&xl)[N]) {
+  constexpr int C = (J1 - J0) >= 4 ? 4 : (J1 - J0);
+  dd c[4];
+#pragma unroll
+  for (int t = 0; t < C; t++) c[t] = {xh[J0 + t], xl[J0 + t]};
+#pragma unroll
+  for (int j = J0 + C; j < J1; j++) pair_mul(c[(j - J0) % C], xh[j], xl[j]);
+  if (C == 4) {
+    pair_mul(c[0], c[1].hi, c[1].lo);
+    pair_mul(c[2], c[3].hi, c[3].lo);
+    pair_mul(c[0], c[2].hi, c[2].lo);
+  } else {
+#pragma unroll
+    for (int t = 1; t < C; t++) pair_mul(c[0], c[t].hi, c[t].lo);
+  }
+  return c[0];
+}
+
+// rows [J0, J1) of X += s * column (s = +-1; compile-time when kSign != 0)
+template <int J0, int J1, int kSign, int N>
+__device__ __forceinline__ void pair_update(double (&xh)[N], double (&xl)[N], const double* colH,
+                                            const double* colL, double s) {
+#pragma unroll
+  for (int j = J0; j < J1; j += 2) {
+    double h0, h1 = 0.0, l0, l1 = 0.0;
+    if (j + 1 < J1) {
+      const double2 vh = lds2(colH + j), vl = lds2(colL + j);
+      h0 = vh.x;
+      h1 = vh.y;
+      l0 = vl.x;
+      l1 = vl.y;
+    } else {
+      h0 = lds1(colH + j);
+      l0 = lds1(colL + j);
+    }
+    if (kSign > 0) {
+      xh[j] = __dadd_rn(xh[j], h0);
+      xl[j] = __dadd_rn(xl[j], l0);
+      if (j + 1 < J1) {
+        xh[j + 1] = __dadd_rn(xh[j + 1], h1);
+        xl[j + 1] = __dadd_rn(xl[j + 1], l1);
+      }
+    } else if (kSign < 0) {
+      xh[j] = __dsub_rn(xh[j], h0);
+      xl[j] = __dsub_rn(xl[j], l0);
+      if (j + 1 < J1) {
+        xh[j + 1] = __dsub_rn(xh[j + 1], h1);
+        xl[j + 1] = __dsub_rn(xl[j + 1], l1);
+      }
+    } else {
+      xh[j] = __fma_rn(s, h0, xh[j]);
+      xl[j] = __fma_rn(s, l0, xl[j]);
+      if (j + 1 < J1) {
+        xh[j + 1] = __fma_rn(s, h1, xh[j + 1]);
+        xl[j + 1] = __fma_rn(s, l1, xl[j + 1]);
+      }
+    }
+  }
+}
+
+// Thread start state: X at Gray index s0 directly from gray(s0).
+template <int N>
+__device__ __forceinline__ void sdd_start(double (&xh)[N], double (&xl)[N], const double* sH, const double* sL,
+                                          const double* sX0h, const double* sX0l, int np, uint64_t s0) {
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    xh[j] = sX0h[j];
+    xl[j] = sX0l[j];
+  }
+  const uint64_t g = s0 ^ (s0 >> 1);
+#pragma unroll 1
+  for (int k = 0; k < N - 1; k++) {
+    if ((g >> k) & 1) {
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        xh[j] = __dadd_rn(xh[j], sH[k * np + j]);
+        xl[j] = __dadd_rn(xl[j], sL[k * np + j]);
+      }
+    }
+  }
+}
+
+__host__ __device__ inline size_t dense_sdd_smem_bytes(int n) {
+  const int np = (n + 1) & ~1;
+  return sizeof(double) * (2 * (size_t)n * np + 2 * np) + 32 * sizeof(dd) + 16;
+}
+
+// Shared tail: sum |term| to the host accumulator, double-double block and
+// grid reduction of the thread totals.
+__device__ __forceinline__ void sdd_finish(double H, double L, double m1, const DenseSddArgs& args, dd* red,
+                                           double factor) {
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) m1 += __shfl_down_sync(0xffffffffu, m1, d);
+  if ((threadIdx.x & 31) == 0 && m1 > 0.0) atomicAdd(args.sums, m1);
+  const dd bt = block_reduce_dd(two_sum(H, L), red);
+  grid_finish_dd(bt, args.partials, args.ticket, args.out, factor, red);
+}
+
+// CTAs per SM by order: the two X vectors plus the product chains fit 3 CTAs
+// (168 registers) up to order 28, 2 above.
+template <int N>
+__global__ void __launch_bounds__(128, (N <= 28 ? 3 : 2)) ryser_dense_sdd_kernel(DenseSddArgs args) {
+  static_assert(N >= 4, "orders below 4 use the other kernels");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sH = reinterpret_cast<double*>(smem_raw);
+  const int np = args.np;
+  const double* sL = sH + (size_t)N * np;
+  const double* sX0h = sL + (size_t)N * np;
+  const double* sX0l = sX0h + np;
+  dd* red = reinterpret_cast<dd*>(sH + 2 * (size_t)N * np + 2 * np);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(red + 32);
+  const bool staged =
+      stage_to_smem(sH, args.img, (uint32_t)(sizeof(double) * (2 * (size_t)N * np + 2 * np)), bar, args.err);
+
+  double H = 0.0, L = 0.0, m1 = 0.0;
+  const uint64_t TT = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t q = args.nblocks / TT, r = args.nblocks % TT;
+  const uint64_t b0 = q * tid + (r * tid) / TT;
+  const uint64_t b1 = q * (tid + 1) + (r * (tid + 1)) / TT;
+
+  if (staged && b1 > b0) {
+    const uint64_t s0 = (args.block0 + b0) << args.m, e0 = (args.block0 + b1) << args.m;
+    double xh[N], xl[N];
+    sdd_start<N>(xh, xl, sH, sL, sX0h, sX0l, np, s0);
+    const dd t0 = rows_product<0, N, N>(xh, xl);  // index s0 is even: sign +
+    H = t0.hi;
+    L = t0.lo;
+    m1 = fabs(t0.hi);
+    // groups of eight steps (s0 and e0 are multiples of 8); the last group
+    // of the range has seven (index e0 belongs to the next range)
+#pragma unroll 1
+    for (uint64_t base = s0; base < e0; base += 8) {
+      const uint64_t top = base + 8 < e0 ? base + 8 : e0 - 1;
+      double gs = 0.0, gc = 0.0, ma = 0.0;
+#pragma unroll 1
+      for (uint64_t i = base + 1; i <= top; i++) {
+        const int k = __ffsll((long long)i) - 1;
+        const double sg = ((i >> (k + 1)) & 1) ? -1.0 : 1.0;
+        pair_update<0, N, 0, N>(xh, xl, sH + k * np, sL + k * np, sg);
+        const dd t = rows_product<0, N, N>(xh, xl);
+        if (i & 1)
+          sum2_add(gs, gc, -t.hi, -t.lo);
+        else
+          sum2_add(gs, gc, t.hi, t.lo);
+        ma += fabs(t.hi);
+      }
+      sum2_add(H, L, gs, gc);
+      m1 += ma;
+    }
+  }
+  sdd_finish(H, L, m1, args, red, (N & 1) ? 2.0 : -2.0);
+}
+
+// The sparse layout.  Columns 0, 1, 2 are zero outside rows 0..R-1 (the host
+// checked it); P_out is the product of rows R..N-1, constant between two
+// flips of a column >= 3.  Rows 0..R-1 of X live in registers; rows R..N-1
+// are touched only at the eighth step of a group, so they live in shared
+// memory as (xh, xl) pairs in a [row][thread] layout (consecutive lanes,
+// consecutive 16-byte words: conflict-free), which keeps the register file
+// for the unrolled inner steps.
+__host__ __device__ inline size_t sparse_sdd_smem_bytes(int n, int r, int threads) {
+  return dense_sdd_smem_bytes(n) + 16 * (size_t)(n - r) * threads;
+}
+
+template <int N, int R>
+__global__ void __launch_bounds__(128, 2) ryser_sparse_sdd_kernel(DenseSddArgs args) {
+  static_assert(R >= 2 && R + 2 <= N && (R & 1) == 0, "inner rows: even, and outer rows must remain");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sH = reinterpret_cast<double*>(smem_raw);
+  const int np = args.np;
+  const double* sL = sH + (size_t)N * np;
+  const double* sX0h = sL + (size_t)N * np;
+  const double* sX0l = sX0h + np;
+  dd* red = reinterpret_cast<dd*>(sH + 2 * (size_t)N * np + 2 * np);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(red + 32);
+  double2* sOut = reinterpret_cast<double2*>(bar + 2);  // [N - R][blockDim.x]
+  const bool staged =
+      stage_to_smem(sH, args.img, (uint32_t)(sizeof(double) * (2 * (size_t)N * np + 2 * np)), bar, args.err);
+
+  double H = 0.0, L = 0.0, m1 = 0.0;
+  const uint64_t TT = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t q = args.nblocks / TT, r = args.nblocks % TT;
+  const uint64_t b0 = q * tid + (r * tid) / TT;
+  const uint64_t b1 = q * (tid + 1) + (r * (tid + 1)) / TT;
+  const int T = blockDim.x, me = threadIdx.x;
+
+  if (staged && b1 > b0) {
+    const uint64_t s0 = (args.block0 + b0) << args.m, e0 = (args.block0 + b1) << args.m;
+    const uint64_t g0 = s0 ^ (s0 >> 1);
+    // start state: inner rows in registers, outer rows in shared memory
+    double xh[R], xl[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+      xh[j] = sX0h[j];
+      xl[j] = sX0l[j];
+    }
+#pragma unroll 1
+    for (int k = 0; k < N - 1; k++) {
+      if ((g0 >> k) & 1) {
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+          xh[j] = __dadd_rn(xh[j], sH[k * np + j]);
+          xl[j] = __dadd_rn(xl[j], sL[k * np + j]);
+        }
+      }
+    }
+#pragma unroll 1
+    for (int j = R; j < N; j++) {
+      double vh = sX0h[j], vl = sX0l[j];
+      for (int k = 0; k < N - 1; k++) {
+        if ((g0 >> k) & 1) {
+          vh = __dadd_rn(vh, sH[k * np + j]);
+          vl = __dadd_rn(vl, sL[k * np + j]);
+        }
+      }
+      sOut[(j - R) * T + me] = make_double2(vh, vl);
+    }
+    // product of the outer rows (four chains), optionally after adding
+    // s * column k to them
+    auto outer = [&](bool upd, int k, double s) {
+      dd c[4];
+#pragma unroll
+      for (int j = R; j < N; j++) {
+        double2 v = sOut[(j - R) * T + me];
+        if (upd) {
+          v.x = __fma_rn(s, sH[k * np + j], v.x);
+          v.y = __fma_rn(s, sL[k * np + j], v.y);
+          sOut[(j - R) * T + me] = v;
+        }
+        const int t = (j - R) & 3;
+        if (j - R < 4)
+          c[t] = {v.x, v.y};
+        else
+          pair_mul(c[t], v.x, v.y);
+      }
+      constexpr int C = (N - R) >= 4 ? 4 : (N - R);
+#pragma unroll
+      for (int t = 1; t < C; t++) pair_mul(c[0], c[t].hi, c[t].lo);
+      return c[0];
+    };
+    dd pout = outer(false, 0, 0.0);
+    auto inner_term = [&]() {
+      dd t = rows_product<0, R, R>(xh, xl);
+      pair_mul(t, pout.hi, pout.lo);
+      return t;
+    };
+    {
+      const dd t0 = inner_term();  // index s0 is even: sign +
+      H = t0.hi;
+      L = t0.lo;
+      m1 = fabs(t0.hi);
+    }
+    const double *h0 = sH, *h1 = sH + np, *h2 = sH + 2 * np;
+    const double *l0 = sL, *l1 = sL + np, *l2 = sL + 2 * np;
+    const uint64_t groups = (e0 - s0) >> 3;
+    uint64_t base = s0;
+    auto group8 = [&](bool kLast) {
+      const double s4 = ((base >> 3) & 1) ? -1.0 : 1.0;
+      pair_update<0, R, +1, R>(xh, xl, h0, l0, 0.0);
+      dd t = inner_term();
+      double gs = -t.hi, gc = -t.lo, ma = fabs(t.hi);
+      pair_update<0, R, +1, R>(xh, xl, h1, l1, 0.0);
+      t = inner_term();
+      sum2_add(gs, gc, t.hi, t.lo);
+      ma += fabs(t.hi);
+      pair_update<0, R, -1, R>(xh, xl, h0, l0, 0.0);
+      t = inner_term();
+      sum2_add(gs, gc, -t.hi, -t.lo);
+      ma += fabs(t.hi);
+      pair_update<0, R, 0, R>(xh, xl, h2, l2, s4);
+      t = inner_term();
+      sum2_add(gs, gc, t.hi, t.lo);
+      ma += fabs(t.hi);
+      pair_update<0, R, +1, R>(xh, xl, h0, l0, 0.0);
+      t = inner_term();
+      sum2_add(gs, gc, -t.hi, -t.lo);
+      ma += fabs(t.hi);
+      pair_update<0, R, -1, R>(xh, xl, h1, l1, 0.0);
+      t = inner_term();
+      sum2_add(gs, gc, t.hi, t.lo);
+      ma += fabs(t.hi);
+      pair_update<0, R, -1, R>(xh, xl, h0, l0, 0.0);
+      t = inner_term();
+      sum2_add(gs, gc, -t.hi, -t.lo);
+      ma += fabs(t.hi);
+      if (!kLast) {
+        // the eighth step flips column k8 >= 3: every row may change
+        const uint64_t i8 = base + 8;
+        const int k8 = __ffsll((long long)i8) - 1;
+        const double s8 = ((i8 >> (k8 + 1)) & 1) ? -1.0 : 1.0;
+        pair_update<0, R, 0, R>(xh, xl, sH + k8 * np, sL + k8 * np, s8);
+        pout = outer(true, k8, s8);
+        t = inner_term();
+        sum2_add(gs, gc, t.hi, t.lo);
+        ma += fabs(t.hi);
+      }
+      sum2_add(H, L, gs, gc);
+      m1 += ma;
+    };
+#pragma unroll 1
+    for (uint64_t gi = 0; gi + 1 < groups; gi++, base += 8) group8(false);
+    group8(true);
+  }
+  sdd_finish(H, L, m1, args, red, (N & 1) ? 2.0 : -2.0);
+}
+
+}  // namespace perm

@@ -61,6 +61,7 @@ struct DenseTcArgs {
   unsigned* ticket;
   double* out;
   int* err;
+  int inject;  // failure injection (tests): the "empty" barriers expect one arrival more than is made
 };
 
 __host__ __device__ constexpr int tc_np(int n) { return (n + 15) & ~15; }
@@ -332,8 +333,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) ryser_dense_tc_kernel(DenseTcAr
     if (t == 0) {
       mbar_init(&full[0], 1);
       mbar_init(&full[1], 1);
-      mbar_init(&empty[0], 4 * kTcBlocks);
-      mbar_init(&empty[1], 4 * kTcBlocks);
+      // (with args.inject, one arrival more than the consumers make: the
+      // producer's bounded wait for a free buffer gives up at the third
+      // round, after which only committed MMAs remain and are drained)
+      mbar_init(&empty[0], 4 * kTcBlocks + (args.inject ? 1 : 0));
+      mbar_init(&empty[1], 4 * kTcBlocks + (args.inject ? 1 : 0));
       *abort_flag = 0;
     }
     fence_async_smem();

@@ -1,0 +1,20 @@
+// ryser_sparse_sdd_r8.cu -- sparse-layout split-dd Ryser kernels whose
+// columns 0..2 touch rows 0..7 only, orders 12..40.
+#include "ryser_dense_sdd.cuh"
+
+namespace perm {
+#define PERM_SPSDD_CASE(n) \
+  case n: return reinterpret_cast<const void*>(&ryser_sparse_sdd_kernel<n, 8>);
+const void* sparse_sdd_kernel_r8(int n) {
+  switch (n) {
+    PERM_SPSDD_CASE(12) PERM_SPSDD_CASE(13) PERM_SPSDD_CASE(14) PERM_SPSDD_CASE(15)
+    PERM_SPSDD_CASE(16) PERM_SPSDD_CASE(17) PERM_SPSDD_CASE(18) PERM_SPSDD_CASE(19) PERM_SPSDD_CASE(20)
+    PERM_SPSDD_CASE(21) PERM_SPSDD_CASE(22) PERM_SPSDD_CASE(23) PERM_SPSDD_CASE(24) PERM_SPSDD_CASE(25)
+    PERM_SPSDD_CASE(26) PERM_SPSDD_CASE(27) PERM_SPSDD_CASE(28) PERM_SPSDD_CASE(29) PERM_SPSDD_CASE(30)
+    PERM_SPSDD_CASE(31) PERM_SPSDD_CASE(32) PERM_SPSDD_CASE(33) PERM_SPSDD_CASE(34) PERM_SPSDD_CASE(35)
+    PERM_SPSDD_CASE(36) PERM_SPSDD_CASE(37) PERM_SPSDD_CASE(38) PERM_SPSDD_CASE(39) PERM_SPSDD_CASE(40)
+    default: return nullptr;
+  }
+}
+#undef PERM_SPSDD_CASE
+}  // namespace perm

@@ -4,6 +4,7 @@ import ctypes
 import re
 import subprocess
 
+import numpy as np
 import pytest
 from conftest import ROOT
 
@@ -72,3 +73,15 @@ def test_header_constants_match_the_binding(pb):
     for name in defines:
         if name.startswith(("PERM_KERNEL_", "PERM_E", "PERM_F", "PERM_I", "PERM_REQ_")):
             assert hasattr(pb, name), name
+
+
+def test_sdd_layout_query(pb):
+    """Host-only layout query: dense matrices keep the dense layout, sparse
+    ones get the smallest inner-row count that holds their three sparsest
+    columns' rows, orders outside 4..40 are refused."""
+    rng = np.random.default_rng(1)
+    assert pb.sdd_layout(1.0 - rng.random((30, 30))) == 0
+    P = np.eye(20)[rng.permutation(20)] + np.eye(20)
+    assert pb.sdd_layout(P) == 6
+    assert pb.sdd_layout(np.ones((41, 41))) == pb.PERM_EUNSUPPORTED
+    assert pb.sdd_layout(np.ones((3, 3))) == pb.PERM_EUNSUPPORTED

@@ -187,3 +187,55 @@ def test_gloo_dynamic_queue_subgroups_then_world(pb, orc, tmp_path):
         v = np.load(f"{out}.{r}.npy")
         assert abs((v[0] + v[1]) - want) <= 1e-14 * abs(want)
         assert abs((v[2] + v[3]) - want) <= 1e-14 * abs(want)
+
+
+def _rank_bench_sharded(rank, world, port, A, out_path):
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    sys.path.insert(0, str(root))
+    sys.path.insert(0, str(root / "tests"))
+    sys.path.insert(0, str(root / "oracle"))
+    import torch.distributed as dist
+    import bench
+    from conftest import load_package
+    from oracle import Oracle
+
+    pb = load_package()
+    orc = Oracle()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    n = A.shape[0]
+    factor = 2.0 if n & 1 else -2.0
+
+    def shard_fn(r, w):  # CPU stand-in for perm_exact_dense_resident_shard
+        a, b = pb.shard_range(n, r, w)
+        hi, lo = orc.ryser_dd_range(A, a, b, threads=1)
+        return hi * factor, lo * factor, 0.0
+
+    (hi, lo), ms = bench.sharded_step(pb, shard_fn, rank, world, dist, None)
+    (hi1, lo1), _ = bench.sharded_step(pb, shard_fn, 0, 1)  # the one-rank step: the whole walk
+    dist.barrier()
+    dist.destroy_process_group()
+    np.save(f"{out_path}.{rank}.npy", np.array([hi, lo, hi1, lo1, ms]))
+
+
+def test_bench_sharded_step_two_ranks(pb, orc, tmp_path):
+    """bench.py's distributed mode (one matrix, Gray-range shards per rank,
+    16-byte all-gather, double-double sum) on two gloo ranks with the oracle
+    as the device: the result equals the one-rank value within 1e-12 and is
+    identical on both ranks."""
+    rng = np.random.default_rng(12)
+    A = (rng.random((17, 17)) < 0.5) * rng.integers(1, 5, (17, 17)).astype(float)
+    A[np.arange(17), np.arange(17)] = 1.0
+    port = _free_port()
+    out = str(tmp_path / "bench")
+    mp.start_processes(_rank_bench_sharded, args=(2, port, A, out), nprocs=2, join=True, start_method="spawn")
+    r0, r1 = np.load(f"{out}.0.npy"), np.load(f"{out}.1.npy")
+    exact = orc.perm_exact_int(A)[0]
+    for r in (r0, r1):
+        assert abs((r[0] + r[1]) - (r[2] + r[3])) <= 1e-12 * abs(r[2] + r[3])
+        assert abs((r[0] + r[1]) - exact) <= 1e-12 * abs(exact)
+    assert r0[0] == r1[0] and r0[1] == r1[1]

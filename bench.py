@@ -170,7 +170,7 @@ def run_reference_arm(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD, "sample": f"Gray indices [1+k*{steps_per}, 1+(k+1)*{steps_per}) per step",
                    "function": "cpu_perman64 (gpu_exact_dense.cu:7), OpenMP"},
@@ -358,7 +358,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_s = float(t.item())
     value = args.steps * total_steps / dev_s
-    perm_value = hi + lo
+    perm_value = r.value if world == 1 else hi + lo
 
     # end to end through the public C ABI with a host matrix: at N=1 the
     # reference-signature entry point gpu_perman64_xshared_coalescing_mshared_int
@@ -695,6 +695,27 @@ def batched_secondary(pb, eng, count=8192):
     pvals, est, reevaluated, policy_ms = b.run_ex()
     b.free()
     finite = est[np.isfinite(est)]
+    # where the batch's time goes: the same replay on sub-batches (binary /
+    # real, by order band), each timed alone; FP64-X-equivalent rate of the
+    # real ones (2n FP64 ops per Gray step) against the live FP64 peak
+    peak_ops = max(eng.fp64_peak()[0], eng.fp64_peak()[0])
+    breakdown = {}
+    kinds = ["binary" if i % 2 == 0 else "real" for i in range(count)]
+    for kind in ("binary", "real"):
+        for lo, hi in ((12, 20), (21, 24), (25, 26), (27, 28)):
+            sel = [m for m, k in zip(mats, kinds) if k == kind and lo <= m.shape[0] <= hi]
+            if not sel:
+                continue
+            sb = eng.batch(sel)
+            sb.run()
+            sub_ms = min(sb.run()[1] for _ in range(2))
+            sb.free()
+            st = sum(2.0 ** (m.shape[0] - 1) for m in sel)
+            ops = sum(2.0 ** (m.shape[0] - 1) * 2 * m.shape[0] for m in sel)
+            breakdown[f"{kind}_n{lo}_{hi}"] = {
+                "matrices": len(sel), "ms": sub_ms, "gray_steps": st, "steps_per_s": st / (sub_ms * 1e-3),
+                "fp64_equivalent_frac_of_peak": ops / (sub_ms * 1e-3) / peak_ops}
+    breakdown["sum_of_parts_ms"] = sum(v["ms"] for v in breakdown.values() if isinstance(v, dict))
     # one launch per matrix (plain kernel, FP64 X, host loop through the C ABI;
     # a context without error estimates, like the plain batch replay above)
     with pb.Engine(eng.device) as plain:
@@ -718,7 +739,7 @@ def batched_secondary(pb, eng, count=8192):
                                      "reevaluated": reevaluated, "exact_zeros": int(np.sum(pvals == 0.0)),
                                      "max_rel_error_estimate": float(np.max(finite)) if finite.size else None,
                                      "unbounded_estimates": int(est.size - finite.size)},
-            "autotune_s": tune_s, "autotuned_lane_log2": table,
+            "autotune_s": tune_s, "autotuned_lane_log2": table, "breakdown": breakdown,
             "timing": "CUDA events around the graph launch (queue reset + kernel + 128 KB readback)"}
 
 

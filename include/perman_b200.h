@@ -79,7 +79,8 @@ typedef struct {
   int kernel;         /* PERM_KERNEL_*                                      */
   int n;
   double abs_term_sum;       /* estimate of sum_i |term(i)| (cancellation scale) */
-  double rel_error_estimate; /* estimated relative error of value (0: not estimated) */
+  double rel_error_estimate; /* estimated relative error of (hi, lo) (0: not estimated);
+                                value, their sum rounded once, adds at most 2^-53 */
 } perm_result;
 
 typedef struct {

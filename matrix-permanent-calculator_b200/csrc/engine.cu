@@ -1002,7 +1002,8 @@ static int check_variant(perm_ctx* ctx, int variant) {
 //    eight and of the groups of one thread range (256, plus (K/4)^2 for the
 //    low-part sum over K terms per thread), the double-double reductions;
 //    for split-dd also the drift of the remainder row sums xl over K updates
-//    (64 n^2 K).  Plus u for rounding hi + lo to one double.
+//    (64 n^2 K).  Like the double-double bound, of the (hi, lo) pair: value,
+//    its sum rounded once, adds at most u.
 constexpr int kSamplesPerClass = 8192;  // term-moment sample: threads per subset-size class
 
 struct ErrEstimate {
@@ -1023,7 +1024,7 @@ static void error_bounds(int variant, int group, int n, double value, ErrEstimat
     const double k = (double)k_terms;
     const double prod = variant == PERM_KERNEL_DENSE_INT_DD ? 8.0 * std::ceil((double)n / group) : 8.0 * n;
     const double drift = variant == PERM_KERNEL_DENSE_SDD ? 64.0 * n * n * k : 0.0;
-    e->worst = e->random = (prod + 256.0 + (k / 4) * (k / 4) + drift) * u * u * s1 / av + u;
+    e->worst = e->random = (prod + 256.0 + (k / 4) * (k / 4) + drift) * u * u * s1 / av;
   } else if (variant == PERM_KERNEL_DENSE_DD) {
     e->worst = e->random = (4.0 * n + 32.0) * u * u * s1 / av;
   } else if (variant == PERM_KERNEL_DENSE_SPLIT) {

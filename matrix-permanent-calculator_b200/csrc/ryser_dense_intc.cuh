@@ -112,8 +112,9 @@ __device__ __forceinline__ dd term_dd(const int (&y)[N]) {
   return {h, l};
 }
 
-template <int N, int G>
-__global__ void __launch_bounds__(128, (N <= 36 ? 3 : 2)) ryser_dense_intc_kernel(DenseIntcArgs args) {
+// CTAs per SM: 3 (168 registers) up to order 36; above, 2 CTAs and no spills.
+template <int N, int G, int kMinBlocks = (N <= 36 ? 3 : 2)>
+__global__ void __launch_bounds__(128, kMinBlocks) ryser_dense_intc_kernel(DenseIntcArgs args) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int np4 = args.np4;
   int* sC = reinterpret_cast<int*>(smem_raw);  // [N][np4] columns, then y0

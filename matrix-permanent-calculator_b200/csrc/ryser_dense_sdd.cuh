@@ -226,8 +226,8 @@ __host__ __device__ inline size_t sparse_sdd_smem_bytes(int n, int r, int thread
   return dense_sdd_smem_bytes(n) + 16 * (size_t)(n - r) * threads;
 }
 
-template <int N, int R>
-__global__ void __launch_bounds__(128, 2) ryser_sparse_sdd_kernel(DenseSddArgs args) {
+template <int N, int R, int kMinBlocks = 2>
+__global__ void __launch_bounds__(128, kMinBlocks) ryser_sparse_sdd_kernel(DenseSddArgs args) {
   static_assert(R >= 2 && R + 2 <= N && (R & 1) == 0, "inner rows: even, and outer rows must remain");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* sH = reinterpret_cast<double*>(smem_raw);

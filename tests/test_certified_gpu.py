@@ -38,6 +38,7 @@ def test_int_dd_vs_exact(engine, orc, pb, n):
         ok, info = _covers(r, exact)
         assert ok, (kind, info)
         assert r.rel_error_estimate < 1e-20, (kind, r.rel_error_estimate)  # u^2-level bound
+        assert rel_err(r.value, exact) <= 1.2e-16  # value is the pair rounded once (<= 2^-53)
 
 
 def test_int_dd_golden_n32(engine, golden, pb):
@@ -94,6 +95,7 @@ def test_sdd_dense_vs_oracle_dd(engine, orc, pb, n):
         ok, info = _covers(r, want, slack)
         assert ok, (kind, info)
         assert r.rel_error_estimate < 1e-18 or abs(want) < 1e-12 * r.abs_term_sum, (kind, r.rel_error_estimate)
+        assert abs(r.value - want) <= 1.2e-16 * abs(want) + slack + r.rel_error_estimate * abs(want)
 
 
 @pytest.mark.parametrize("n,d", [(12, 0.2), (16, 0.2), (20, 0.25), (24, 0.2), (26, 0.3), (28, 0.2)])
@@ -102,7 +104,10 @@ def test_sdd_sparse_layout_vs_oracle_dd(engine, orc, pb, n, d):
     sparsest columns at seven of eight steps, against the CPU double-double
     Ryser; the automatic path (dense and CRS/CCS entry points) runs it first."""
     rng = np.random.default_rng(900 + n)
-    A = bernoulli(rng, n, d) * (1.0 - rng.random((n, n)))
+    # a Bernoulli pattern plus a random permutation: a perfect matching exists,
+    # so the permanent is positive and the relative bound is meaningful
+    mask = (bernoulli(rng, n, d) + np.eye(n)[rng.permutation(n)]) > 0
+    A = mask * (1.0 - rng.random((n, n)))
     inner = pb.sdd_layout(A)
     assert inner in (6, 8, 12, 16), inner
     r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SDD)

@@ -112,3 +112,22 @@ def test_grid_mode_estimates_tilings(pb):
     assert name == "gpu_perman64_rasmussen_sparse" and abs(v - 12988816) < 5 * se
     r = run(pb, "-i", "-m", "20", "-n", "10", "-p2", "-x", "20000")
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.gpu
+def test_sparse_ccs_ids_run_the_sparse_walk(pb, orc, tmp_path):
+    """-s -p1..-p4 (the reference's CCS walks) run the split-dd kernel, whose
+    sparse layout walks only the rows of the three sparsest columns; the
+    kernel that ran is named on its own line."""
+    rng = np.random.default_rng(23)
+    A = bernoulli(rng, 22, 0.2) * (1.0 - rng.random((22, 22)))
+    p = tmp_path / "r.txt"
+    write_matrix(p, A, "double")
+    want = sum(orc.perm_dd(A))
+    for pid in ("-p1", "-p4"):
+        r = run(pb, "-f", p, "-s", pid)
+        assert r.returncode == 0, r.stderr
+        name, v = result_value(r.stdout)
+        assert name.endswith("_sparse")
+        assert "engine kernel: split-dd walk" in r.stdout
+        assert rel_err(v, want) < 1e-10

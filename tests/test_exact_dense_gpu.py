@@ -167,12 +167,21 @@ def test_int_kernel_signed_entries(engine, orc, pb):
 
 
 def test_automatic_kernel_choice(engine, pb):
+    """With the accuracy policy on, integer matrices start with the certified
+    int32-X walk; with it off (one evaluation) the plain int32-X walk runs;
+    non-integer and large-entry matrices take FP64 X (dense real matrices
+    keep their FP64-X value when its bound meets the target)."""
     rng = np.random.default_rng(18)
     A = bernoulli(rng, 20, 0.5)
-    assert engine.exact_dense(A).kernel == pb.PERM_KERNEL_DENSE_INT
-    assert engine.exact_dense(A * 0.5).kernel == pb.PERM_KERNEL_DENSE
-    big = A * 100000  # row products no longer fit int32 in groups of 3
-    assert engine.exact_dense(big).kernel == pb.PERM_KERNEL_DENSE
+    assert engine.exact_dense(A).kernel == pb.PERM_KERNEL_DENSE_INT_DD
+    engine.set_rel_target(0.0)
+    try:
+        assert engine.exact_dense(A).kernel == pb.PERM_KERNEL_DENSE_INT
+        assert engine.exact_dense(A * 0.5).kernel == pb.PERM_KERNEL_DENSE
+        big = A * 100000  # row products no longer fit int32 in groups of 3
+        assert engine.exact_dense(big).kernel == pb.PERM_KERNEL_DENSE
+    finally:
+        engine.set_rel_target(1e-10)
     with pytest.raises(pb.PermError):
         engine.exact_dense(A * 0.5, variant=pb.PERM_KERNEL_DENSE_INT)
 
@@ -194,7 +203,10 @@ def test_int_kernel_shards(engine, pb):
 
 
 def test_dense_autotune_sets_the_automatic_choice(pb):
+    """The autotuned kernel is the automatic choice for single evaluations
+    (policy off); with the policy on, integer inputs take the certified walk."""
     with pb.Engine(0) as eng:
+        eng.set_rel_target(0.0)
         table = eng.dense_autotune(8, 22)
         assert set(table.values()) <= {pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_INT, pb.PERM_KERNEL_DENSE_TC}
         rng = np.random.default_rng(1)
@@ -240,11 +252,11 @@ def test_automatic_double_double_rerun(pb, orc):
     rng = np.random.default_rng(33)
     A = rng.standard_normal((20, 20))
     with pb.Engine(0) as eng:
-        eng.set_rel_target(1e-16)  # unreachable in FP64: forces the double-double rerun
+        eng.set_rel_target(1e-16)  # unreachable in FP64: forces the certified (split-dd) rerun
         r = eng.exact_dense(A)
-        assert r.kernel == pb.PERM_KERNEL_DENSE_DD
+        assert r.kernel == pb.PERM_KERNEL_DENSE_SDD
         hi, lo = orc.perm_dd(A)
-        assert abs((r.hi - hi) + (r.lo - lo)) <= 1e-24 * abs(hi)
+        assert abs((r.hi - hi) + (r.lo - lo)) <= max(r.rel_error_estimate, 1e-24) * abs(hi)
         assert r.rel_error_estimate < 1e-20
         eng.set_rel_target(0.0)  # no reruns
         assert eng.exact_dense(A).kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_INT)
@@ -261,9 +273,9 @@ def test_fp64_error_grows_and_double_double_fixes_it(engine, pb):
     actual = abs(f.value - d.value) / abs(d.value)
     assert actual <= f.rel_error_estimate
     if f.rel_error_estimate > 1e-10:
-        # kept after the transpose cross-check, or recomputed in double-double
-        if auto.kernel == pb.PERM_KERNEL_DENSE_DD:
-            assert auto.value == d.value
+        # kept after the transpose cross-check, or recomputed by the certified split-dd walk
+        if auto.kernel == pb.PERM_KERNEL_DENSE_SDD:
+            assert abs(auto.value - d.value) <= (auto.rel_error_estimate + d.rel_error_estimate + 2.3e-16) * abs(d.value)
         else:
             assert auto.kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_SPLIT)
             assert abs(auto.value - d.value) / abs(d.value) <= auto.rel_error_estimate <= 1e-10

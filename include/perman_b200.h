@@ -283,8 +283,23 @@ int perm_batch_exact(perm_ctx* ctx, int count, const int* orders, const double* 
                      double* kernel_ms);
 /* Measures, for each order in [n_lo, n_hi], the batch kernel with every
  * candidate lane-range length and keeps the fastest in the context (used by
- * later perm_batch_create calls).  m_out receives n_hi - n_lo + 1 exponents. */
+ * later perm_batch_create calls); then measures every compiled batch kernel
+ * variant that covers order n_hi -- threads per block (64, 128, 256), the
+ * register budget it was compiled for (CTAs per SM), and FP64 X of dense
+ * matrices in registers or in shared memory -- on a mixed batch of these
+ * orders and keeps the fastest for later batches whose orders it covers.
+ * m_out receives n_hi - n_lo + 1 exponents.  Per matrix, perm_batch_create
+ * also picks the dense or the sparse layout (orders 12..32: three columns
+ * whose nonzeros lie in at most 8 / 16 rows for FP64 X, 6 / 12 rows for
+ * int32 X; those rows are walked alone at seven of eight Gray steps, and in
+ * int32 X a group whose other rows' product is 0 skips its seven vanishing
+ * terms). */
 int perm_batch_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* m_out);
+/* The batch kernel variant later perm_batch_create calls use (0 = the
+ * general one, orders up to 40): its largest order, threads per block, CTAs
+ * per SM it was compiled for, and whether dense FP64 matrices keep X in
+ * shared memory. */
+int perm_batch_variant(perm_ctx* ctx, int* variant, int* max_n, int* block, int* min_blocks, int* shared_x);
 
 /* ---- request loop: continuous batching on one GPU ------------------------------
  * No counterpart in the reference.  `slots` worker contexts run requests

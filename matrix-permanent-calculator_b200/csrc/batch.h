@@ -7,9 +7,8 @@
 namespace perm {
 
 constexpr int kBatchMaxOrder = 40;
-constexpr int kBatchBlock = 128;  // 4 warps, one tile each at a time
-// per-warp shared slot: columns [n][np] + x0[np] for the largest order
-constexpr int kBatchSlotDoubles = kBatchMaxOrder * kBatchMaxOrder + kBatchMaxOrder;
+// per-warp shared slot: columns [n][np] + x0[np] for the largest order (np = n
+// rounded up to even: n (n + 1) doubles hold it for every n)
 
 // One matrix of a batch, in queue order (largest work first).
 struct BatchMatrix {
@@ -22,6 +21,9 @@ struct BatchMatrix {
   int g;                // 0: FP64 X (column-major doubles, stride np); 5 or 6: int32 X
                         // with product groups of g rows (doubled int columns, stride
                         // np4 = n rounded up to 4, then y0) -- orders >= 9 only
+  int r;                // 0: dense walk; > 0: sparse layout, columns 0..2 nonzero in
+                        // rows 0..r-1 only (FP64: r in {8, 16}; int32, g = 6: r in {6, 12}),
+                        // orders 12..32
 };
 
 struct BatchArgs {
@@ -36,9 +38,25 @@ struct BatchArgs {
   double* results;                // (hi, lo, sum |term|) per matrix, caller order
 };
 
-__global__ void batch_kernel(BatchArgs a);
+// per-warp shared slot of a kernel variant whose largest order is max_n:
+// columns and x0, then (shared-memory X) 32 lanes' X vectors
+__host__ __device__ constexpr int batch_slot_doubles(int max_n, bool xs) {
+  return max_n * max_n + max_n + (xs ? 32 * max_n : 0);
+}
 
-inline size_t batch_smem_bytes() { return sizeof(double) * (size_t)kBatchSlotDoubles * (kBatchBlock / 32); }
+// A compiled batch kernel: largest order it walks, threads per block, CTAs
+// per SM it was compiled for (launch bounds), whether dense FP64 matrices
+// keep X in shared memory, entry point.
+struct BatchVariant {
+  int max_n, block, min_blocks, xs;
+  const void* fn;
+};
+constexpr int kBatchVariantCount = 6;
+extern const BatchVariant kBatchVariants[kBatchVariantCount];
+
+inline size_t batch_smem_bytes(const BatchVariant& v) {
+  return sizeof(double) * (size_t)batch_slot_doubles(v.max_n, v.xs != 0) * (v.block / 32);
+}
 
 // Lane-range exponent used when the autotuner has not measured an order:
 // about 2^12 Gray indices per lane, at least 8, at most a 32-lane tile per matrix.

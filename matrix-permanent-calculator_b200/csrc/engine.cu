@@ -284,7 +284,8 @@ struct perm_ctx {
   double walk_m1 = 0;                            // last certified (int32-X dd or split-dd) walk: sum |term|
   uint64_t walk_terms_per_thread = 0;            // ... and its longest thread range
   int inject_timeouts = 0;                       // failure injection: launches left to inject into
-  int batch_occ = 0;
+  int batch_occ[kBatchVariantCount] = {};  // CTAs per SM of each batch kernel variant
+  int batch_variant = 0;                   // autotuned batch kernel variant (kBatchVariants)
   std::string err;
   std::mutex mu;
 };
@@ -636,27 +637,35 @@ static int sdd_inner_rows(const std::vector<double>& a, int n, int* c3) {
 // most 16 rows, of the matrix with those columns moved to positions 0..2
 // and their rows to the top (the sparse layout; the permanent is invariant
 // under row and column permutations).
+// The sparse layout's permutation: columns c3[0..2] move to positions 0..2
+// (the others keep their order), the rows where any of them is nonzero to
+// the top (in order), the other rows after them.  The permanent is
+// invariant under row and column permutations.
+static std::vector<double> sparse_permutation(const double* a, int n, const int* c3) {
+  std::vector<int> cols = {c3[0], c3[1], c3[2]}, rows;
+  for (int k = 0; k < n; k++)
+    if (k != c3[0] && k != c3[1] && k != c3[2]) cols.push_back(k);
+  std::vector<char> in_union(n, 0);
+  for (int j = 0; j < n; j++)
+    for (int t = 0; t < 3; t++)
+      if (a[(size_t)j * n + c3[t]] != 0.0) in_union[j] = 1;
+  for (int j = 0; j < n; j++)
+    if (in_union[j]) rows.push_back(j);
+  for (int j = 0; j < n; j++)
+    if (!in_union[j]) rows.push_back(j);
+  std::vector<double> p((size_t)n * n);
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < n; k++) p[(size_t)i * n + k] = a[(size_t)rows[i] * n + cols[k]];
+  return p;
+}
+
 static int build_sdd_operand(perm_ctx* ctx, const std::vector<double>& a, int n, DenseOperand* op) {
   if (n < 4 || n > 40) return fail(ctx, PERM_EUNSUPPORTED, "split-dd kernel covers orders 4..40 (got %d)", n);
   int c3[3] = {0, 1, 2};
   const int inner = sdd_inner_rows(a, n, c3);
   int rc;
   if (inner) {
-    std::vector<int> cols = {c3[0], c3[1], c3[2]}, rows;
-    for (int k = 0; k < n; k++)
-      if (k != c3[0] && k != c3[1] && k != c3[2]) cols.push_back(k);
-    std::vector<char> in_union(n, 0);
-    for (int j = 0; j < n; j++)
-      for (int t = 0; t < 3; t++)
-        if (a[(size_t)j * n + c3[t]] != 0.0) in_union[j] = 1;
-    for (int j = 0; j < n; j++)
-      if (in_union[j]) rows.push_back(j);
-    for (int j = 0; j < n; j++)
-      if (!in_union[j]) rows.push_back(j);
-    std::vector<double> p((size_t)n * n);
-    for (int i = 0; i < n; i++)
-      for (int k = 0; k < n; k++) p[(size_t)i * n + k] = a[(size_t)rows[i] * n + cols[k]];
-    rc = build_split_operand(ctx, p, n, op);
+    rc = build_split_operand(ctx, sparse_permutation(a.data(), n, c3), n, op);
   } else {
     rc = build_split_operand(ctx, a, n, op);
   }
@@ -1874,6 +1883,8 @@ struct perm_batch {
   int count = 0;
   uint64_t total_tiles = 0;
   int grid = 1;
+  int variant = 0;  // kBatchVariants index
+  int sparse = 0;   // matrices walked in the sparse layout
   double* d_operands = nullptr;
   BatchMatrix* d_mats = nullptr;
   dd* d_tile_partials = nullptr;
@@ -1906,10 +1917,11 @@ static void batch_free(perm_batch* b) {
 }
 
 static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, const double* values,
-                               const int* m_override, perm_batch** out) {
+                               const int* m_override, perm_batch** out, int variant_override = -1) {
   if (count < 1 || !orders || !values || !out) return fail(ctx, PERM_EINVAL, "empty batch or null pointer");
   std::vector<BatchMatrix> mats(count);
   std::vector<uint64_t> src_off(count);
+  std::vector<std::vector<double>> sparse_images(count);  // permuted matrices of the sparse layout
   uint64_t off = 0, img = 0;
   for (int i = 0; i < count; i++) {
     const int n = orders[i];
@@ -1929,10 +1941,31 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
     // int32 X for integer matrices whose groups of 5 or 6 rows fit in int32
     // (every 0/1 matrix up to order 35); FP64 X otherwise
     M.g = 0;
+    M.r = 0;
     if (n >= 9) {
       std::vector<double> a(values + src_off[i], values + src_off[i] + (size_t)n * n);
       const int G = int_group_size(a, n);
       if (G >= 5) M.g = G;
+      // sparse layout (orders 12..32) when three columns have their nonzeros
+      // in few rows: FP64 X with 8 or 16 inner rows, int32 X (groups of 6)
+      // with 6 or 12
+      if (n >= 12 && n <= 32) {
+        int c3[3];
+        const int u = sparsest_column_triple(a, n, c3);
+        int r = 0;
+        if (M.g)
+          r = u <= 6 ? 6 : u <= 12 ? 12 : 0;
+        else
+          r = u <= 8 ? 8 : u <= 16 ? 16 : 0;
+        if (r && r + 4 <= n) {
+          std::vector<double> p = sparse_permutation(a.data(), n, c3);
+          if (!M.g || int_group_size(p, n) == 6) {
+            M.r = r;
+            if (M.g) M.g = 6;
+            sparse_images[i] = std::move(p);
+          }
+        }
+      }
     }
   }
   // queue order: most Gray work first (longest-processing-time scheduling)
@@ -1949,7 +1982,7 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
   std::vector<double> image(img);
   for (int i = 0; i < count; i++) {
     const int n = mats[i].n, np = (n + 1) & ~1;
-    const double* a = values + src_off[i];
+    const double* a = mats[i].r ? sparse_images[i].data() : values + src_off[i];
     double* dst = image.data() + mats[i].offset;
     if (mats[i].g) {
       // doubled int columns (stride np4), then y0 = 2 a[j][n-1] - rowsum_j;
@@ -1972,6 +2005,15 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
   perm_batch* b = new perm_batch();
   b->count = count;
   b->total_tiles = tiles;
+  int max_n = 0;
+  for (int i = 0; i < count; i++) {
+    max_n = std::max(max_n, mats[i].n);
+    if (mats[i].r) b->sparse++;
+  }
+  int vi = variant_override >= 0 ? variant_override : ctx->batch_variant;
+  if (vi < 0 || vi >= kBatchVariantCount || kBatchVariants[vi].max_n < max_n) vi = 0;
+  b->variant = vi;
+  const BatchVariant& V = kBatchVariants[vi];
   b->orders.assign(orders, orders + count);
   b->groups.resize(count);
   for (int i = 0; i < count; i++) b->groups[i] = mats[i].g;
@@ -1997,18 +2039,19 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
   BT(cudaMemcpy(b->d_operands, image.data(), sizeof(double) * img, cudaMemcpyHostToDevice));
   BT(cudaMemcpy(b->d_mats, q.data(), sizeof(BatchMatrix) * count, cudaMemcpyHostToDevice));
   BT(cudaMemset(b->d_mat_done, 0, sizeof(unsigned) * count));
-  if (!ctx->batch_occ) {
-    if (int rc2 = allow_smem(ctx, (const void*)batch_kernel, batch_smem_bytes())) {
+  if (!ctx->batch_occ[vi]) {
+    if (int rc2 = allow_smem(ctx, V.fn, batch_smem_bytes(V))) {
       batch_free(b);
       return rc2;
     }
     int occ = 0;
-    BT(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, kBatchBlock, batch_smem_bytes()));
-    ctx->batch_occ = std::max(occ, 1);
+    BT(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, V.fn, V.block, batch_smem_bytes(V)));
+    ctx->batch_occ[vi] = std::max(occ, 1);
   }
-  const uint64_t warps = (uint64_t)ctx->num_sms * ctx->batch_occ * (kBatchBlock / 32);
+  const int wpb = V.block / 32;
+  const uint64_t warps = (uint64_t)ctx->num_sms * ctx->batch_occ[vi] * wpb;
   const uint64_t want = std::min<uint64_t>(warps, tiles);
-  b->grid = (int)std::max<uint64_t>(1, (want + (kBatchBlock / 32) - 1) / (kBatchBlock / 32));
+  b->grid = (int)std::max<uint64_t>(1, (want + wpb - 1) / wpb);
   // capture: reset the queue head, run, read the results back
   BatchArgs args;
   args.operands = b->d_operands;
@@ -2023,7 +2066,7 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
   void* kargs[] = {&args};
   BT(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), ctx->stream);
-  cudaLaunchKernel((const void*)batch_kernel, dim3(b->grid), dim3(kBatchBlock), kargs, batch_smem_bytes(), ctx->stream);
+  cudaLaunchKernel(V.fn, dim3(b->grid), dim3(V.block), kargs, batch_smem_bytes(V), ctx->stream);
   cudaMemcpyAsync(b->h_results, b->d_results, sizeof(double) * 3 * count, cudaMemcpyDeviceToHost, ctx->stream);
   BT(cudaStreamEndCapture(ctx->stream, &b->graph));
   BT(cudaGraphInstantiate(&b->exec, b->graph, 0));
@@ -2173,6 +2216,63 @@ extern "C" int perm_batch_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* m_out
     ctx->batch_m[n] = best_m;
     if (m_out) m_out[n - n_lo] = best_m;
   }
+  // kernel variant (threads per block, register budget, register or
+  // shared-memory X) on a mixed batch of these orders, about 2^26 Gray steps
+  // per order, half 0/1 and half real matrices at densities 0.3..0.8
+  std::vector<int> orders;
+  std::vector<double> vals;
+  for (int n = std::max(n_lo, 9); n <= n_hi; n++) {
+    const int count = (int)std::max<uint64_t>(2, (1ull << 26) >> (n - 1));
+    for (int c = 0; c < count; c++) {
+      const double d = 0.3 + 0.5 * (c % 6) / 5.0;
+      orders.push_back(n);
+      for (int e = 0; e < n * n; e++) {
+        state = state * 6364136223846793005ull + 1442695040888963407ull;
+        const double u1 = (double)(state >> 11) * (1.0 / 9007199254740992.0);
+        state = state * 6364136223846793005ull + 1442695040888963407ull;
+        const double u2 = 1.0 - (double)(state >> 11) * (1.0 / 9007199254740992.0);
+        vals.push_back(u1 < d ? ((c & 1) ? u2 : 1.0) : 0.0);
+      }
+      for (int j = 0; j < n; j++) vals[vals.size() - (size_t)n * n + (size_t)j * n + j] = 1.0;  // no empty row
+    }
+  }
+  if (!orders.empty()) {
+    double best_ms = 1e30;
+    int best_v = 0;
+    for (int v = 0; v < kBatchVariantCount; v++) {
+      if (kBatchVariants[v].max_n < n_hi) continue;
+      perm_batch* b = nullptr;
+      int rc = batch_create_locked(ctx, (int)orders.size(), orders.data(), vals.data(), nullptr, &b, v);
+      if (rc) return rc;
+      double ms = 1e30, t = 0;
+      for (int rep = 0; rep < 3; rep++) {
+        rc = batch_run_locked(ctx, b, nullptr, &t);
+        if (rc) {
+          batch_free(b);
+          return rc;
+        }
+        if (rep) ms = std::min(ms, t);
+      }
+      batch_free(b);
+      if (ms < best_ms * 0.98) {
+        best_ms = ms;
+        best_v = v;
+      }
+    }
+    ctx->batch_variant = best_v;
+  }
+  return PERM_OK;
+}
+
+extern "C" int perm_batch_variant(perm_ctx* ctx, int* variant, int* max_n, int* block, int* min_blocks,
+                                  int* shared_x) {
+  if (!ctx) return PERM_EINVAL;
+  const BatchVariant& V = kBatchVariants[ctx->batch_variant];
+  if (variant) *variant = ctx->batch_variant;
+  if (max_n) *max_n = V.max_n;
+  if (block) *block = V.block;
+  if (min_blocks) *min_blocks = V.min_blocks;
+  if (shared_x) *shared_x = V.xs;
   return PERM_OK;
 }
 

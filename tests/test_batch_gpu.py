@@ -136,3 +136,44 @@ def test_order_35_binary_in_batch_matches_single_kernel(engine, pb):
     vals, _ = engine.batch_exact([A])
     single = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT).value
     assert abs(vals[0] - single) <= 1e-12 * abs(single)
+
+
+def test_sparse_layout_in_the_batch(engine, orc, pb):
+    """Sparse matrices walk the two-level layout inside the batch (FP64 X with
+    8 or 16 inner rows, int32 X with 6 or 12 and vanishing-group skips):
+    every result agrees with the oracle (exact for integers, double-double for
+    reals) exactly as the dense walk's would."""
+    rng = np.random.default_rng(91)
+    mats = []
+    for n in (12, 14, 17, 20, 23, 26):
+        for d in (0.15, 0.25):
+            P = (bernoulli(rng, n, d) + np.eye(n)[rng.permutation(n)]) > 0
+            mats.append(P.astype(np.float64))                          # 0/1
+            mats.append(P * rng.integers(1, 4, (n, n)).astype(float))   # small integers
+            mats.append(P * (1.0 - rng.random((n, n))))                 # real
+    assert sum(pb.sdd_layout(m) > 0 for m in mats) >= len(mats) // 2
+    vals, _ = engine.batch_exact(mats)
+    for m, v in zip(mats, vals):
+        if np.all(m == np.round(m)):
+            want = orc.perm_exact_int(m)[0]
+            assert rel_err(v, want) < 1e-13, (m.shape, v, want)
+        else:
+            hi, lo = orc.perm_dd(m)
+            assert rel_err(v, hi + lo) < 1e-11, (m.shape, v, hi + lo)
+
+
+def test_batch_variants_agree_and_autotune_picks_one(pb):
+    """The autotuner measures the compiled batch kernel variants (threads per
+    block, register budget, shared-memory X), keeps one, and later batches
+    run it with the same permanents (to rounding) as the general variant."""
+    rng = np.random.default_rng(92)
+    mats = mixed_batch(rng, 120, 9, 24)
+    with pb.Engine(0) as eng:
+        base, _ = eng.batch_exact(mats)
+        table = eng.batch_autotune(9, 24)
+        assert set(table) == set(range(9, 25))
+        v = eng.batch_variant()
+        assert 0 <= v["variant"] < 6 and v["max_order"] >= 24
+        tuned, _ = eng.batch_exact(mats)
+        for a, b in zip(base, tuned):
+            assert abs(a - b) <= 1e-11 * abs(b) or abs(a - b) < 1e-12

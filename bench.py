@@ -220,7 +220,8 @@ def kernel_template(kname: str, A: np.ndarray) -> str:
     if kname == "int32x":
         return f"ryser_dense_int_kernel<{n}, {int_group_size(A)}>"
     if kname == "int32x_dd":
-        return f"ryser_dense_intc_kernel<{n}, {int_group_size(A)}>"
+        # third template argument: CTAs per SM compiled for (3 up to order 36, 2 above)
+        return f"ryser_dense_intc_kernel<{n}, {int_group_size(A)}, {3 if n <= 36 else 2}>"
     if kname == "fp64x":
         return f"ryser_dense_kernel<{n}>"
     return kname
@@ -284,7 +285,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
     ap.add_argument("--order", type=int, default=N_ORDER, help="matrix order (profiling runs use a smaller one)")
-    ap.add_argument("--variant", choices=["auto", "fp64", "int", "tc", "split", "intdd"], default="auto",
+    ap.add_argument("--workload", choices=["dense", "sparse"], default="dense",
+                    help="dense: the n=40 U{1..4} headline matrix; sparse: the sparse exact configuration's "
+                         "distribution (Bernoulli(0.2) mask, U(0,1] values, seed 2026) at --order, walked by "
+                         "the certified split-dd kernel (profiling runs)")
+    ap.add_argument("--variant", choices=["auto", "fp64", "int", "tc", "split", "intdd", "sdd"], default="auto",
                     help="dense kernel: automatic, FP64-X, int32-X, tensor-core row sums, split X or the "
                          "certified int32-X walk (double-double products and sum)")
     args = ap.parse_args()
@@ -306,11 +311,13 @@ def main():
     torch.cuda.set_device(device)
     pb = load_pkg()
     eng = pb.Engine(device)
-    A = make_matrix(0, args.order)  # the one matrix every rank shards
+    A = make_matrix(0, args.order) if args.workload == "dense" else cfg2_matrix(args.order)  # every rank shards it
     n = A.shape[0]
     variant = {"auto": 0, "fp64": pb.PERM_KERNEL_DENSE, "int": pb.PERM_KERNEL_DENSE_INT,
                "tc": pb.PERM_KERNEL_DENSE_TC, "split": pb.PERM_KERNEL_DENSE_SPLIT,
-               "intdd": pb.PERM_KERNEL_DENSE_INT_DD}[args.variant]
+               "intdd": pb.PERM_KERNEL_DENSE_INT_DD, "sdd": pb.PERM_KERNEL_DENSE_SDD}[args.variant]
+    if args.workload == "sparse" and variant == 0:
+        variant = pb.PERM_KERNEL_DENSE_SDD  # the sparse configuration's automatic kernel
     total_steps = 2.0 ** (n - 1)
     ops_per_step = 2.0 * n  # n X-updates + n multiplies per Gray step (algorithmic)
     ops_text = f"2n = {int(ops_per_step)} FP64 ops per Gray step x 2^{n - 1} steps"
@@ -434,8 +441,10 @@ def main():
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, resident in HBM)",
-        "config": {"workload": WORKLOAD.replace("n=40", f"n={n}"), "n": n, "density": DENSITY,
-                   "values": "U{1,2,3,4}",
+        "config": {"workload": (WORKLOAD.replace("n=40", f"n={n}") if args.workload == "dense" else
+                                f"sparse exact Ryser (split-dd), n={n}, density 0.2, values U(0,1]"),
+                   "n": n, "density": DENSITY if args.workload == "dense" else 0.2,
+                   "values": "U{1,2,3,4}" if args.workload == "dense" else "U(0,1]",
                    "gray_steps_per_permanent": total_steps,
                    "parallelism": (f"{world} ranks: Gray-range shards of one matrix, 16-byte NCCL all-gather"
                                    if world > 1 else "1 rank, the whole walk"),
@@ -561,16 +570,16 @@ class _Capture:
         return float(m[-1]) if m else None
 
 
-def cfg2_matrix():
+def cfg2_matrix(n: int = 36):
     """The sparse exact configuration: n=36, Bernoulli(0.20) mask with no empty
     row or column, values U(0,1], seed 2026 (tests/golden holds its
-    double-double value)."""
+    double-double value); other orders from the same generator."""
     rng = np.random.default_rng(2026)
     while True:
-        mk = rng.random((36, 36)) < 0.2
+        mk = rng.random((n, n)) < 0.2
         if mk.any(0).all() and mk.any(1).all():
             break
-    return mk * (1.0 - rng.random((36, 36)))
+    return mk * (1.0 - rng.random((n, n)))
 
 
 def golden_value(name: str):

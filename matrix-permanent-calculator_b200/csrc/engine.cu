@@ -1022,9 +1022,10 @@ static int check_variant(perm_ctx* ctx, int variant) {
 //  * double-double: (4n + 32) u^2 S1 / |perm|;
 //  * certified walks (int32 X with double-double products, split-dd), whose
 //    S1 is the walk's own exact sum: products of relative error below
-//    ~4u^2 per factor (8 ceil(n/G) or 8n in all), Sum2 of each Gray group of
-//    eight and of the groups of one thread range (256, plus (K/4)^2 for the
-//    low-part sum over K terms per thread), the double-double reductions;
+//    ~4u^2 per factor (8 ceil(n/G) or 8n in all), Sum2 of the terms (256,
+//    plus the low part's own rounding: K^2 for K terms added one by one per
+//    thread in the int32-X walk, (K/4)^2 for split-dd's groups of eight),
+//    the double-double reductions;
 //    for split-dd also the drift of the remainder row sums xl over K updates
 //    (64 n^2 K).  Like the double-double bound, of the (hi, lo) pair: value,
 //    its sum rounded once, adds at most u.
@@ -1047,8 +1048,11 @@ static void error_bounds(int variant, int group, int n, double value, ErrEstimat
   if (variant == PERM_KERNEL_DENSE_INT_DD || variant == PERM_KERNEL_DENSE_SDD) {
     const double k = (double)k_terms;
     const double prod = variant == PERM_KERNEL_DENSE_INT_DD ? 8.0 * std::ceil((double)n / group) : 8.0 * n;
+    // low-part rounding: the int32-X walk adds every term to one (hi, lo),
+    // split-dd adds groups of eight
+    const double lows = variant == PERM_KERNEL_DENSE_INT_DD ? k * k : (k / 4) * (k / 4);
     const double drift = variant == PERM_KERNEL_DENSE_SDD ? 64.0 * n * n * k : 0.0;
-    e->worst = e->random = (prod + 256.0 + (k / 4) * (k / 4) + drift) * u * u * s1 / av;
+    e->worst = e->random = (prod + 256.0 + lows + drift) * u * u * s1 / av;
   } else if (variant == PERM_KERNEL_DENSE_DD) {
     e->worst = e->random = (4.0 * n + 32.0) * u * u * s1 / av;
   } else if (variant == PERM_KERNEL_DENSE_SPLIT) {
@@ -1182,7 +1186,8 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
   DenseOperand f;
   const DenseOperand* fp = &op;
   if (op.variant == PERM_KERNEL_DENSE_INT || op.variant == PERM_KERNEL_DENSE_TC ||
-      op.variant == PERM_KERNEL_DENSE_SPLIT) {
+      op.variant == PERM_KERNEL_DENSE_SPLIT || op.variant == PERM_KERNEL_DENSE_INT_DD ||
+      op.variant == PERM_KERNEL_DENSE_SDD) {
     if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE, &f))) return rc;
     fp = &f;
   }

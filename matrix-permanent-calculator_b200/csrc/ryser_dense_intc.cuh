@@ -9,20 +9,22 @@
 // cannot certify 1e-10 once the terms cancel by more than ~4e4 (dense
 // integer matrices of order 40).  Here both roundings are made error-free:
 //  * each group value v_g (an exact int32 product converted exactly to
-//    FP64) enters a double-double product: the first two values of a chain
-//    by TwoProd (h = v0 v1, l = fma(v0, v1, -h), exact), every further value
-//    by h' = h v, l' = fma(l, v, fma(h, v, -h')) (3 operations, relative
-//    error a few u^2); even and odd groups form two chains for
-//    instruction-level parallelism, joined by one double-double product;
-//  * the eight signed terms of a Gray group are summed with TwoSum into a
-//    (hi, lo) pair whose low parts collect every rounding error (Sum2 of
-//    Ogita, Rump and Oishi), and each group is added to the thread total the
-//    same way;
+//    FP64) enters a double-double product as soon as it is formed: the
+//    first two by TwoProd (h = v0 v1, l = fma(v0, v1, -h), exact), every
+//    further value by h' = h v, l' = fma(l, v, fma(h, v, -h')) (3
+//    operations, relative error a few u^2);
+//  * every signed term is added to the thread's total with TwoSum into a
+//    (hi, lo) pair whose low part collects every rounding error (Sum2 of
+//    Ogita, Rump and Oishi);
 //  * the walk also sums |hi| of its own terms, so the bound uses the exact
 //    cancellation scale sum|t| instead of a sampled estimate.
 // Per Gray step this adds ~2 ceil(n/G) + 9 FP64 operations to the int32-X
-// step (which is issue-bound with the FP64 pipe mostly idle); the error is
-// below (4 ceil(n/G) + 64) u^2 sum|t| plus the final rounding.
+// step (which is issue-bound with the FP64 pipe mostly idle).  One product
+// chain and one running (hi, lo) keep the step within 168 registers, so 3
+// CTAs fit an SM up to order 40 without spills (two chains and per-group
+// partial sums needed 184 registers: 2 CTAs, 1.33x the int32-X walk's time).
+// Error: below (8 ceil(n/G) + 256 + K^2) u^2 sum|t| for K terms per thread
+// (the low part's own rounding over K terms), plus the final rounding.
 #pragma once
 #include "ryser_dense_int.cuh"
 
@@ -61,59 +63,45 @@ __device__ __forceinline__ void iupdate(int (&y)[N], const int* col, int s) {
   }
 }
 
-// Exact group values: v_g = prod of y over rows [gG, gG + G), formed in
-// uint32 (the host proved |v_g| < 2^31) and converted exactly to FP64.
+// Exact value of group g: the uint32 product of y over rows [gG, gG + G)
+// (the host proved |product| < 2^31), converted exactly to FP64.
 template <int N, int G>
-__device__ __forceinline__ void group_values(const int (&y)[N], double (&v)[(N + G - 1) / G]) {
-  constexpr int NG = (N + G - 1) / G;
+__device__ __forceinline__ double group_value(const int (&y)[N], int g) {
+  const int j0 = g * G;
+  uint32_t pr = (uint32_t)y[j0];
 #pragma unroll
-  for (int g = 0; g < NG; g++) {
-    const int j0 = g * G;
-    uint32_t pr = (uint32_t)y[j0];
-#pragma unroll
-    for (int t = 1; t < G; t++)
-      if (j0 + t < N) pr = pr * (uint32_t)y[j0 + t];
-    v[g] = __int2double_rn((int)pr);
-  }
+  for (int t = 1; t < G; t++)
+    if (j0 + t < N) pr = pr * (uint32_t)y[j0 + t];
+  return __int2double_rn((int)pr);
 }
 
-// Double-double product of v[first], v[first + 2], v[first + 4], ... (an
-// unevaluated pair; the first multiply is an exact TwoProd).
-template <int NG, int kFirst>
-__device__ __forceinline__ dd chain_product(const double (&v)[NG]) {
-  dd p = {v[kFirst], 0.0};
-  if (kFirst + 2 < NG) {
-    p.hi = __dmul_rn(v[kFirst], v[kFirst + 2]);
-    p.lo = __fma_rn(v[kFirst], v[kFirst + 2], -p.hi);
+// Double-double product of the group values (an unevaluated pair), each
+// multiplied in as it is formed.
+template <int N, int G>
+__device__ __forceinline__ dd term_dd(const int (&y)[N]) {
+  constexpr int NG = (N + G - 1) / G;
+  dd p = {group_value<N, G>(y, 0), 0.0};
+  if (NG == 1) return p;
+  {
+    const double v = group_value<N, G>(y, 1);
+    const double h = __dmul_rn(p.hi, v);
+    p.lo = __fma_rn(p.hi, v, -h);
+    p.hi = h;
   }
 #pragma unroll
-  for (int g = kFirst + 4; g < NG; g += 2) {
-    const double h = __dmul_rn(p.hi, v[g]);
-    const double l = __fma_rn(p.hi, v[g], -h);
-    p.lo = __fma_rn(p.lo, v[g], l);
+  for (int g = 2; g < NG; g++) {
+    const double v = group_value<N, G>(y, g);
+    const double h = __dmul_rn(p.hi, v);
+    const double l = __fma_rn(p.hi, v, -h);
+    p.lo = __fma_rn(p.lo, v, l);
     p.hi = h;
   }
   return p;
 }
 
-template <int N, int G>
-__device__ __forceinline__ dd term_dd(const int (&y)[N]) {
-  constexpr int NG = (N + G - 1) / G;
-  double v[NG];
-  group_values<N, G>(y, v);
-  const dd a = chain_product<NG, 0>(v);
-  if (NG == 1) return a;
-  const dd b = chain_product<NG, 1>(v);
-  // a x b: exact high product and its error, plus both cross terms
-  const double h = __dmul_rn(a.hi, b.hi);
-  double l = __fma_rn(a.hi, b.hi, -h);
-  if (NG > 3) l = __fma_rn(a.hi, b.lo, l);  // b has a low part from three groups on
-  if (NG > 2) l = __fma_rn(a.lo, b.hi, l);  // a has one from three groups on
-  return {h, l};
-}
-
-// CTAs per SM: 3 (168 registers) up to order 36; above, 2 CTAs and no spills.
-template <int N, int G, int kMinBlocks = (N <= 36 ? 3 : 2)>
+// CTAs per SM: 3 (168 registers, no spills) up to order 36, and up to order
+// 40 with groups of 5 or 6 rows; 2 otherwise.
+template <int N, int G, int kMinBlocks = ((N <= 36 || (N <= 40 && G >= 5)) ? 3 : 2)>
 __global__ void __launch_bounds__(128, kMinBlocks) ryser_dense_intc_kernel(DenseIntcArgs args) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int np4 = args.np4;
@@ -159,47 +147,43 @@ __global__ void __launch_bounds__(128, kMinBlocks) ryser_dense_intc_kernel(Dense
     // the eighth flips column k8 >= 3 (kLast: only seven steps)
     auto group8 = [&](bool kLast) {
       const int s4 = ((base >> 3) & 1) ? -1 : 1;
-      double gs, gc;
       iupdate<N, +1>(y, c0, 0);
       dd t = term_dd<N, G>(y);
-      gs = -t.hi;
-      gc = -t.lo;
-      double ma = fabs(t.hi);
+      sum2_add(H, L, -t.hi, -t.lo);
+      m1 += fabs(t.hi);
       iupdate<N, +1>(y, c1, 0);
       t = term_dd<N, G>(y);
-      sum2_add(gs, gc, t.hi, t.lo);
-      ma += fabs(t.hi);
+      sum2_add(H, L, t.hi, t.lo);
+      m1 += fabs(t.hi);
       iupdate<N, -1>(y, c0, 0);
       t = term_dd<N, G>(y);
-      sum2_add(gs, gc, -t.hi, -t.lo);
-      ma += fabs(t.hi);
+      sum2_add(H, L, -t.hi, -t.lo);
+      m1 += fabs(t.hi);
       iupdate<N, 0>(y, c2, s4);
       t = term_dd<N, G>(y);
-      sum2_add(gs, gc, t.hi, t.lo);
-      ma += fabs(t.hi);
+      sum2_add(H, L, t.hi, t.lo);
+      m1 += fabs(t.hi);
       iupdate<N, +1>(y, c0, 0);
       t = term_dd<N, G>(y);
-      sum2_add(gs, gc, -t.hi, -t.lo);
-      ma += fabs(t.hi);
+      sum2_add(H, L, -t.hi, -t.lo);
+      m1 += fabs(t.hi);
       iupdate<N, -1>(y, c1, 0);
       t = term_dd<N, G>(y);
-      sum2_add(gs, gc, t.hi, t.lo);
-      ma += fabs(t.hi);
+      sum2_add(H, L, t.hi, t.lo);
+      m1 += fabs(t.hi);
       iupdate<N, -1>(y, c0, 0);
       t = term_dd<N, G>(y);
-      sum2_add(gs, gc, -t.hi, -t.lo);
-      ma += fabs(t.hi);
+      sum2_add(H, L, -t.hi, -t.lo);
+      m1 += fabs(t.hi);
       if (!kLast) {
         const uint64_t i8 = base + 8;
         const int k8 = __ffsll((long long)i8) - 1;
         const int s8 = ((i8 >> (k8 + 1)) & 1) ? -1 : 1;
         iupdate<N, 0>(y, sC + k8 * np4, s8);
         t = term_dd<N, G>(y);
-        sum2_add(gs, gc, t.hi, t.lo);
-        ma += fabs(t.hi);
+        sum2_add(H, L, t.hi, t.lo);
+        m1 += fabs(t.hi);
       }
-      sum2_add(H, L, gs, gc);
-      m1 += ma;
     };
 #pragma unroll 1
     for (uint64_t gi = 0; gi + 1 < groups; gi++, base += 8) group8(false);

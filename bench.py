@@ -220,10 +220,8 @@ def kernel_template(kname: str, A: np.ndarray) -> str:
     if kname == "int32x":
         return f"ryser_dense_int_kernel<{n}, {int_group_size(A)}>"
     if kname == "int32x_dd":
-        # third template argument: CTAs per SM compiled for (3 up to order 36, and up
-        # to 40 with groups of 5 or 6 rows; 2 otherwise)
-        g = int_group_size(A)
-        return f"ryser_dense_intc_kernel<{n}, {g}, {3 if n <= 36 or (n <= 40 and g >= 5) else 2}>"
+        # third template argument: CTAs per SM compiled for (3 up to order 36, 2 above)
+        return f"ryser_dense_intc_kernel<{n}, {int_group_size(A)}, {3 if n <= 36 else 2}>"
     if kname == "fp64x":
         return f"ryser_dense_kernel<{n}>"
     return kname

@@ -20,9 +20,9 @@
 //    cancellation scale sum|t| instead of a sampled estimate.
 // Per Gray step this adds ~2 ceil(n/G) + 9 FP64 operations to the int32-X
 // step (which is issue-bound with the FP64 pipe mostly idle).  One product
-// chain and one running (hi, lo) keep the step within 168 registers, so 3
-// CTAs fit an SM up to order 40 without spills (two chains and per-group
-// partial sums needed 184 registers: 2 CTAs, 1.33x the int32-X walk's time).
+// chain and one running (hi, lo) per thread: at order 40 this measured 1.4%
+// faster than two chains joined at the end with per-group partial sums
+// (2628 against 2664 ms; the int32-X walk: 2007 ms).
 // Error: below (8 ceil(n/G) + 256 + K^2) u^2 sum|t| for K terms per thread
 // (the low part's own rounding over K terms), plus the final rounding.
 #pragma once
@@ -99,9 +99,10 @@ __device__ __forceinline__ dd term_dd(const int (&y)[N]) {
   return p;
 }
 
-// CTAs per SM: 3 (168 registers, no spills) up to order 36, and up to order
-// 40 with groups of 5 or 6 rows; 2 otherwise.
-template <int N, int G, int kMinBlocks = ((N <= 36 || (N <= 40 && G >= 5)) ? 3 : 2)>
+// CTAs per SM: 3 up to order 36 (at most 168 registers without a cap), 2
+// above: at order 40 a 168-register (3-CTA) schedule fits without spills
+// but measured 2% slower than the 203-register one (2680 against 2628 ms).
+template <int N, int G, int kMinBlocks = (N <= 36 ? 3 : 2)>
 __global__ void __launch_bounds__(128, kMinBlocks) ryser_dense_intc_kernel(DenseIntcArgs args) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int np4 = args.np4;

@@ -694,7 +694,9 @@ def batched_secondary(pb, eng, count=8192):
     tune_s = time.perf_counter() - t
     variant = eng.batch_variant()
     sparse_layout = sum(1 for m in mats if m.shape[0] >= 12 and pb.sdd_layout(m) > 0)
+    t = time.perf_counter()
     b = eng.batch(mats)
+    create_ms = (time.perf_counter() - t) * 1e3  # host layout choice and images, upload, graph capture
     b.run()
     times = []
     for _ in range(3):
@@ -750,7 +752,8 @@ def batched_secondary(pb, eng, count=8192):
                                      "reevaluated": reevaluated, "exact_zeros": int(np.sum(pvals == 0.0)),
                                      "max_rel_error_estimate": float(np.max(finite)) if finite.size else None,
                                      "unbounded_estimates": int(est.size - finite.size)},
-            "autotune_s": tune_s, "autotuned_lane_log2": table, "autotuned_kernel_variant": variant,
+            "create_ms": create_ms, "autotune_s": tune_s, "autotuned_lane_log2": table,
+            "autotuned_kernel_variant": variant,
             "matrices_with_a_sparse_column_triple": sparse_layout, "breakdown": breakdown,
             "timing": "CUDA events around the graph launch (queue reset + kernel + 128 KB readback)"}
 

@@ -300,6 +300,10 @@ int perm_batch_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* m_out);
  * per SM it was compiled for, and whether dense FP64 matrices keep X in
  * shared memory. */
 int perm_batch_variant(perm_ctx* ctx, int* variant, int* max_n, int* block, int* min_blocks, int* shared_x);
+/* Makes later perm_batch_create calls use batch kernel variant `variant`
+ * (0 .. 5; a batch with an order above the variant's largest falls back to
+ * variant 0). */
+int perm_batch_use_variant(perm_ctx* ctx, int variant);
 
 /* ---- request loop: continuous batching on one GPU ------------------------------
  * No counterpart in the reference.  `slots` worker contexts run requests

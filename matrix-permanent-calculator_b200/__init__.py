@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = (
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
     "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
-    "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune", "perm_batch_variant",
+    "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune", "perm_batch_variant", "perm_batch_use_variant",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
     "perm_approx_scaling_sparse", "perm_read_matrix", "perm_compress", "perm_grid_graph", "perm_fp64_peak",
@@ -145,6 +145,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_batch_exact": (i, [_P, i, _P, _P, _P, ctypes.POINTER(d)]),
         "perm_batch_autotune": (i, [_P, i, i, _P]),
         "perm_batch_variant": (i, [_P, _P, _P, _P, _P, _P]),
+        "perm_batch_use_variant": (i, [_P, i]),
         "perm_dense_autotune": (i, [_P, i, i, _P]),
         "perm_ctx_set_rel_target": (i, [_P, d]),
         "perm_ctx_inject_wait_timeout": (i, [_P, i]),
@@ -368,6 +369,10 @@ class Engine:
         out = np.zeros(n_hi - n_lo + 1, dtype=np.int32)
         self._check(self.lib.perm_batch_autotune(self.ctx, n_lo, n_hi, _ptr(out)))
         return {n_lo + i: int(m) for i, m in enumerate(out)}
+
+    def batch_use_variant(self, variant: int):
+        """Later batches run kernel variant `variant` (perm_batch_use_variant)."""
+        self._check(self.lib.perm_batch_use_variant(self.ctx, variant))
 
     def batch_variant(self) -> dict:
         """The batch kernel variant later batches use (perm_batch_variant)."""

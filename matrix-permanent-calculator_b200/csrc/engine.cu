@@ -2284,6 +2284,15 @@ extern "C" int perm_batch_autotune(perm_ctx* ctx, int n_lo, int n_hi, int* m_out
   return PERM_OK;
 }
 
+extern "C" int perm_batch_use_variant(perm_ctx* ctx, int variant) {
+  if (!ctx) return PERM_EINVAL;
+  if (variant < 0 || variant >= kBatchVariantCount)
+    return fail(ctx, PERM_EINVAL, "batch kernel variant %d outside [0, %d)", variant, kBatchVariantCount);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->batch_variant = variant;
+  return PERM_OK;
+}
+
 extern "C" int perm_batch_variant(perm_ctx* ctx, int* variant, int* max_n, int* block, int* min_blocks,
                                   int* shared_x) {
   if (!ctx) return PERM_EINVAL;

@@ -165,6 +165,26 @@ def test_sparse_layout_in_the_batch(engine, orc, pb):
         assert rel_err(v, want) < 1e-11, (m.shape, v, want)
 
 
+def test_every_batch_variant_agrees(pb, orc):
+    """Each compiled batch kernel variant (threads per block, register budget,
+    shared-memory X) returns the same permanents, to rounding, on a batch of
+    dense and sparse, 0/1 and real matrices of orders 9..28."""
+    rng = np.random.default_rng(93)
+    mats = mixed_batch(rng, 80, 9, 22)
+    for n in (24, 26, 28):
+        mats.append(bernoulli(rng, n, 0.3) * (1.0 - rng.random((n, n))))
+        mats.append(bernoulli(rng, n, 0.7))
+    with pb.Engine(0) as eng:
+        eng.set_rel_target(-1.0)
+        ref = [eng.exact_dense(m, variant=pb.PERM_KERNEL_DENSE).value for m in mats]
+        for v in range(6):
+            eng.batch_use_variant(v)
+            vals, _ = eng.batch_exact(mats)
+            assert eng.batch_variant()["variant"] == v
+            for m, a, b in zip(mats, vals, ref):
+                assert abs(a - b) <= 1e-10 * abs(b) or abs(a - b) < 1e-12, (v, m.shape, a, b)
+
+
 def test_batch_variants_agree_and_autotune_picks_one(pb):
     """The autotuner measures the compiled batch kernel variants (threads per
     block, register budget, shared-memory X), keeps one, and later batches

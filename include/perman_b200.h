@@ -203,6 +203,17 @@ int perm_ctx_inject_wait_timeout(perm_ctx* ctx, int launches);
  * No counterpart in the reference. */
 int perm_sdd_layout(const double* mat, int n);
 
+/* Host only (no device): the layout PERM_KERNEL_DENSE_INT_DD uses for the
+ * row-major n x n matrix `mat`: returns the product-group size G (3..6:
+ * every run of G rows has prod(sum_k |a_jk|) < 2^31, so group values are
+ * exact int32 products) and sets *pair to 1 when consecutive group values
+ * are multiplied in FP64 first (every run of 2G rows below 2^53, so those
+ * products are exact; orders >= 16), 0 otherwise; the layout with the
+ * fewest FP64 operations per Gray step is taken.  PERM_EUNSUPPORTED for
+ * non-integer matrices, |a| >= 2^24, orders below 8 or no fitting G;
+ * PERM_EINVAL for bad arguments.  No counterpart in the reference. */
+int perm_intc_layout(const double* mat, int n, int* pair);
+
 /* Measures, for orders n_lo..n_hi (within 8..40), which of the int32-X, the
  * FP64-X and (n >= 16) the tensor-core kernel is fastest on this device for
  * integer inputs and makes variant 0 follow the measurement in this context.

@@ -61,6 +61,9 @@ const void* dense_intc_kernel_g3(int n);
 const void* dense_intc_kernel_g4(int n);
 const void* dense_intc_kernel_g5(int n);
 const void* dense_intc_kernel_g6(int n);
+const void* dense_intc_pair_kernel_g4(int n);
+const void* dense_intc_pair_kernel_g5(int n);
+const void* dense_intc_pair_kernel_g6(int n);
 
 const void* dense_sdd_kernel(int n);
 const void* sparse_sdd_kernel_r6(int n);
@@ -93,7 +96,15 @@ static const void* dense_int_kernel(int n, int g) {
   }
 }
 
-static const void* dense_intc_kernel(int n, int g) {
+static const void* dense_intc_kernel(int n, int g, int pair) {
+  if (pair) {
+    switch (g) {
+      case 4: return dense_intc_pair_kernel_g4(n);
+      case 5: return dense_intc_pair_kernel_g5(n);
+      case 6: return dense_intc_pair_kernel_g6(n);
+      default: return nullptr;
+    }
+  }
   switch (g) {
     case 3: return dense_intc_kernel_g3(n);
     case 4: return dense_intc_kernel_g4(n);
@@ -274,8 +285,9 @@ struct perm_ctx {
   size_t d_trials_cap = 0;
   // occupancy per kernel family and order: [0] FP64-X, [G] int32-X, [7] dd,
   // [8 + G - 3] tensor core, [12] split X, [13 + G - 3] certified int32-X,
-  // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows
-  int dense_occ[22][PERM_MAX_EXACT_N + 1] = {};
+  // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows,
+  // [22 + G - 4] certified int32-X with exact pairs of groups
+  int dense_occ[25][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
@@ -495,32 +507,73 @@ static int finish_and_read(perm_ctx* ctx, int nout) {
 // rounded up to a multiple of 4) for the int32-X kernel.
 struct DenseOperand {
   int n = 0, variant = PERM_KERNEL_DENSE, group = 0;
+  int pair = 0;   // certified int32-X walk: consecutive groups multiplied in exact FP64 pairs
   int inner = 0;  // split-dd: rows 0..inner-1 hold the support of columns 0..2 (0: dense layout)
   std::vector<unsigned char> image;
 };
+
+// Row absolute sums of an integer-valued matrix with |a| < 2^24 (each bounds
+// |y_j| = |2 x_j| along the whole walk); false for other matrices.
+static bool int_row_abs(const std::vector<double>& a, int n, std::vector<double>& rowabs) {
+  rowabs.assign(n, 0.0);
+  for (int j = 0; j < n; j++)
+    for (int k = 0; k < n; k++) {
+      const double v = a[(size_t)j * n + k];
+      if (v != std::floor(v) || std::fabs(v) >= 16777216.0) return false;
+      rowabs[j] += std::fabs(v);
+    }
+  return true;
+}
+
+// Whether every run of `span` consecutive rows starting at multiples of
+// `span` has prod(max(sum_k |a_jk|, 1)) below `limit`.
+static bool runs_fit(const std::vector<double>& rowabs, int n, int span, double limit) {
+  for (int j0 = 0; j0 < n; j0 += span) {
+    double b = 1.0;
+    for (int t = 0; t < span && j0 + t < n; t++) b *= std::max(rowabs[j0 + t], 1.0);
+    if (!(b < limit)) return false;
+  }
+  return true;
+}
 
 // Integer-valued with |a| < 2^24 and a product grouping that provably fits in
 // int32: returns the largest group size G in {6,5,4,3} such that every run of
 // G consecutive rows has prod(sum_k |a_jk|) < 2^31, or 0.
 static int int_group_size(const std::vector<double>& a, int n) {
   if (n < 8) return 0;
-  std::vector<double> rowabs(n, 0.0);
-  for (int j = 0; j < n; j++)
-    for (int k = 0; k < n; k++) {
-      const double v = a[(size_t)j * n + k];
-      if (v != std::floor(v) || std::fabs(v) >= 16777216.0) return 0;
-      rowabs[j] += std::fabs(v);
-    }
-  for (int G = 6; G >= 3; G--) {
-    bool ok = true;
-    for (int j0 = 0; j0 < n && ok; j0 += G) {
-      double b = 1.0;
-      for (int t = 0; t < G && j0 + t < n; t++) b *= std::max(rowabs[j0 + t], 1.0);
-      ok = b < 2147483648.0;
-    }
-    if (ok) return G;
-  }
+  std::vector<double> rowabs;
+  if (!int_row_abs(a, n, rowabs)) return 0;
+  for (int G = 6; G >= 3; G--)
+    if (runs_fit(rowabs, n, G, 2147483648.0)) return G;
   return 0;
+}
+
+// Layout of the certified int32-X walk (ryser_dense_intc.cuh): product
+// groups of G rows (each |product| < 2^31) whose values enter a
+// double-double product, optionally (*pair, orders >= 16, G >= 4) first
+// multiplied in consecutive pairs in FP64, exact when every run of 2G rows
+// has prod(sum_k |a_jk|) < 2^53.  The integer multiplies and conversions
+// cost n per Gray step whatever G is; the FP64 part costs 3 F - 4 operations
+// for F double-double factors plus one per exact pair, so the layout with
+// the fewest of those is taken.  Returns G, or 0 when int32 X does not apply.
+static int intc_layout(const std::vector<double>& a, int n, int* pair) {
+  *pair = 0;
+  if (n < 8) return 0;
+  std::vector<double> rowabs;
+  if (!int_row_abs(a, n, rowabs)) return 0;
+  int best_g = 0, best_pair = 0, best_cost = 1 << 30;
+  for (int G = 6; G >= 3; G--) {
+    if (!runs_fit(rowabs, n, G, 2147483648.0)) continue;
+    const int ng = (n + G - 1) / G;
+    const int chain = 3 * ng - 4;
+    if (chain < best_cost) best_g = G, best_pair = 0, best_cost = chain;
+    if (n >= 16 && G >= 4 && runs_fit(rowabs, n, 2 * G, 9007199254740992.0)) {
+      const int nf = (ng + 1) / 2, paired = ng / 2 + 3 * nf - 4;
+      if (paired < best_cost) best_g = G, best_pair = 1, best_cost = paired;
+    }
+  }
+  *pair = best_pair;
+  return best_g;
 }
 
 // The tensor-core kernel takes int8 operands: |2a| <= 127, which also keeps
@@ -714,6 +767,8 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
                   : variant == PERM_KERNEL_DENSE_INT_DD ? PERM_KERNEL_DENSE_INT_DD
                                                         : PERM_KERNEL_DENSE_INT;
     op->group = G;
+    op->pair = 0;
+    if (op->variant == PERM_KERNEL_DENSE_INT_DD) op->group = intc_layout(a, n, &op->pair);
     op->image.assign(sizeof(int) * (size_t)(n + 1) * np4, 0);
     int* img = reinterpret_cast<int*>(op->image.data());
     for (int k = 0; k < n; k++)
@@ -743,7 +798,7 @@ struct perm_matrix {
 
 static const void* operand_kernel(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_kernel(op.n, op.group);
-  if (op.variant == PERM_KERNEL_DENSE_INT_DD) return dense_intc_kernel(op.n, op.group);
+  if (op.variant == PERM_KERNEL_DENSE_INT_DD) return dense_intc_kernel(op.n, op.group, op.pair);
   if (op.variant == PERM_KERNEL_DENSE_SDD) return sdd_kernel(op.n, op.inner);
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
@@ -785,6 +840,13 @@ static void shard_bounds(int n, int shard, int nshards, uint64_t* first, uint64_
   if (ms_out) *ms_out = ms;
 }
 
+extern "C" int perm_intc_layout(const double* mat, int n, int* pair) {
+  if (!mat || !pair || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
+  std::vector<double> a(mat, mat + (size_t)n * n);
+  const int g = intc_layout(a, n, pair);
+  return g ? g : PERM_EUNSUPPORTED;
+}
+
 extern "C" int perm_sdd_layout(const double* mat, int n) {
   if (!mat || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
   std::vector<double> a(mat, mat + (size_t)n * n);
@@ -811,7 +873,7 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
                                  : op.variant == PERM_KERNEL_DENSE_DD ? 7
                                  : op.variant == PERM_KERNEL_DENSE_TC ? 8 + op.group - 3
                                  : op.variant == PERM_KERNEL_DENSE_SPLIT ? 12
-                                 : op.variant == PERM_KERNEL_DENSE_INT_DD ? 13 + op.group - 3
+                                 : op.variant == PERM_KERNEL_DENSE_INT_DD ? (op.pair ? 22 + op.group - 4 : 13 + op.group - 3)
                                  : op.variant == PERM_KERNEL_DENSE_SDD ? (op.inner ? sparse_slot : 17) : 0][n];
   if (!occ_slot) {
     int rc = allow_smem(ctx, fn, operand_smem(op));

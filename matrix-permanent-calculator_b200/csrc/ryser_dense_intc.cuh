@@ -13,6 +13,11 @@
 //    first two by TwoProd (h = v0 v1, l = fma(v0, v1, -h), exact), every
 //    further value by h' = h v, l' = fma(l, v, fma(h, v, -h')) (3
 //    operations, relative error a few u^2);
+//  * with kPair, consecutive group values are first multiplied in FP64,
+//    which is exact because the host proved every pair's |product| < 2^53:
+//    one multiply replaces a 3-operation double-double step (order 40,
+//    groups of 4 rows: 16 FP64 operations per term instead of 20 with
+//    groups of 5, measured 3.4% faster: 2534 against 2624 ms);
 //  * every signed term is added to the thread's total with TwoSum into a
 //    (hi, lo) pair whose low part collects every rounding error (Sum2 of
 //    Ogita, Rump and Oishi);
@@ -75,22 +80,34 @@ __device__ __forceinline__ double group_value(const int (&y)[N], int g) {
   return __int2double_rn((int)pr);
 }
 
-// Double-double product of the group values (an unevaluated pair), each
+// Factor i of the double-double product: group value i, or with kPair the
+// exact FP64 product of group values 2i and 2i + 1 (the last one alone when
+// the number of groups is odd).
+template <int N, int G, bool kPair>
+__device__ __forceinline__ double term_factor(const int (&y)[N], int i) {
+  constexpr int NG = (N + G - 1) / G;
+  if (!kPair) return group_value<N, G>(y, i);
+  const double a = group_value<N, G>(y, 2 * i);
+  return (2 * i + 1 < NG) ? __dmul_rn(a, group_value<N, G>(y, 2 * i + 1)) : a;
+}
+
+// Double-double product of the factors (an unevaluated pair), each
 // multiplied in as it is formed.
-template <int N, int G>
+template <int N, int G, bool kPair>
 __device__ __forceinline__ dd term_dd(const int (&y)[N]) {
   constexpr int NG = (N + G - 1) / G;
-  dd p = {group_value<N, G>(y, 0), 0.0};
-  if (NG == 1) return p;
+  constexpr int NF = kPair ? (NG + 1) / 2 : NG;
+  dd p = {term_factor<N, G, kPair>(y, 0), 0.0};
+  if (NF == 1) return p;
   {
-    const double v = group_value<N, G>(y, 1);
+    const double v = term_factor<N, G, kPair>(y, 1);
     const double h = __dmul_rn(p.hi, v);
     p.lo = __fma_rn(p.hi, v, -h);
     p.hi = h;
   }
 #pragma unroll
-  for (int g = 2; g < NG; g++) {
-    const double v = group_value<N, G>(y, g);
+  for (int i = 2; i < NF; i++) {
+    const double v = term_factor<N, G, kPair>(y, i);
     const double h = __dmul_rn(p.hi, v);
     const double l = __fma_rn(p.hi, v, -h);
     p.lo = __fma_rn(p.lo, v, l);
@@ -101,8 +118,9 @@ __device__ __forceinline__ dd term_dd(const int (&y)[N]) {
 
 // CTAs per SM: 3 up to order 36 (at most 168 registers without a cap), 2
 // above: at order 40 a 168-register (3-CTA) schedule fits without spills
-// but measured 2% slower than the 203-register one (2680 against 2628 ms).
-template <int N, int G, int kMinBlocks = (N <= 36 ? 3 : 2)>
+// but measured 2% slower than the 203-register one (2680 against 2628 ms;
+// paired groups of 4: 2560 against 2534 ms).
+template <int N, int G, bool kPair = false, int kMinBlocks = (N <= 36 ? 3 : 2)>
 __global__ void __launch_bounds__(128, kMinBlocks) ryser_dense_intc_kernel(DenseIntcArgs args) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int np4 = args.np4;
@@ -133,7 +151,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) ryser_dense_intc_kernel(Dense
       }
     }
     {
-      const dd t0 = term_dd<N, G>(y);  // index s0 is even: sign +
+      const dd t0 = term_dd<N, G, kPair>(y);  // index s0 is even: sign +
       H = t0.hi;
       L = t0.lo;
       m1 = fabs(t0.hi);
@@ -149,31 +167,31 @@ __global__ void __launch_bounds__(128, kMinBlocks) ryser_dense_intc_kernel(Dense
     auto group8 = [&](bool kLast) {
       const int s4 = ((base >> 3) & 1) ? -1 : 1;
       iupdate<N, +1>(y, c0, 0);
-      dd t = term_dd<N, G>(y);
+      dd t = term_dd<N, G, kPair>(y);
       sum2_add(H, L, -t.hi, -t.lo);
       m1 += fabs(t.hi);
       iupdate<N, +1>(y, c1, 0);
-      t = term_dd<N, G>(y);
+      t = term_dd<N, G, kPair>(y);
       sum2_add(H, L, t.hi, t.lo);
       m1 += fabs(t.hi);
       iupdate<N, -1>(y, c0, 0);
-      t = term_dd<N, G>(y);
+      t = term_dd<N, G, kPair>(y);
       sum2_add(H, L, -t.hi, -t.lo);
       m1 += fabs(t.hi);
       iupdate<N, 0>(y, c2, s4);
-      t = term_dd<N, G>(y);
+      t = term_dd<N, G, kPair>(y);
       sum2_add(H, L, t.hi, t.lo);
       m1 += fabs(t.hi);
       iupdate<N, +1>(y, c0, 0);
-      t = term_dd<N, G>(y);
+      t = term_dd<N, G, kPair>(y);
       sum2_add(H, L, -t.hi, -t.lo);
       m1 += fabs(t.hi);
       iupdate<N, -1>(y, c1, 0);
-      t = term_dd<N, G>(y);
+      t = term_dd<N, G, kPair>(y);
       sum2_add(H, L, t.hi, t.lo);
       m1 += fabs(t.hi);
       iupdate<N, -1>(y, c0, 0);
-      t = term_dd<N, G>(y);
+      t = term_dd<N, G, kPair>(y);
       sum2_add(H, L, -t.hi, -t.lo);
       m1 += fabs(t.hi);
       if (!kLast) {
@@ -181,7 +199,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) ryser_dense_intc_kernel(Dense
         const int k8 = __ffsll((long long)i8) - 1;
         const int s8 = ((i8 >> (k8 + 1)) & 1) ? -1 : 1;
         iupdate<N, 0>(y, sC + k8 * np4, s8);
-        t = term_dd<N, G>(y);
+        t = term_dd<N, G, kPair>(y);
         sum2_add(H, L, t.hi, t.lo);
         m1 += fabs(t.hi);
       }

@@ -75,6 +75,23 @@ def test_header_constants_match_the_binding(pb):
             assert hasattr(pb, name), name
 
 
+def test_intc_layout_query(pb):
+    """Host-only layout of the certified int32-X walk: the product-group size
+    is the int32-X rule's, and consecutive groups are paired (exact FP64
+    products) from order 16 when every run of 2G rows stays below 2^53 --
+    the layout with the fewest FP64 operations per Gray step."""
+    rng = np.random.default_rng(3)
+    A = ((rng.random((40, 40)) < 0.5) * rng.integers(1, 5, (40, 40))).astype(float)
+    assert pb.intc_layout(A) == (4, True)  # groups of 5 fit int32, pairs of 5 would not fit 2^53
+    B = (rng.random((40, 40)) < 0.5).astype(float)
+    assert pb.intc_layout(B) == (6, True)
+    assert pb.intc_layout(B[:12, :12])[1] is False  # pairs from order 16
+    C = rng.integers(0, 60, (24, 24)).astype(float)
+    assert pb.intc_layout(C) == (3, False)  # large entries: groups of 3, no pairs
+    assert pb.intc_layout(rng.random((20, 20)))[0] == pb.PERM_EUNSUPPORTED
+    assert pb.intc_layout(np.ones((7, 7)))[0] == pb.PERM_EUNSUPPORTED
+
+
 def test_sdd_layout_query(pb):
     """Host-only layout query: dense matrices keep the dense layout, sparse
     ones get the smallest inner-row count that holds their three sparsest

@@ -28,7 +28,9 @@ def test_int_dd_vs_exact(engine, orc, pb, n):
         "binary": bernoulli(rng, n, 0.5),
         "large": rng.integers(0, 60, (n, n)).astype(float),  # small product groups
     }
+    layouts = set()
     for kind, A in cases.items():
+        layouts.add(pb.intc_layout(A))
         exact = orc.perm_exact_int(A)[0]
         r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT_DD)
         assert r.kernel == pb.PERM_KERNEL_DENSE_INT_DD
@@ -39,6 +41,8 @@ def test_int_dd_vs_exact(engine, orc, pb, n):
         assert ok, (kind, info)
         assert r.rel_error_estimate < 1e-20, (kind, r.rel_error_estimate)  # u^2-level bound
         assert rel_err(r.value, exact) <= 1.2e-16  # value is the pair rounded once (<= 2^-53)
+    if n >= 16:  # both product layouts ran: exact FP64 pairs of groups and the plain chain
+        assert {p for _, p in layouts} == {True, False}, layouts
 
 
 def test_int_dd_golden_n32(engine, golden, pb):

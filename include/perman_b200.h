@@ -162,24 +162,38 @@ int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int va
  * policy; < 0 also skips the estimate):
  *  - a zero pattern without a perfect matching returns exactly 0;
  *  - whole walks of integer matrices whose group products fit in int32 run
- *    PERM_KERNEL_DENSE_INT_DD at once (about 1.2 int32-X walks), and real
+ *    PERM_KERNEL_DENSE_INT_DD at once (about 1.3 int32-X walks), and real
  *    matrices of order 12..40 whose three sparsest columns touch at most 16
  *    rows run PERM_KERNEL_DENSE_SDD in its sparse layout: their bound is the
  *    estimate, no other step runs;
+ *  - for other nonnegative real matrices of order 28..40 the FP64-X walk's
+ *    bound is predicted on the device before any walk (stratified sample of
+ *    sum |term| and a weighted-Rasmussen estimate of perm, 4096 trials); when
+ *    it is above 1.5x the target PERM_KERNEL_DENSE_SDD (dense layout, about
+ *    4.2 FP64-X walks) runs at once and alone;
  *  - a result whose bound exceeds the target is cross-checked against
  *    B = A^T with its first row times 3 (perm(B) = 3 perm(A), independent
  *    roundings) and kept when max(4-sigma independent-rounding estimate from
  *    sum term^2, 16 |perm(A) - perm(B)/3| / |perm(A)|) meets the target, which
- *    then is the reported estimate;
- *  - after an FP64-X first pass (orders 4..40) the same check runs on split-X
- *    walks of A and B, returning the split-X value (kernel
- *    PERM_KERNEL_DENSE_SPLIT) when it passes;
+ *    then is the reported estimate; after an FP64-X first pass whose bound is
+ *    above 4x the target this check is skipped where split-dd applies
+ *    (orders 4..40), since it rarely passes there;
  *  - otherwise it is recomputed by a certified kernel: PERM_KERNEL_DENSE_INT_DD
  *    (integer, orders 8..64, directly after an int32-X first pass),
- *    PERM_KERNEL_DENSE_SDD (orders 4..40) or the double-double kernel (orders
- *    <= 40, where neither applies).
+ *    PERM_KERNEL_DENSE_SDD (orders 4..40, about 4.2 FP64-X walks) or the
+ *    double-double kernel (orders <= 40, where neither applies).
  * kernel_ms covers every launch.  PERM_KERNEL_DENSE_DD forces that kernel. */
 int perm_ctx_set_rel_target(perm_ctx* ctx, double rel_target);
+
+/* The kernel the accuracy policy starts a whole-walk perm_exact_dense call
+ * with for this matrix: PERM_KERNEL_DENSE_INT_DD or PERM_KERNEL_DENSE_SDD
+ * when a certified walk goes first and is the whole evaluation, 0 when the
+ * FP64-X / int32-X walk goes first or the policy is off.  For nonnegative
+ * real matrices of order 28..40 this runs the device prediction above (tens
+ * of microseconds) and *fp64_bound (may be NULL) receives the predicted
+ * FP64-X bound; otherwise 0.  The request loop uses it to run such requests
+ * unsliced.  No counterpart in the reference. */
+int perm_exact_dense_plan(perm_ctx* ctx, const void* mat, int n, int dtype, int* kernel, double* fp64_bound);
 
 /* Failure-injection hook for tests of the bounded device waits.  The next
  * `launches` launches of the FP64-X dense kernel (PERM_KERNEL_DENSE) or of

@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
-    "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_intc_layout", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
+    "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_intc_layout", "perm_exact_dense_plan", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
     "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune", "perm_batch_variant", "perm_batch_use_variant",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
@@ -120,6 +120,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_shard_range": (i, [i, i, i, ctypes.POINTER(u64), ctypes.POINTER(u64)]),
         "perm_sdd_layout": (i, [_P, i]),
         "perm_intc_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int)]),
+        "perm_exact_dense_plan": (i, [_P, _P, i, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
         "perm_matrix_create_dense_ex": (i, [_P, _P, i, i, i, ctypes.POINTER(_P)]),
         "perm_exact_sparse": (i, [_P, i, _P, _P, _P, _P, _P, _P, ctypes.POINTER(PermResult)]),
         "perm_exact_sparse_ex": (i, [_P, i, _P, _P, _P, _P, _P, _P, i, ctypes.POINTER(PermResult)]),
@@ -261,6 +262,17 @@ class Engine:
         else:
             self._check(self.lib.perm_exact_dense(self.ctx, _ptr(a), a.shape[0], dt, ctypes.byref(r)))
         return _exact(r)
+
+    def dense_plan(self, mat) -> tuple[int, float]:
+        """(kernel, predicted FP64-X bound) the accuracy policy starts a
+        whole-walk call with (perm_exact_dense_plan): PERM_KERNEL_DENSE_INT_DD
+        or PERM_KERNEL_DENSE_SDD when a certified walk is the whole
+        evaluation, 0 when the FP64-X / int32-X walk goes first; the bound is
+        0 where no prediction ran."""
+        a, dt = _as_matrix(mat)
+        k, b = ctypes.c_int(0), ctypes.c_double(0.0)
+        self._check(self.lib.perm_exact_dense_plan(self.ctx, _ptr(a), a.shape[0], dt, ctypes.byref(k), ctypes.byref(b)))
+        return k.value, b.value
 
     def refine_dense(self, mat, hi: float, lo: float, kernel_ms: float = 0.0) -> ExactResult:
         """Accuracy policy and error estimate for a whole-walk value assembled

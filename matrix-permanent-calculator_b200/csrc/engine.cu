@@ -238,6 +238,63 @@ __global__ void __launch_bounds__(256) ryser_abs_sample_kernel(const double* col
   }
 }
 
+// Size estimate of perm(A) for a nonnegative matrix, for the accuracy
+// policy's choice of its first walk: Rasmussen's estimator with weights.
+// Row i picks an unused column c with probability a_ic / R_i (R_i: the row's
+// sum over unused columns) and multiplies the trial weight by R_i, so the
+// expected weight is perm(A).  One trial per thread on a splitmix64 stream;
+// weights are kept as log2 and scaled by 2^-log2_ub (log2_ub: log2 of the
+// product of the row sums, an upper bound of every weight), so the scaled
+// weights lie in [0, 1] and their block sums are added to *out.  A trial
+// whose row sum vanishes has weight 0.
+__global__ void __launch_bounds__(256) weighted_rasmussen_kernel(const double* colA, int n, int np, int trials,
+                                                                 uint64_t seed, double log2_ub, double* out) {
+  __shared__ double sA[64 * 64];
+  __shared__ double red[8];
+  for (int idx = threadIdx.x; idx < n * np; idx += blockDim.x) sA[idx] = colA[idx];
+  __syncthreads();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double w = 0.0;
+  if (t < trials) {
+    uint64_t st = seed ^ ((uint64_t)t * 0xD1B54A32D192ED03ull);
+    uint64_t used = 0;
+    double lw = 0.0;
+    bool alive = true;
+    for (int i = 0; i < n && alive; i++) {
+      double r = 0.0;
+      for (int c = 0; c < n; c++)
+        if (!((used >> c) & 1)) r += sA[c * np + i];
+      if (!(r > 0.0)) {
+        alive = false;
+        break;
+      }
+      lw += log2(r);
+      const double u = r * ((double)(splitmix64(st) >> 11) * 0x1.0p-53);
+      double acc = 0.0;
+      int pick = -1;
+      for (int c = 0; c < n; c++) {
+        if ((used >> c) & 1) continue;
+        const double v = sA[c * np + i];
+        if (v > 0.0) {
+          pick = c;
+          acc += v;
+          if (acc > u) break;
+        }
+      }
+      used |= 1ull << pick;  // r > 0: some unused column is positive
+    }
+    if (alive) w = exp2(lw - log2_ub);
+  }
+  for (int d = 16; d >= 1; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = w;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) b += red[k];
+    atomicAdd(out, b);
+  }
+}
+
 __global__ void fp64_peak_kernel(double* out, int iters, double a, double b) {
   double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-3, x2 = x0 + 2e-3, x3 = x0 + 3e-3;
   double x4 = x0 + 4e-3, x5 = x0 + 5e-3, x6 = x0 + 6e-3, x7 = x0 + 7e-3;
@@ -291,7 +348,7 @@ struct perm_ctx {
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
-  double* d_est = nullptr;                       // sample-kernel / split-walk moment accumulator
+  double* d_est = nullptr;  // [0..1] sample-kernel / walk moment accumulators, [2] size-estimate sum
   double split_m1 = 0, split_m2 = 0;             // last split-X walk: sum |term|, sum term^2
   double walk_m1 = 0;                            // last certified (int32-X dd or split-dd) walk: sum |term|
   uint64_t walk_terms_per_thread = 0;            // ... and its longest thread range
@@ -455,7 +512,7 @@ static int ctx_init(perm_ctx* ctx, int device) {
   CU(ctx, cudaMalloc(&ctx->d_out, sizeof(double) * 8));
   CU(ctx, cudaMalloc(&ctx->d_err, sizeof(int) * 4));
   CU(ctx, cudaMalloc(&ctx->d_counters, sizeof(unsigned long long) * 4));
-  CU(ctx, cudaMalloc(&ctx->d_est, sizeof(double) * 2));
+  CU(ctx, cudaMalloc(&ctx->d_est, sizeof(double) * 4));
   CU(ctx, cudaMemset(ctx->ticket, 0, sizeof(unsigned) * 4));
   CU(ctx, cudaMemset(ctx->d_err, 0, sizeof(int) * 4));
   CU(ctx, cudaMallocHost(&ctx->h_out, sizeof(double) * 16));
@@ -1267,27 +1324,25 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
   const double target = ctx->rel_target;
   if (!policy || e.worst <= target || op.variant == PERM_KERNEL_DENSE_DD) return PERM_OK;
   const bool int_first = op.variant == PERM_KERNEL_DENSE_INT || op.variant == PERM_KERNEL_DENSE_TC;
-  std::vector<double> b((size_t)n * n);
-  for (int i2 = 0; i2 < n; i2++)
-    for (int j2 = 0; j2 < n; j2++)
-      b[(size_t)i2 * n + j2] = elem(mat, dtype, (size_t)j2 * n + i2) * (i2 == 0 ? 3.0 : 1.0);
-  // Split X (orders 4..40) after an FP64-X first pass; an int32-X one has
-  // ceil(n/G) roundings per term, already fewer than split X's 2n - 1.
   std::vector<double> av((size_t)n * n);
   for (size_t i = 0; i < av.size(); i++) av[i] = elem(mat, dtype, i);
-  const bool split_ok = n >= 4 && n <= 40 && op.variant != PERM_KERNEL_DENSE_INT &&
-                        op.variant != PERM_KERNEL_DENSE_TC && split_rows_ok(av, n) && split_rows_ok(b, n);
+  // Split-dd (orders 4..40) certifies a real matrix in about 4.2 FP64-X walks.
   // An FP64-X bound well above the target rarely passes an FP64-X
   // cross-check (its correlated X roundings give errors near the bound), so
-  // B is then walked with split X at once, and reused for the split stage.
-  const bool b_split = split_ok && e.worst > 8.0 * target;
-  perm_result rb;
-  bool have_rb = false;
-  // the cross-check's estimate is at least the independent-rounding one
-  if (out->value != 0.0 && e.random <= target && !int_first) {
+  // the certified walk then runs at once; closer to the target one FP64-X
+  // walk of B is tried first.  Split-X cross-checks of A and B would cost
+  // 5.4 walks and can still fail, so the policy does not take them.
+  const bool sdd_ok = !int_first && n >= 4 && n <= 40 && split_rows_ok(av, n);
+  const bool try_cross = out->value != 0.0 && e.random <= target && !int_first &&
+                         !(sdd_ok && e.worst > 4.0 * target);
+  if (try_cross) {
+    std::vector<double> b((size_t)n * n);
+    for (int i2 = 0; i2 < n; i2++)
+      for (int j2 = 0; j2 < n; j2++)
+        b[(size_t)i2 * n + j2] = elem(mat, dtype, (size_t)j2 * n + i2) * (i2 == 0 ? 3.0 : 1.0);
     DenseOperand t;
     perm_result rt;
-    if ((rc = build_operand(ctx, b.data(), n, PERM_F64, b_split ? PERM_KERNEL_DENSE_SPLIT : 0, &t))) return rc;
+    if ((rc = build_operand(ctx, b.data(), n, PERM_F64, 0, &t))) return rc;
     if ((rc = run_whole(ctx, t, &rt))) return rc;
     out->kernel_ms += rt.kernel_ms;
     const double diff = std::fabs(out->value - rt.value / 3.0) / std::fabs(out->value);
@@ -1295,41 +1350,6 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
     if (est <= target) {
       out->rel_error_estimate = est;
       return PERM_OK;
-    }
-    if (b_split) {
-      rb = rt;
-      have_rb = true;
-    }
-  }
-  // split-X walks of A and B: independent per-term roundings; A's walk also
-  // returns the exact moments of its terms, and B runs only if the estimate
-  // from those can meet the target
-  if (split_ok && out->value != 0.0) {
-    DenseOperand sa, sb;
-    perm_result ra;
-    if ((rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE_SPLIT, &sa))) return rc;
-    if ((rc = run_whole(ctx, sa, &ra))) return rc;
-    out->kernel_ms += ra.kernel_ms;
-    ErrEstimate es;
-    es.s1 = ctx->split_m1;
-    es.s2 = ctx->split_m2;
-    error_bounds(PERM_KERNEL_DENSE_SPLIT, 0, n, ra.value, &es);
-    if (ra.value != 0.0 && es.random <= target) {
-      if (!have_rb) {
-        if ((rc = build_operand(ctx, b.data(), n, PERM_F64, PERM_KERNEL_DENSE_SPLIT, &sb))) return rc;
-        if ((rc = run_whole(ctx, sb, &rb))) return rc;
-        out->kernel_ms += rb.kernel_ms;
-      }
-      const double diff = std::fabs(ra.value - rb.value / 3.0) / std::fabs(ra.value);
-      const double est = std::max(es.random, 16.0 * diff);
-      if (est <= target) {
-        const double ms = out->kernel_ms;
-        *out = ra;
-        out->kernel_ms = ms;
-        out->abs_term_sum = es.s1;
-        out->rel_error_estimate = est;
-        return PERM_OK;
-      }
     }
   }
   int cv = 0;
@@ -1359,10 +1379,11 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
 
 // With the accuracy policy on, the kernel a whole-walk call starts with
 // when a certified walk is cheap enough to go first: int32 X with
-// double-double products for integer matrices (about 1.2 int32-X walks, its
+// double-double products for integer matrices (about 1.3 int32-X walks, its
 // bound needs no sample), split-dd in the sparse layout for real matrices
 // whose three sparsest columns touch at most 16 rows (close to an FP64-X
-// walk in cost).  0: the FP64-X / int32-X walk goes first.
+// walk in cost).  0: the FP64-X / int32-X walk goes first (host checks only;
+// policy_predicts_sdd may still choose split-dd for a real matrix).
 static int policy_first_kernel(const void* mat, int n, int dtype) {
   std::vector<double> a((size_t)n * n);
   for (size_t i = 0; i < a.size(); i++) a[i] = elem(mat, dtype, i);
@@ -1370,6 +1391,89 @@ static int policy_first_kernel(const void* mat, int n, int dtype) {
   int c3[3];
   if (split_rows_ok(a, n) && sdd_inner_rows(a, n, c3) > 0) return PERM_KERNEL_DENSE_SDD;
   return 0;
+}
+
+constexpr int kPredictMinOrder = 28;      // below, FP64-X walks cost less than the prediction
+constexpr int kPredictTrials = 4096;      // size-estimate trials (about +-20% at orders 28..40)
+constexpr double kPredictMargin = 1.5;    // predicted FP64-X bound / target that sends a matrix to split-dd
+
+// For a nonnegative real matrix of order kPredictMinOrder..40 whose split
+// image exists: predicts the FP64-X walk's worst-case bound before running
+// it, (2n + 16) u S1 / |perm|, from the stratified sample of S1 = sum|term|
+// and a weighted-Rasmussen estimate of perm(A), and sets *sdd when it is
+// above kPredictMargin x the target.  Such a walk would be followed by the
+// certified split-dd walk anyway (its bound misses the target and an FP64-X
+// cross-check rarely passes there), so split-dd alone costs about 4.2
+// FP64-X walks instead of 5.2 to 6.2.  Context lock held.
+static int policy_predicts_sdd(perm_ctx* ctx, const void* mat, int n, int dtype, bool* sdd, double* bound) {
+  *sdd = false;
+  *bound = 0.0;
+  if (n < kPredictMinOrder || n > 40 || ctx->rel_target <= 0) return PERM_OK;
+  std::vector<double> a((size_t)n * n);
+  double log2_ub = 0.0;
+  for (int j = 0; j < n; j++) {
+    double r = 0.0;
+    for (int k = 0; k < n; k++) {
+      const double v = elem(mat, dtype, (size_t)j * n + k);
+      if (!(v >= 0.0) || !std::isfinite(v)) return PERM_OK;  // nonnegative finite entries only
+      a[(size_t)j * n + k] = v;
+      r += v;
+    }
+    if (!(r > 0.0)) return PERM_OK;  // a zero row: the policy returns 0 at once
+    log2_ub += std::log2(r);
+  }
+  if (!split_rows_ok(a, n)) return PERM_OK;
+  DenseOperand f;
+  int rc = build_operand(ctx, mat, n, dtype, PERM_KERNEL_DENSE, &f);
+  if (rc) return rc;
+  if ((rc = stage_operand(ctx, f))) return rc;
+  const int np = (n + 1) & ~1;
+  const uint64_t threads = (uint64_t)n * kSamplesPerClass;
+  CU(ctx, cudaMemsetAsync(ctx->d_est, 0, 4 * sizeof(double), ctx->stream));
+  ryser_abs_sample_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, ctx->stream>>>(
+      reinterpret_cast<const double*>(ctx->d_stage), n, np, kSamplesPerClass, 0x243F6A8885A308D3ull, ctx->d_est);
+  CU(ctx, cudaGetLastError());
+  weighted_rasmussen_kernel<<<(kPredictTrials + 255) / 256, 256, 0, ctx->stream>>>(
+      reinterpret_cast<const double*>(ctx->d_stage), n, np, kPredictTrials, 0x13198A2E03707344ull, log2_ub,
+      ctx->d_est + 2);
+  CU(ctx, cudaGetLastError());
+  CU(ctx, cudaMemcpyAsync(ctx->h_out + 12, ctx->d_est, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(ctx, cudaStreamSynchronize(ctx->stream));
+  const double s1 = ctx->h_out[12] * 2.0;  // |factor| = 2
+  const double mean_scaled = ctx->h_out[14] / kPredictTrials;
+  if (!(mean_scaled > 0.0)) return PERM_OK;  // no trial found a permutation: leave it to the walk
+  const double log2_perm = std::log2(mean_scaled) + log2_ub;
+  const double log2_bound = std::log2((2.0 * n + 16.0) * std::ldexp(1.0, -53) * s1) - log2_perm;
+  *bound = std::exp2(log2_bound);
+  *sdd = log2_bound > std::log2(kPredictMargin * ctx->rel_target);
+  return PERM_OK;
+}
+
+// The policy's first kernel for a whole-walk call (variant 0, target > 0),
+// with the device prediction for real matrices.  Context lock NOT held.
+static int policy_plan(perm_ctx* ctx, const void* mat, int n, int dtype, int* first, double* bound = nullptr) {
+  double b = 0.0;
+  if (bound) *bound = 0.0;
+  *first = policy_first_kernel(mat, n, dtype);
+  if (*first) return PERM_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CU(ctx, cudaSetDevice(ctx->device));
+  bool sdd = false;
+  const int rc = policy_predicts_sdd(ctx, mat, n, dtype, &sdd, &b);
+  if (bound) *bound = b;
+  if (rc) return rc;
+  if (sdd) *first = PERM_KERNEL_DENSE_SDD;
+  return PERM_OK;
+}
+
+extern "C" int perm_exact_dense_plan(perm_ctx* ctx, const void* mat, int n, int dtype, int* kernel,
+                                     double* fp64_bound) {
+  int rc = check_dense_args(ctx, mat, n, dtype, kernel);
+  if (rc) return rc;
+  *kernel = 0;
+  if (fp64_bound) *fp64_bound = 0.0;
+  if (ctx->rel_target <= 0) return PERM_OK;
+  return policy_plan(ctx, mat, n, dtype, kernel, fp64_bound);
 }
 
 extern "C" int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int variant, int shard,
@@ -1380,7 +1484,9 @@ extern "C" int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dt
   if (nshards < 1 || shard < 0 || shard >= nshards)
     return fail(ctx, PERM_EINVAL, "shard %d of %d", shard, nshards);
   DenseOperand op;
-  const int first = variant == 0 && nshards == 1 && ctx->rel_target > 0 ? policy_first_kernel(mat, n, dtype) : 0;
+  int first = 0;
+  if (variant == 0 && nshards == 1 && ctx->rel_target > 0 && (rc = policy_plan(ctx, mat, n, dtype, &first)))
+    return rc;
   if ((rc = build_operand(ctx, mat, n, dtype, first ? first : variant, &op))) return rc;
   // shards are Gray-index ranges of the walking kernels; the tensor-core
   // kernel's operand image is the int32-X one

@@ -18,7 +18,10 @@
 //    not hold the whole GPU for tens of milliseconds while small requests
 //    wait; shard results are added in double-double and the sum gets the
 //    context's accuracy policy (perm_exact_dense_refine), like an unsliced
-//    request.
+//    request.  A request whose policy starts with a certified walk
+//    (perm_exact_dense_plan: integer matrices, sparse or strongly cancelling
+//    real ones) runs unsliced: that walk is its whole evaluation, where
+//    sliced FP64-X or int32-X shards would be followed by it.
 //  * Every request gets a status; a failing request (bad size, CUDA error)
 //    fails alone.
 #include <cuda_runtime.h>
@@ -141,7 +144,10 @@ void run_job(perm_server* s, perm_ctx* ctx, Job* j) {
         r.kernel = pr.kernel;
       } else {
         const double total = q.n >= 1 && q.n <= PERM_MAX_EXACT_N ? std::ldexp(1.0, q.n - 1) : 1.0;
-        const int shards = (int)std::min(4096.0, std::max(1.0, std::ceil(total / (double)s->slice_steps)));
+        int plan = 0;
+        if (total > (double)s->slice_steps) rc = perm_exact_dense_plan(ctx, a, q.n, PERM_F64, &plan, nullptr);
+        const int shards =
+            plan ? 1 : (int)std::min(4096.0, std::max(1.0, std::ceil(total / (double)s->slice_steps)));
         double hi = 0, lo = 0, dev = 0;
         for (int k = 0; k < shards && rc == PERM_OK; k++) {
           rc = perm_exact_dense_shard(ctx, a, q.n, PERM_F64, k, shards, &pr);

@@ -277,7 +277,7 @@ def test_fp64_error_grows_and_double_double_fixes_it(engine, pb):
         if auto.kernel == pb.PERM_KERNEL_DENSE_SDD:
             assert abs(auto.value - d.value) <= (auto.rel_error_estimate + d.rel_error_estimate + 2.3e-16) * abs(d.value)
         else:
-            assert auto.kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_SPLIT)
+            assert auto.kernel == pb.PERM_KERNEL_DENSE
             assert abs(auto.value - d.value) / abs(d.value) <= auto.rel_error_estimate <= 1e-10
 
 
@@ -521,15 +521,16 @@ def test_split_kernel_order_limits(engine, pb):
 
 
 @pytest.mark.parametrize("n", [31, 33])
-def test_policy_split_stage_meets_the_target(engine, pb, n):
-    """Where the FP64-X cross-check fails, the split-X stage settles most
-    positive real requests without the double-double rerun; whichever kernel
-    the policy ends on, the value is within 1e-10 of double-double."""
+def test_policy_certified_stage_meets_the_target(engine, pb, n):
+    """Where the FP64-X bound misses the target (and the cross-check, where
+    it runs, fails), positive real requests end on the certified split-dd
+    walk; whichever kernel the policy ends on, the value is within 1e-10 of
+    double-double and no split-X pass runs."""
     rng = np.random.default_rng(990 + n)
     A = 1.0 - rng.random((n, n))
     d = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_DD)
     auto = engine.exact_dense(A)
-    assert auto.kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_SPLIT, pb.PERM_KERNEL_DENSE_DD)
+    assert auto.kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_SDD)
     assert abs(auto.value - d.value) <= 1e-10 * abs(d.value)
     assert auto.rel_error_estimate <= 1e-10
 
@@ -580,3 +581,33 @@ def test_term_moment_sample_tracks_the_exact_sum(engine, pb, n):
     f = engine.exact_dense(G, variant=pb.PERM_KERNEL_DENSE)
     s = engine.exact_dense(G, variant=pb.PERM_KERNEL_DENSE_SPLIT)
     assert 0.1 < f.abs_term_sum / s.abs_term_sum < 10.0
+
+
+def test_policy_predicts_the_fp64_bound_before_the_walk(engine, pb):
+    """Nonnegative real matrices of order 28..40: the policy predicts the
+    FP64-X walk's bound before any walk (stratified sample of sum|term| and a
+    weighted-Rasmussen size estimate of perm) and, above 1.5x the target,
+    runs the certified split-dd walk alone.  The prediction is checked
+    against the bound of the FP64-X walk itself; the routing against the
+    planned kernel; the value against the FP64-X value within its bound."""
+    rng = np.random.default_rng(4242)
+    seen = set()
+    for n in (28, 30, 33):
+        A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+        kernel, predicted = engine.dense_plan(A)
+        f = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE)
+        assert predicted > 0.0
+        assert f.rel_error_estimate / 3.0 <= predicted <= 3.0 * f.rel_error_estimate, (n, predicted, f)
+        assert kernel == (pb.PERM_KERNEL_DENSE_SDD if predicted > 1.5e-10 else 0)
+        auto = engine.exact_dense(A)
+        if kernel == pb.PERM_KERNEL_DENSE_SDD:
+            assert auto.kernel == pb.PERM_KERNEL_DENSE_SDD
+            assert auto.kernel_ms < 1.5 * engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SDD).kernel_ms
+        assert auto.rel_error_estimate <= 1e-10
+        assert abs(auto.value - f.value) <= (f.rel_error_estimate + auto.rel_error_estimate) * abs(f.value)
+        seen.add(kernel)
+    assert seen == {0, pb.PERM_KERNEL_DENSE_SDD}, seen
+    # no prediction: below order 28, signed entries, integer matrices (certified first)
+    assert engine.dense_plan(1.0 - rng.random((24, 24))) == (0, 0.0)
+    assert engine.dense_plan(rng.standard_normal((30, 30))) == (0, 0.0)
+    assert engine.dense_plan(rng.integers(0, 4, (30, 30)).astype(float)) == (pb.PERM_KERNEL_DENSE_INT_DD, 0.0)

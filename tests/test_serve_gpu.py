@@ -51,8 +51,8 @@ def test_results_same_alone_and_in_the_mix(engine, pb):
         want, kern = alone(engine, pb, k, A, kw)
         if k in (pb.PERM_REQ_RASMUSSEN, pb.PERM_REQ_SCALING):
             assert r["value"] == want
-        elif {pb.PERM_KERNEL_DENSE_DD, pb.PERM_KERNEL_DENSE_SPLIT} & {kern, r["kernel"]}:
-            # the accuracy policy recomputed one of them (split X or double-double): both meet 1e-10
+        elif {pb.PERM_KERNEL_DENSE_DD, pb.PERM_KERNEL_DENSE_SDD} & {kern, r["kernel"]}:
+            # the accuracy policy recomputed one of them (split-dd or double-double): both meet 1e-10
             assert rel_err(r["value"], want) < 1e-10
         else:
             assert rel_err(r["value"], want) < 1e-12
@@ -60,6 +60,24 @@ def test_results_same_alone_and_in_the_mix(engine, pb):
     for (a0, d0), (a1, d1) in zip(spans, spans[1:]):
         overlap += a1 < d0
     assert overlap > 0, "no two requests were ever in flight together"
+
+
+def test_certified_requests_run_unsliced(engine, pb):
+    """Requests whose policy starts with a certified walk (an integer matrix;
+    a strongly cancelling real one, predicted on the device) run as that one
+    walk even when they are longer than slice_steps: same kernel and the same
+    bits as the call alone."""
+    rng = np.random.default_rng(31)
+    I = (bernoulli(rng, 24, 0.5) * rng.integers(1, 5, (24, 24))).astype(float)
+    R = (rng.random((32, 32)) < 0.5) * (1.0 - rng.random((32, 32)))
+    assert engine.dense_plan(I)[0] == pb.PERM_KERNEL_DENSE_INT_DD
+    assert engine.dense_plan(R)[0] == pb.PERM_KERNEL_DENSE_SDD
+    with pb.Server(0, slots=2, slice_steps=1 << 20) as srv:
+        resps = [srv.wait(srv.submit(pb.PERM_REQ_EXACT_DENSE, M)) for M in (I, R)]
+    for M, r in zip((I, R), resps):
+        assert r["status"] == pb.PERM_OK, r["message"]
+        alone = engine.exact_dense(M)
+        assert r["kernel"] == alone.kernel and r["value"] == alone.value
 
 
 def test_bad_request_fails_alone(pb):

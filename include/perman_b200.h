@@ -163,14 +163,16 @@ int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int va
  *  - a zero pattern without a perfect matching returns exactly 0;
  *  - whole walks of integer matrices whose group products fit in int32 run
  *    PERM_KERNEL_DENSE_INT_DD at once (about 1.3 int32-X walks), and real
- *    matrices of order 12..40 whose three sparsest columns touch at most 16
- *    rows run PERM_KERNEL_DENSE_SDD in its sparse layout: their bound is the
- *    estimate, no other step runs;
+ *    matrices of order 12..40 whose three sparsest columns touch so few rows
+ *    R that the sparse layout's (7 (6R + 9) + 6n + 5) / 8 FP64 operations
+ *    per Gray step are at most FP64 X's 2n run PERM_KERNEL_DENSE_SDD in
+ *    that layout: their bound is the estimate, no other step runs;
  *  - for other nonnegative real matrices of order 28..40 the FP64-X walk's
  *    bound is predicted on the device before any walk (stratified sample of
  *    sum |term| and a weighted-Rasmussen estimate of perm, 4096 trials); when
- *    it is above 1.5x the target PERM_KERNEL_DENSE_SDD (dense layout, about
- *    4.2 FP64-X walks) runs at once and alone;
+ *    it is above 1.5x the target PERM_KERNEL_DENSE_SDD (about 4.2 FP64-X
+ *    walks in the dense layout, less in the sparse one) runs at once and
+ *    alone;
  *  - a result whose bound exceeds the target is cross-checked against
  *    B = A^T with its first row times 3 (perm(B) = 3 perm(A), independent
  *    roundings) and kept when max(4-sigma independent-rounding estimate from

@@ -1381,15 +1381,19 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
 // when a certified walk is cheap enough to go first: int32 X with
 // double-double products for integer matrices (about 1.3 int32-X walks, its
 // bound needs no sample), split-dd in the sparse layout for real matrices
-// whose three sparsest columns touch at most 16 rows (close to an FP64-X
-// walk in cost).  0: the FP64-X / int32-X walk goes first (host checks only;
+// whose three sparsest columns touch so few rows R that its
+// (7 (6R + 9) + 6n + 5) / 8 FP64 operations per Gray step are no more than
+// the FP64-X walk's 2n (cfg-2-like matrices: n = 36, R = 6, 67 against 72).
+// 0: the FP64-X / int32-X walk goes first (host checks only;
 // policy_predicts_sdd may still choose split-dd for a real matrix).
 static int policy_first_kernel(const void* mat, int n, int dtype) {
   std::vector<double> a((size_t)n * n);
   for (size_t i = 0; i < a.size(); i++) a[i] = elem(mat, dtype, i);
   if (int_group_size(a, n) > 0) return PERM_KERNEL_DENSE_INT_DD;
   int c3[3];
-  if (split_rows_ok(a, n) && sdd_inner_rows(a, n, c3) > 0) return PERM_KERNEL_DENSE_SDD;
+  if (!split_rows_ok(a, n)) return 0;
+  const int r = sdd_inner_rows(a, n, c3);
+  if (r > 0 && 7 * (6 * r + 9) + 6 * n + 5 <= 16 * n) return PERM_KERNEL_DENSE_SDD;
   return 0;
 }
 

@@ -106,7 +106,9 @@ def test_sdd_dense_vs_oracle_dd(engine, orc, pb, n):
 def test_sdd_sparse_layout_vs_oracle_dd(engine, orc, pb, n, d):
     """Sparse real matrices: the layout that walks only the rows of the three
     sparsest columns at seven of eight steps, against the CPU double-double
-    Ryser; the automatic path (dense and CRS/CCS entry points) runs it first."""
+    Ryser; the automatic path (dense and CRS/CCS entry points) runs it first
+    where its FP64 operations per Gray step are no more than FP64 X's, and
+    meets 1e-10 either way."""
     rng = np.random.default_rng(900 + n)
     # a Bernoulli pattern plus a random permutation: a perfect matching exists,
     # so the permanent is positive and the relative bound is meaningful
@@ -122,7 +124,13 @@ def test_sdd_sparse_layout_vs_oracle_dd(engine, orc, pb, n, d):
     assert ok, info
     assert r.rel_error_estimate <= TOL
     a = engine.exact_dense(A)
-    assert a.kernel == pb.PERM_KERNEL_DENSE_SDD and a.value == r.value
+    if 7 * (6 * inner + 9) + 6 * n + 5 <= 16 * n:
+        assert engine.dense_plan(A)[0] == pb.PERM_KERNEL_DENSE_SDD
+    if a.kernel == pb.PERM_KERNEL_DENSE_SDD:
+        assert a.value == r.value
+    else:
+        assert a.kernel == pb.PERM_KERNEL_DENSE
+    assert a.rel_error_estimate <= TOL and rel_err(a.value, want) <= TOL
     s = engine.exact_sparse_matrix(A)
     assert s.kernel in (pb.PERM_KERNEL_DENSE_SDD, pb.PERM_KERNEL_SKIPPER)
     assert rel_err(s.value, want) < TOL

@@ -132,7 +132,7 @@ def test_sdd_sparse_layout_vs_oracle_dd(engine, orc, pb, n, d):
         assert a.kernel == pb.PERM_KERNEL_DENSE
     assert a.rel_error_estimate <= TOL and rel_err(a.value, want) <= TOL
     s = engine.exact_sparse_matrix(A)
-    assert s.kernel in (pb.PERM_KERNEL_DENSE_SDD, pb.PERM_KERNEL_SKIPPER)
+    assert s.kernel in (pb.PERM_KERNEL_DENSE, pb.PERM_KERNEL_DENSE_SDD, pb.PERM_KERNEL_SKIPPER)
     assert rel_err(s.value, want) < TOL
 
 

@@ -608,11 +608,12 @@ static int int_group_size(const std::vector<double>& a, int n) {
 // Layout of the certified int32-X walk (ryser_dense_intc.cuh): product
 // groups of G rows (each |product| < 2^31) whose values enter a
 // double-double product, optionally (*pair, orders >= 16, G >= 4) first
-// multiplied in consecutive pairs in FP64, exact when every run of 2G rows
-// has prod(sum_k |a_jk|) < 2^53.  The integer multiplies and conversions
-// cost n per Gray step whatever G is; the FP64 part costs 3 F - 4 operations
-// for F double-double factors plus one per exact pair, so the layout with
-// the fewest of those is taken.  Returns G, or 0 when int32 X does not apply.
+// multiplied in consecutive pairs in int64, exact when every run of 2G rows
+// has prod(sum_k |a_jk|) < 2^53.  Per Gray step a chain of g groups costs
+// n - g int32 multiplies, g conversions and 3g - 4 double-double operations;
+// pairs cost n - g multiplies, floor(g/2) 64-bit multiplies, f = ceil(g/2)
+// conversions and 3f - 4 operations; the layout with the fewest instructions
+// is taken.  Returns G, or 0 when int32 X does not apply.
 static int intc_layout(const std::vector<double>& a, int n, int* pair) {
   *pair = 0;
   if (n < 8) return 0;
@@ -622,10 +623,10 @@ static int intc_layout(const std::vector<double>& a, int n, int* pair) {
   for (int G = 6; G >= 3; G--) {
     if (!runs_fit(rowabs, n, G, 2147483648.0)) continue;
     const int ng = (n + G - 1) / G;
-    const int chain = 3 * ng - 4;
+    const int chain = n + 3 * ng - 4;
     if (chain < best_cost) best_g = G, best_pair = 0, best_cost = chain;
     if (n >= 16 && G >= 4 && runs_fit(rowabs, n, 2 * G, 9007199254740992.0)) {
-      const int nf = (ng + 1) / 2, paired = ng / 2 + 3 * nf - 4;
+      const int nf = (ng + 1) / 2, paired = n - ng + ng / 2 + 4 * nf - 4;
       if (paired < best_cost) best_g = G, best_pair = 1, best_cost = paired;
     }
   }

@@ -13,11 +13,13 @@
 //    first two by TwoProd (h = v0 v1, l = fma(v0, v1, -h), exact), every
 //    further value by h' = h v, l' = fma(l, v, fma(h, v, -h')) (3
 //    operations, relative error a few u^2);
-//  * with kPair, consecutive group values are first multiplied in FP64,
+//  * with kPair, consecutive int32 group products are first multiplied
+//    into one int64 (a 32 x 32 -> 64-bit multiply) and converted once,
 //    which is exact because the host proved every pair's |product| < 2^53:
-//    one multiply replaces a 3-operation double-double step (order 40,
-//    groups of 4 rows: 16 FP64 operations per term instead of 20 with
-//    groups of 5, measured 3.4% faster: 2534 against 2624 ms);
+//    a multiply and a conversion replace a 3-operation double-double step
+//    and a conversion (order 40, groups of 4 rows: 2446 ms against 2624 ms
+//    for groups of 5 in one chain; pairs multiplied in FP64 after two
+//    conversions: 2542 ms);
 //  * every signed term is added to the thread's total with TwoSum into a
 //    (hi, lo) pair whose low part collects every rounding error (Sum2 of
 //    Ogita, Rump and Oishi);
@@ -68,27 +70,34 @@ __device__ __forceinline__ void iupdate(int (&y)[N], const int* col, int s) {
   }
 }
 
-// Exact value of group g: the uint32 product of y over rows [gG, gG + G)
-// (the host proved |product| < 2^31), converted exactly to FP64.
+// Exact int32 product of y over the rows of group g (the host proved
+// |product| < 2^31; the uint32 product wraps to the right two's complement).
 template <int N, int G>
-__device__ __forceinline__ double group_value(const int (&y)[N], int g) {
+__device__ __forceinline__ int group_int(const int (&y)[N], int g) {
   const int j0 = g * G;
   uint32_t pr = (uint32_t)y[j0];
 #pragma unroll
   for (int t = 1; t < G; t++)
     if (j0 + t < N) pr = pr * (uint32_t)y[j0 + t];
-  return __int2double_rn((int)pr);
+  return (int)pr;
+}
+
+// Exact value of group g converted to FP64.
+template <int N, int G>
+__device__ __forceinline__ double group_value(const int (&y)[N], int g) {
+  return __int2double_rn(group_int<N, G>(y, g));
 }
 
 // Factor i of the double-double product: group value i, or with kPair the
-// exact FP64 product of group values 2i and 2i + 1 (the last one alone when
-// the number of groups is odd).
+// int64 product of groups 2i and 2i + 1 (the last group alone when the
+// number of groups is odd) converted exactly (|product| < 2^53).
 template <int N, int G, bool kPair>
 __device__ __forceinline__ double term_factor(const int (&y)[N], int i) {
   constexpr int NG = (N + G - 1) / G;
   if (!kPair) return group_value<N, G>(y, i);
-  const double a = group_value<N, G>(y, 2 * i);
-  return (2 * i + 1 < NG) ? __dmul_rn(a, group_value<N, G>(y, 2 * i + 1)) : a;
+  long long v = group_int<N, G>(y, 2 * i);
+  if (2 * i + 1 < NG) v *= group_int<N, G>(y, 2 * i + 1);
+  return __ll2double_rn(v);
 }
 
 // Double-double product of the factors (an unevaluated pair), each

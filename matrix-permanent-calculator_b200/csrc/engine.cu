@@ -1272,16 +1272,15 @@ static bool has_perfect_matching(const void* mat, int n, int dtype) {
 //     changes every product's significand, even for symmetric or constant
 //     matrices, so B's roundings are independent of A's.  Keep when
 //     max(independent-rounding estimate, 16 |perm(A) - perm(B)/3| / |perm(A)|)
-//     meets the target (B walked with split X when the FP64-X bound is far
-//     above the target);
-//  4. the same cross-check with the split-X kernel on A and B (orders 4..40,
-//     after an FP64-X first pass), whose per-term roundings are independent;
-//  5. otherwise recompute with a certified walk: int32 X with double-double
+//     meets the target;
+//  4. otherwise recompute with a certified walk: int32 X with double-double
 //     products for integer matrices (orders 8..64), split-dd for the rest
 //     (orders 4..40), double-double where neither applies (orders <= 40).
-// Steps 3 and 4 are skipped when their independent-rounding estimate alone
-// misses the target, and after an int32-X first pass (its certified twin
-// costs about 1.2 walks, less than a failed cross-check plus the rerun).
+// Step 3 is skipped when its independent-rounding estimate alone misses the
+// target, after an int32-X first pass (its certified twin costs about 1.2
+// walks, less than a failed cross-check plus the rerun), and when split-dd
+// applies and the FP64-X bound is above 4x the target (the cross-check
+// rarely passes there).
 // A certified walk (int32 X with dd products, split-dd) is its own estimate:
 // its bound uses the exact sum |term| the walk accumulated.
 // Context lock held.

@@ -881,6 +881,24 @@ def secondary(pb, eng):
                                        "rasmussen_mean": e.mean, "rasmussen_rel_se": e.std_error / e.mean,
                                        "scaling_ms": f.kernel_ms, "scaling_call_s": f_wall, "scaling_mean": f.mean,
                                        "scaling_rel_se": f.std_error / f.mean}
+    # the accuracy policy on the request loop's real matrices (density 0.5,
+    # U(0,1]): the kernel it plans from the device prediction of the FP64-X
+    # bound, that prediction against the FP64-X walk's own bound, and the
+    # policy's device time in FP64-X walks
+    rng = np.random.default_rng(5555)
+    pol = {}
+    for n in (28, 30, 32, 34):
+        A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+        kern, predicted = eng.dense_plan(A)
+        f = eng.exact_dense(A, variant=pb.PERM_KERNEL_DENSE)
+        eng.exact_dense(A)
+        r = eng.exact_dense(A)
+        pol[f"n{n}"] = {"planned_kernel": kern, "predicted_fp64_bound": predicted,
+                        "fp64_walk_bound": f.rel_error_estimate, "fp64_walk_ms": f.kernel_ms,
+                        "policy_kernel": r.kernel, "policy_ms": r.kernel_ms,
+                        "policy_in_fp64_walks": r.kernel_ms / f.kernel_ms,
+                        "policy_rel_error_estimate": r.rel_error_estimate}
+    out["policy_real_dense_d050"] = pol
     return out
 
 

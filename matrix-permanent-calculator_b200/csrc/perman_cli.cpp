@@ -77,9 +77,11 @@ int die(perm_ctx* ctx, int rc) {
   return 3;
 }
 
-// Multi-GPU exact dense: one host thread and context per device, shards of
-// the Gray range, double-double sum of the per-device results.
-int multi_gpu_dense(const std::vector<double>& a, int n, int gpus, perm_result* total) {
+// Multi-GPU exact: one host thread and context per device, shards of the
+// Gray range walked by `variant` (0: the engine's choice per shard), double-
+// double sum of the per-device results.  Evaluates once, like the
+// reference's multi-GPU ids (no error estimate on the sum).
+int multi_gpu_dense(const std::vector<double>& a, int n, int gpus, int variant, perm_result* total) {
   int avail = perm_device_count();
   if (avail < 1) {
     fprintf(stderr, "perman: no CUDA device\n");
@@ -95,7 +97,7 @@ int multi_gpu_dense(const std::vector<double>& a, int n, int gpus, perm_result* 
       perm_ctx* ctx = nullptr;
       rcs[g] = perm_ctx_create(g, &ctx);
       if (rcs[g] == PERM_OK) {
-        rcs[g] = perm_exact_dense_shard(ctx, a.data(), n, PERM_F64, g, gpus, &parts[g]);
+        rcs[g] = perm_exact_dense_ex(ctx, a.data(), n, PERM_F64, variant, g, gpus, &parts[g]);
         if (rcs[g] != PERM_OK) errs[g] = perm_ctx_last_error(ctx);
       }
       perm_ctx_destroy(ctx);
@@ -280,7 +282,7 @@ int main(int argc, char** argv) {
                              : "gpu_perman64_xshared_coalescing_mshared_multigpu_manual_distribution";
         perm_ctx_destroy(ctx);
         ctx = nullptr;
-        if (multi_gpu_dense(a, n, o.algo == 66 ? 4 : o.gpu_num, &r)) return 3;
+        if (multi_gpu_dense(a, n, o.algo == 66 ? 4 : o.gpu_num, 0, &r)) return 3;
         rc = PERM_OK;
       } else {
         printf("Unknown Algorithm ID\n");
@@ -300,14 +302,26 @@ int main(int argc, char** argv) {
       if ((o.algo >= 1 && o.algo <= 8) || o.algo == 66) {
         name = o.algo == 66 ? "gpu_perman64_xshared_coalescing_mshared_multigpu_sparse_manual_distribution"
                             : snames[o.algo];
-        // -p1..-p4 are the reference's CCS walks that touch only the flipped
-        // column's nonzeros (gpu_exact_sparse.cu:194-552): here the split-dd
-        // kernel, whose sparse layout walks only the rows of the three
-        // sparsest columns at seven of eight steps (orders 4..40); the other
-        // ids run the sparse dispatcher (SkipPer when most terms vanish)
-        const bool ccs_walk = o.algo >= 1 && o.algo <= 4 && perm_sdd_layout(a.data(), n) >= 0;
-        rc = perm_exact_sparse_ex(ctx, n, rptrs.data(), cols.data(), rvals.data(), cptrs.data(), rows.data(),
-                                  cvals.data(), ccs_walk ? PERM_KERNEL_DENSE_SDD : 0, &r);
+        // -p1..-p6 and -p66 are the reference's CCS walks that touch only the
+        // flipped column's nonzeros (gpu_exact_sparse.cu:194-552; -p5, -p6,
+        // -p66 on several devices, :823-1120): here the split-dd kernel,
+        // whose sparse layout walks only the rows of the three sparsest
+        // columns at seven of eight steps (orders 4..40), sharded over -d
+        // devices for the multi-GPU ids; -p7/-p8 and matrices outside the
+        // split-dd orders run the sparse dispatcher (SkipPer when most terms
+        // vanish)
+        const bool sdd = perm_sdd_layout(a.data(), n) >= 0;
+        const bool multi = o.algo == 5 || o.algo == 6 || o.algo == 66;
+        if (multi && sdd) {
+          perm_ctx_destroy(ctx);
+          ctx = nullptr;
+          if (multi_gpu_dense(a, n, o.algo == 66 ? 4 : o.gpu_num, PERM_KERNEL_DENSE_SDD, &r)) return 3;
+          rc = PERM_OK;
+        } else {
+          const bool ccs_walk = o.algo >= 1 && o.algo <= 4 && sdd;
+          rc = perm_exact_sparse_ex(ctx, n, rptrs.data(), cols.data(), rvals.data(), cptrs.data(), rows.data(),
+                                    cvals.data(), ccs_walk ? PERM_KERNEL_DENSE_SDD : 0, &r);
+        }
       } else {
         printf("Unknown Algorithm ID\n");
         perm_ctx_destroy(ctx);

@@ -116,15 +116,16 @@ def test_grid_mode_estimates_tilings(pb):
 
 @pytest.mark.gpu
 def test_sparse_ccs_ids_run_the_sparse_walk(pb, orc, tmp_path):
-    """-s -p1..-p4 (the reference's CCS walks) run the split-dd kernel, whose
-    sparse layout walks only the rows of the three sparsest columns; the
-    kernel that ran is named on its own line."""
+    """-s -p1..-p6 (the reference's CCS walks; -p5/-p6 on -d devices) run the
+    split-dd kernel, whose sparse layout walks only the rows of the three
+    sparsest columns (the multi-GPU ids as Gray-range shards, one per
+    device); the kernel that ran is named on its own line."""
     rng = np.random.default_rng(23)
     A = bernoulli(rng, 22, 0.2) * (1.0 - rng.random((22, 22)))
     p = tmp_path / "r.txt"
     write_matrix(p, A, "double")
     want = sum(orc.perm_dd(A))
-    for pid in ("-p1", "-p4"):
+    for pid in ("-p1", "-p4", "-p5", "-p6"):
         r = run(pb, "-f", p, "-s", pid)
         assert r.returncode == 0, r.stderr
         name, v = result_value(r.stdout)

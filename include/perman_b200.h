@@ -384,6 +384,18 @@ int perm_approx_rasmussen(perm_ctx* ctx, const void* mat, int n, int dtype, int6
 int perm_approx_scaling(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trials,
                         int scale_intervals, int scale_times, uint64_t seed, double* trial_values,
                         perm_estimate* out);
+/* Trials [trial0, trial0 + trials) of the same estimate (same streams): the
+ * multi-GPU split by trial id.  Ranges run on different devices give exactly
+ * the per-trial weights of the whole run; their (sum, sum_sq, zero_trials)
+ * add up to the whole run's.  Replaces the trial chunks that the
+ * reference's multi-GPU estimators hand to each device
+ * (gpu_perman64_rasmussen_multigpucpu_chunks, gpu_approximation_dense.cu:412;
+ * gpu_perman64_approximation_multigpucpu_chunks, :574). */
+int perm_approx_rasmussen_range(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trial0,
+                                int64_t trials, uint64_t seed, double* trial_values, perm_estimate* out);
+int perm_approx_scaling_range(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trial0,
+                              int64_t trials, int scale_intervals, int scale_times, uint64_t seed,
+                              double* trial_values, perm_estimate* out);
 /* Sparse forms take the CRS of the pattern (columns ascending within a row),
  * orders 1..2047 (the reference's sparse kernels stop at 672); above 64 they
  * run a bitset kernel with the same streams and arithmetic, and the CCS

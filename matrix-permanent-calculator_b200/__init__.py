@@ -17,6 +17,7 @@ on ``T``.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 from dataclasses import dataclass
 from pathlib import Path
@@ -46,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_intc_layout", "perm_exact_dense_plan", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
     "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune", "perm_batch_variant", "perm_batch_use_variant",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
-    "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_sparse",
+    "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_range", "perm_approx_scaling_range", "perm_approx_rasmussen_sparse",
     "perm_approx_scaling_sparse", "perm_read_matrix", "perm_compress", "perm_grid_graph", "perm_fp64_peak",
     "gpu_perman64_xshared_coalescing_mshared_int", "gpu_perman64_xshared_coalescing_mshared_float",
     "gpu_perman64_xshared_coalescing_mshared_double",
@@ -132,6 +133,8 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_exact_dense_tc_rounds": (i, [_P, _P, i, i, u64, u64, ctypes.POINTER(PermResult)]),
         "perm_approx_rasmussen": (i, [_P, _P, i, i, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
         "perm_approx_scaling": (i, [_P, _P, i, i, i64, i, i, u64, _P, ctypes.POINTER(PermEstimate)]),
+        "perm_approx_rasmussen_range": (i, [_P, _P, i, i, i64, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
+        "perm_approx_scaling_range": (i, [_P, _P, i, i, i64, i64, i, i, u64, _P, ctypes.POINTER(PermEstimate)]),
         "perm_approx_rasmussen_sparse": (i, [_P, i, _P, _P, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
         "perm_approx_scaling_sparse": (i, [_P, i, _P, _P, _P, _P, i64, i, i, u64, _P,
                                            ctypes.POINTER(PermEstimate)]),
@@ -206,6 +209,8 @@ class Estimate:
     zero_trials: float
     kernel_ms: float
     trial_values: np.ndarray | None = None
+    sum: float = 0.0      # sum of the trial weights (mean = sum / trials)
+    sum_sq: float = 0.0   # sum of their squares
 
 
 def _exact(r: PermResult) -> ExactResult:
@@ -323,23 +328,36 @@ class Engine:
 
     # ---- Monte Carlo ----
     def _estimate(self, e: PermEstimate, tv) -> Estimate:
-        return Estimate(e.mean, e.std_error, e.trials, e.zero_trials, e.kernel_ms, tv)
+        return Estimate(e.mean, e.std_error, e.trials, e.zero_trials, e.kernel_ms, tv, e.sum, e.sum_sq)
 
-    def rasmussen(self, mat, trials: int, seed: int = 1, keep_trials: bool = False) -> Estimate:
+    def rasmussen(self, mat, trials: int, seed: int = 1, keep_trials: bool = False, trial0: int = 0) -> Estimate:
+        """Rasmussen estimate over trials [trial0, trial0 + trials) of the
+        streams keyed by `seed` (trial0 > 0: perm_approx_rasmussen_range)."""
         a, dt = _as_matrix(mat)
         tv = np.empty(trials, dtype=np.float64) if keep_trials else None
         e = PermEstimate()
-        self._check(self.lib.perm_approx_rasmussen(self.ctx, _ptr(a), a.shape[0], dt, trials, seed, _ptr(tv),
-                                                   ctypes.byref(e)))
+        if trial0:
+            self._check(self.lib.perm_approx_rasmussen_range(self.ctx, _ptr(a), a.shape[0], dt, trial0, trials, seed,
+                                                             _ptr(tv), ctypes.byref(e)))
+        else:
+            self._check(self.lib.perm_approx_rasmussen(self.ctx, _ptr(a), a.shape[0], dt, trials, seed, _ptr(tv),
+                                                       ctypes.byref(e)))
         return self._estimate(e, tv)
 
     def scaling(self, mat, trials: int, scale_intervals: int = 4, scale_times: int = 5, seed: int = 1,
-                keep_trials: bool = False) -> Estimate:
+                keep_trials: bool = False, trial0: int = 0) -> Estimate:
+        """Sinkhorn-scaled estimate over trials [trial0, trial0 + trials)
+        (trial0 > 0: perm_approx_scaling_range)."""
         a, dt = _as_matrix(mat)
         tv = np.empty(trials, dtype=np.float64) if keep_trials else None
         e = PermEstimate()
-        self._check(self.lib.perm_approx_scaling(self.ctx, _ptr(a), a.shape[0], dt, trials, scale_intervals,
-                                                 scale_times, seed, _ptr(tv), ctypes.byref(e)))
+        if trial0:
+            self._check(self.lib.perm_approx_scaling_range(self.ctx, _ptr(a), a.shape[0], dt, trial0, trials,
+                                                           scale_intervals, scale_times, seed, _ptr(tv),
+                                                           ctypes.byref(e)))
+        else:
+            self._check(self.lib.perm_approx_scaling(self.ctx, _ptr(a), a.shape[0], dt, trials, scale_intervals,
+                                                     scale_times, seed, _ptr(tv), ctypes.byref(e)))
         return self._estimate(e, tv)
 
     def rasmussen_sparse(self, n, rptrs, cols, trials, seed=1, keep_trials=False) -> Estimate:
@@ -701,6 +719,110 @@ def distributed_exact_dense_dynamic(mat, chunks: int | None = None, group=None, 
     if not bool((table[:, 0] == 1.0).all()):
         raise PermError(PERM_EINVAL, "chunk queue: a chunk was not computed exactly once")
     return dd_sum((float(table[c, 1]), float(table[c, 2])) for c in range(chunks))
+
+
+def _gather_rows(row, group):
+    """All-gather of one float64 row per rank (rank order), on the device for
+    NCCL groups and on the host for gloo."""
+    import torch
+    import torch.distributed as dist
+
+    backend = dist.get_backend(group)
+    dev = f"cuda:{torch.cuda.current_device()}" if backend == "nccl" else "cpu"
+    t = torch.tensor(row, dtype=torch.float64, device=dev)
+    out = [torch.zeros_like(t) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(out, t, group=group)
+    return [g.cpu().numpy() for g in out]
+
+
+def distributed_estimate(mat, trials: int, method: str = "rasmussen", scale_intervals: int = 4,
+                         scale_times: int = 5, seed: int = 1, group=None, engine: Engine | None = None,
+                         range_fn=None) -> Estimate:
+    """Monte-Carlo estimate of one matrix over all ranks of a torch.distributed
+    group, split by trial id (the reference's multi-GPU estimators,
+    gpu_approximation_dense.cu:412, 574, with static ranges instead of its
+    chunk queue: trials cost alike).
+
+    Rank r runs trials [r T / W, (r + 1) T / W) of the streams keyed by `seed`
+    (perm_approx_*_range), so the union of the ranks' trials is exactly the
+    single-device run's; one all-gather of (sum, sum of squares, zero trials,
+    device ms) per rank -- the only collective -- and every rank adds them in
+    rank order.  `range_fn(mat, trial0, count) -> (sum, sum_sq, zeros)`
+    replaces the device call (host-logic tests without a GPU)."""
+    import torch.distributed as dist
+
+    if trials < 1:
+        raise PermError(PERM_EINVAL, f"trials must be >= 1 (got {trials})")
+    if method not in ("rasmussen", "scaling"):
+        raise PermError(PERM_EINVAL, f"unknown estimator {method!r}")
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    t0, t1 = trials * rank // world, trials * (rank + 1) // world
+    row = [0.0, 0.0, 0.0, 0.0]
+    if t1 > t0:
+        if range_fn is not None:
+            s, s2, z = range_fn(mat, t0, t1 - t0)
+            row = [s, s2, z, 0.0]
+        else:
+            eng = engine or default_engine()
+            if method == "rasmussen":
+                e = eng.rasmussen(mat, t1 - t0, seed=seed, trial0=t0)
+            else:
+                e = eng.scaling(mat, t1 - t0, scale_intervals, scale_times, seed=seed, trial0=t0)
+            row = [e.sum, e.sum_sq, e.zero_trials, e.kernel_ms]
+    rows = _gather_rows(row, group)
+    s = s2 = z = 0.0
+    ms = 0.0
+    for g in rows:
+        s += float(g[0])
+        s2 += float(g[1])
+        z += float(g[2])
+        ms = max(ms, float(g[3]))
+    T = float(trials)
+    mean = s / T
+    var = (s2 - s * mean) / (T - 1) if T > 1 else 0.0
+    return Estimate(mean, math.sqrt(max(var, 0.0) / T), T, z, ms, None, s, s2)
+
+
+def batch_assignment(orders, world: int) -> list[int]:
+    """Owner rank of every matrix of a batch split over `world` ranks: longest
+    walk first to the least-loaded rank (cost 2^(n-1) Gray steps; ties to the
+    lower index and rank), the same on every rank."""
+    load = [0.0] * world
+    owner = [0] * len(orders)
+    for i in sorted(range(len(orders)), key=lambda i: (-int(orders[i]), i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += 2.0 ** (int(orders[i]) - 1)
+    return owner
+
+
+def distributed_batch_exact(mats, group=None, engine: Engine | None = None, batch_fn=None) -> np.ndarray:
+    """Exact permanents of a list of matrices over all ranks: each rank runs
+    one resident batch (perm_batch_*) of the matrices batch_assignment gives
+    it, and one all-reduce of a count x 2 table (owner flag, value; every row
+    written by exactly one rank, so the sum is exact) gives every rank all
+    values, in the caller's order.  `batch_fn(list_of_matrices) -> values`
+    replaces the device call (host-logic tests without a GPU)."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    orders = [np.asarray(m).shape[0] for m in mats]
+    owner = batch_assignment(orders, world)
+    mine = [i for i in range(len(mats)) if owner[i] == rank]
+    table = torch.zeros((len(mats), 2), dtype=torch.float64)
+    if mine:
+        sub = [mats[i] for i in mine]
+        vals = batch_fn(sub) if batch_fn is not None else (engine or default_engine()).batch_exact(sub)[0]
+        for i, v in zip(mine, vals):
+            table[i, 0], table[i, 1] = 1.0, float(v)
+    if dist.get_backend(group) == "nccl":
+        table = table.to(f"cuda:{torch.cuda.current_device()}")
+    dist.all_reduce(table, op=dist.ReduceOp.SUM, group=group)
+    table = table.cpu()
+    if not bool((table[:, 0] == 1.0).all()):
+        raise PermError(PERM_EINVAL, "batch split: a matrix was not computed exactly once")
+    return table[:, 1].numpy().copy()
 
 
 # ---- reference-named entry points (argument meaning as in the reference) ------

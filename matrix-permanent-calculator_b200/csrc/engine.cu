@@ -1819,7 +1819,7 @@ extern "C" int perm_exact_sparse(perm_ctx* ctx, int n, const int* rptrs, const i
 // ---------------------------------------------------------------------------
 static int mc_run(perm_ctx* ctx, const std::vector<uint64_t>& rowmask, const std::vector<double>* dense,
                   int n, bool scaling, int64_t trials, int y, int z, uint64_t seed, double* trial_values,
-                  perm_estimate* out) {
+                  perm_estimate* out, uint64_t trial0 = 0) {
   if (trials < 1) return fail(ctx, PERM_EINVAL, "trials must be >= 1 (got %lld)", (long long)trials);
   if (scaling && (y < 1 || z < 0)) return fail(ctx, PERM_EINVAL, "scale interval must be >= 1 and scale times >= 0");
   std::lock_guard<std::mutex> lock(ctx->mu);
@@ -1879,7 +1879,7 @@ static int mc_run(perm_ctx* ctx, const std::vector<uint64_t>& rowmask, const std
   }
   a.pack = ctx->d_stage;
   a.trials = trials;
-  a.trial0 = 0;
+  a.trial0 = trial0;
   a.seed = seed;
   a.trial_out = trial_values ? ctx->d_trials : nullptr;
   a.partials = reinterpret_cast<double*>(ctx->partials);
@@ -1912,7 +1912,7 @@ static int mc_run(perm_ctx* ctx, const std::vector<uint64_t>& rowmask, const std
 }
 
 static int mc_dense(perm_ctx* ctx, const void* mat, int n, int dtype, bool scaling, int64_t trials, int y,
-                    int z, uint64_t seed, double* tv, perm_estimate* out) {
+                    int z, uint64_t seed, double* tv, perm_estimate* out, uint64_t trial0 = 0) {
   if (!ctx) return PERM_EINVAL;
   if (!mat || !out) return fail(ctx, PERM_EINVAL, "null matrix or result pointer");
   if (n < 1 || n > PERM_MAX_MC_N) return fail(ctx, PERM_EUNSUPPORTED, "order %d outside [1, %d]", n, PERM_MAX_MC_N);
@@ -1925,7 +1925,7 @@ static int mc_dense(perm_ctx* ctx, const void* mat, int n, int dtype, bool scali
       dense[(size_t)i * n + j] = v;
       if (v != 0.0) mask[i] |= 1ull << j;
     }
-  return mc_run(ctx, mask, &dense, n, scaling, trials, y, z, seed, tv, out);
+  return mc_run(ctx, mask, &dense, n, scaling, trials, y, z, seed, tv, out, trial0);
 }
 
 // Orders above 64: bitset kernel on the packed CRS + CCS of the pattern.
@@ -2055,6 +2055,22 @@ extern "C" int perm_approx_rasmussen(perm_ctx* ctx, const void* mat, int n, int 
 extern "C" int perm_approx_scaling(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trials, int y,
                                    int z, uint64_t seed, double* tv, perm_estimate* out) {
   return mc_dense(ctx, mat, n, dtype, true, trials, y, z, seed, tv, out);
+}
+// Trials [trial0, trial0 + trials) of the same streams: ranges of one
+// estimate run on different devices give the per-trial weights of the whole
+// run (the estimators' multi-GPU split by trial id).
+extern "C" int perm_approx_rasmussen_range(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trial0,
+                                           int64_t trials, uint64_t seed, double* tv, perm_estimate* out) {
+  if (!ctx) return PERM_EINVAL;
+  if (trial0 < 0) return fail(ctx, PERM_EINVAL, "first trial must be >= 0 (got %lld)", (long long)trial0);
+  return mc_dense(ctx, mat, n, dtype, false, trials, 1, 0, seed, tv, out, (uint64_t)trial0);
+}
+extern "C" int perm_approx_scaling_range(perm_ctx* ctx, const void* mat, int n, int dtype, int64_t trial0,
+                                         int64_t trials, int y, int z, uint64_t seed, double* tv,
+                                         perm_estimate* out) {
+  if (!ctx) return PERM_EINVAL;
+  if (trial0 < 0) return fail(ctx, PERM_EINVAL, "first trial must be >= 0 (got %lld)", (long long)trial0);
+  return mc_dense(ctx, mat, n, dtype, true, trials, y, z, seed, tv, out, (uint64_t)trial0);
 }
 extern "C" int perm_approx_rasmussen_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
                                             int64_t trials, uint64_t seed, double* tv, perm_estimate* out) {

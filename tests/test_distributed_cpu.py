@@ -239,3 +239,78 @@ def test_bench_sharded_step_two_ranks(pb, orc, tmp_path):
         assert abs((r[0] + r[1]) - (r[2] + r[3])) <= 1e-12 * abs(r[2] + r[3])
         assert abs((r[0] + r[1]) - exact) <= 1e-12 * abs(exact)
     assert r0[0] == r1[0] and r0[1] == r1[1]
+
+
+def _rank_estimate_and_batch(rank, world, port, A, mats, out_path):
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    sys.path.insert(0, str(root / "tests"))
+    sys.path.insert(0, str(root / "oracle"))
+    import torch.distributed as dist
+    from conftest import load_package
+    from oracle import Oracle
+
+    pb = load_package()
+    orc = Oracle()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+
+    def ras_range(mat, t0, count):  # CPU stand-in for perm_approx_rasmussen_range
+        w = orc.rasmussen_trials(mat, 77, t0, count)
+        return float(w.sum()), float((w * w).sum()), float((w == 0).sum())
+
+    def sca_range(mat, t0, count):  # ... and perm_approx_scaling_range
+        w = orc.scaling_trials(mat, 3, 2, 77, t0, count)
+        return float(w.sum()), float((w * w).sum()), float((w == 0).sum())
+
+    e = pb.distributed_estimate(A, 1001, "rasmussen", seed=77, range_fn=ras_range)
+    f = pb.distributed_estimate(A, 301, "scaling", 3, 2, seed=77, range_fn=sca_range)
+    vals = pb.distributed_batch_exact(mats, batch_fn=lambda sub: [sum(orc.perm_dd(m)) for m in sub])
+    dist.barrier()
+    dist.destroy_process_group()
+    np.save(f"{out_path}.{rank}.npy", np.concatenate([[e.mean, e.std_error, e.zero_trials, f.mean, f.std_error],
+                                                      vals]))
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_estimates_and_batches_split_over_ranks(pb, orc, tmp_path, world):
+    """Monte Carlo split by trial id: the ranks' trials are exactly the
+    single-device run's (same Philox streams, the oracle standing in for the
+    device), so the combined mean and standard error equal the whole run's;
+    a batch split by walk length gives every rank every value, each computed
+    once, in the caller's order."""
+    rng = np.random.default_rng(11)
+    A = (rng.random((12, 12)) < 0.6).astype(np.float64)
+    mats = [rng.random((n, n)) for n in (4, 9, 7, 11, 5, 10, 8, 6)]
+    port = _free_port()
+    out = str(tmp_path / "mc")
+    mp.start_processes(_rank_estimate_and_batch, args=(world, port, A, mats, out), nprocs=world, join=True,
+                       start_method="spawn")
+    w = orc.rasmussen_trials(A, 77, 0, 1001)
+    v = orc.scaling_trials(A, 3, 2, 77, 0, 301)
+    se = lambda x: np.sqrt(((x * x).sum() - x.sum() * x.mean()) / (len(x) - 1) / len(x))
+    want_vals = [sum(orc.perm_dd(m)) for m in mats]
+    rows = [np.load(f"{out}.{r}.npy") for r in range(world)]
+    for r in rows:
+        assert abs(r[0] - w.mean()) <= 1e-13 * abs(w.mean())
+        assert abs(r[1] - se(w)) <= 1e-9 * se(w)
+        assert r[2] == (w == 0).sum()
+        assert abs(r[3] - v.mean()) <= 1e-13 * abs(v.mean())
+        assert abs(r[4] - se(v)) <= 1e-9 * se(v)
+        assert list(r[5:]) == want_vals
+    assert all((rows[0] == r).all() for r in rows)
+
+
+def test_batch_assignment_balances_walks(pb):
+    """Longest walk first to the least-loaded rank: deterministic, every
+    matrix owned once, loads within one largest walk of each other."""
+    rng = np.random.default_rng(3)
+    orders = rng.integers(12, 29, 500)
+    for world in (1, 2, 3, 8):
+        owner = pb.batch_assignment(orders, world)
+        assert owner == pb.batch_assignment(list(orders), world)
+        loads = [sum(2.0 ** (o - 1) for o, w in zip(orders, owner) if w == r) for r in range(world)]
+        assert max(loads) - min(loads) <= 2.0 ** (orders.max() - 1)

@@ -67,6 +67,22 @@ def test_streams_independent_of_trial_count(engine):
     np.testing.assert_array_equal(a, b[:1000])
 
 
+def test_trial_ranges_are_the_whole_runs_trials(engine):
+    """perm_approx_*_range: trials [t0, t0 + k) of the same streams give the
+    whole run's weights bit for bit, and ranges' sums add up to its sums
+    (the multi-GPU split by trial id)."""
+    rng = np.random.default_rng(8)
+    A = bernoulli(rng, 30, 0.5)
+    whole = engine.rasmussen(A, 3000, seed=4, keep_trials=True)
+    lo = engine.rasmussen(A, 1234, seed=4, keep_trials=True)
+    hi = engine.rasmussen(A, 1766, seed=4, keep_trials=True, trial0=1234)
+    np.testing.assert_array_equal(np.concatenate([lo.trial_values, hi.trial_values]), whole.trial_values)
+    assert abs((lo.sum + hi.sum) - whole.sum) <= 1e-13 * abs(whole.sum)
+    s_whole = engine.scaling(A, 600, 4, 5, seed=6, keep_trials=True)
+    s_hi = engine.scaling(A, 250, 4, 5, seed=6, keep_trials=True, trial0=350)
+    np.testing.assert_array_equal(s_hi.trial_values, s_whole.trial_values[350:])
+
+
 def test_sparse_equals_dense_pattern(engine, pb):
     rng = np.random.default_rng(8)
     A = bernoulli(rng, 24, 0.4)

@@ -407,6 +407,14 @@ int perm_approx_scaling_sparse(perm_ctx* ctx, int n, const int* rptrs, const int
                                const int* cptrs, const int* rows, int64_t trials,
                                int scale_intervals, int scale_times, uint64_t seed,
                                double* trial_values, perm_estimate* out);
+/* Trial ranges of the sparse forms (as perm_approx_*_range; the scaling
+ * form rebuilds its CCS from the CRS). */
+int perm_approx_rasmussen_sparse_range(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
+                                       int64_t trial0, int64_t trials, uint64_t seed, double* trial_values,
+                                       perm_estimate* out);
+int perm_approx_scaling_sparse_range(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
+                                     int64_t trial0, int64_t trials, int scale_intervals, int scale_times,
+                                     uint64_t seed, double* trial_values, perm_estimate* out);
 
 /* ---- matrix input (host only; no device needed) ------------------------------ */
 /* The reference's grid-graph input mode (util.h:403-520): the dense 0/1

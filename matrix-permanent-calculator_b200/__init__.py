@@ -47,7 +47,8 @@ EXPORTED_SYMBOLS = (
     "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_intc_layout", "perm_exact_dense_plan", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
     "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune", "perm_batch_variant", "perm_batch_use_variant",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
-    "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_range", "perm_approx_scaling_range", "perm_approx_rasmussen_sparse",
+    "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_range", "perm_approx_scaling_range",
+    "perm_approx_rasmussen_sparse_range", "perm_approx_scaling_sparse_range", "perm_approx_rasmussen_sparse",
     "perm_approx_scaling_sparse", "perm_read_matrix", "perm_compress", "perm_grid_graph", "perm_fp64_peak",
     "gpu_perman64_xshared_coalescing_mshared_int", "gpu_perman64_xshared_coalescing_mshared_float",
     "gpu_perman64_xshared_coalescing_mshared_double",
@@ -135,6 +136,9 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_approx_scaling": (i, [_P, _P, i, i, i64, i, i, u64, _P, ctypes.POINTER(PermEstimate)]),
         "perm_approx_rasmussen_range": (i, [_P, _P, i, i, i64, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
         "perm_approx_scaling_range": (i, [_P, _P, i, i, i64, i64, i, i, u64, _P, ctypes.POINTER(PermEstimate)]),
+        "perm_approx_rasmussen_sparse_range": (i, [_P, i, _P, _P, i64, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
+        "perm_approx_scaling_sparse_range": (i, [_P, i, _P, _P, i64, i64, i, i, u64, _P,
+                                                 ctypes.POINTER(PermEstimate)]),
         "perm_approx_rasmussen_sparse": (i, [_P, i, _P, _P, i64, u64, _P, ctypes.POINTER(PermEstimate)]),
         "perm_approx_scaling_sparse": (i, [_P, i, _P, _P, _P, _P, i64, i, i, u64, _P,
                                            ctypes.POINTER(PermEstimate)]),
@@ -360,22 +364,31 @@ class Engine:
                                                      scale_times, seed, _ptr(tv), ctypes.byref(e)))
         return self._estimate(e, tv)
 
-    def rasmussen_sparse(self, n, rptrs, cols, trials, seed=1, keep_trials=False) -> Estimate:
+    def rasmussen_sparse(self, n, rptrs, cols, trials, seed=1, keep_trials=False, trial0: int = 0) -> Estimate:
         rp = np.ascontiguousarray(rptrs, dtype=np.int32)
         cl = np.ascontiguousarray(cols, dtype=np.int32)
         tv = np.empty(trials, dtype=np.float64) if keep_trials else None
         e = PermEstimate()
-        self._check(self.lib.perm_approx_rasmussen_sparse(self.ctx, n, _ptr(rp), _ptr(cl), trials, seed,
-                                                          _ptr(tv), ctypes.byref(e)))
+        if trial0:
+            self._check(self.lib.perm_approx_rasmussen_sparse_range(self.ctx, n, _ptr(rp), _ptr(cl), trial0, trials,
+                                                                    seed, _ptr(tv), ctypes.byref(e)))
+        else:
+            self._check(self.lib.perm_approx_rasmussen_sparse(self.ctx, n, _ptr(rp), _ptr(cl), trials, seed,
+                                                              _ptr(tv), ctypes.byref(e)))
         return self._estimate(e, tv)
 
     def scaling_sparse(self, n, rptrs, cols, cptrs, rows, trials, scale_intervals=4, scale_times=5, seed=1,
-                       keep_trials=False) -> Estimate:
+                       keep_trials=False, trial0: int = 0) -> Estimate:
         arrs = [np.ascontiguousarray(x, dtype=np.int32) for x in (rptrs, cols, cptrs, rows)]
         tv = np.empty(trials, dtype=np.float64) if keep_trials else None
         e = PermEstimate()
-        self._check(self.lib.perm_approx_scaling_sparse(self.ctx, n, *map(_ptr, arrs), trials, scale_intervals,
-                                                        scale_times, seed, _ptr(tv), ctypes.byref(e)))
+        if trial0:
+            self._check(self.lib.perm_approx_scaling_sparse_range(self.ctx, n, _ptr(arrs[0]), _ptr(arrs[1]), trial0,
+                                                                  trials, scale_intervals, scale_times, seed,
+                                                                  _ptr(tv), ctypes.byref(e)))
+        else:
+            self._check(self.lib.perm_approx_scaling_sparse(self.ctx, n, *map(_ptr, arrs), trials, scale_intervals,
+                                                            scale_times, seed, _ptr(tv), ctypes.byref(e)))
         return self._estimate(e, tv)
 
     # ---- batches ----

@@ -1930,7 +1930,7 @@ static int mc_dense(perm_ctx* ctx, const void* mat, int n, int dtype, bool scali
 
 // Orders above 64: bitset kernel on the packed CRS + CCS of the pattern.
 static int mc_sparse_large(perm_ctx* ctx, int n, const int* rptrs, const int* cols, bool scaling, int64_t trials,
-                           int y, int z, uint64_t seed, double* tv, perm_estimate* out) {
+                           int y, int z, uint64_t seed, double* tv, perm_estimate* out, uint64_t trial0 = 0) {
   if (trials < 1) return fail(ctx, PERM_EINVAL, "trials must be >= 1 (got %lld)", (long long)trials);
   if (scaling && (y < 1 || z < 0)) return fail(ctx, PERM_EINVAL, "scale interval must be >= 1 and scale times >= 0");
   const int nnz = rptrs[n];
@@ -1978,7 +1978,7 @@ static int mc_sparse_large(perm_ctx* ctx, int n, const int* rptrs, const int* co
   }
   a.pack = ctx->d_stage;
   a.trials = trials;
-  a.trial0 = 0;
+  a.trial0 = trial0;
   a.seed = seed;
   a.trial_out = tv ? ctx->d_trials : nullptr;
   a.partials = reinterpret_cast<double*>(ctx->partials);
@@ -2009,7 +2009,7 @@ static int mc_sparse_large(perm_ctx* ctx, int n, const int* rptrs, const int* co
 }
 
 static int mc_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols, bool scaling, int64_t trials,
-                     int y, int z, uint64_t seed, double* tv, perm_estimate* out) {
+                     int y, int z, uint64_t seed, double* tv, perm_estimate* out, uint64_t trial0 = 0) {
   if (!ctx) return PERM_EINVAL;
   if (!rptrs || !cols || !out) return fail(ctx, PERM_EINVAL, "null CRS or result pointer");
   if (n < 1 || n > kMcSparseMaxOrder)
@@ -2022,7 +2022,7 @@ static int mc_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols, bo
       if (p > rptrs[i] && cols[p] <= cols[p - 1]) return fail(ctx, PERM_EINVAL, "CRS columns must ascend within a row");
     }
   }
-  if (n > PERM_MAX_MC_N) return mc_sparse_large(ctx, n, rptrs, cols, scaling, trials, y, z, seed, tv, out);
+  if (n > PERM_MAX_MC_N) return mc_sparse_large(ctx, n, rptrs, cols, scaling, trials, y, z, seed, tv, out, trial0);
   std::vector<uint64_t> mask(n, 0);
   std::vector<double> pattern((size_t)n * n, 0.0);
   for (int i = 0; i < n; i++)
@@ -2030,7 +2030,7 @@ static int mc_sparse(perm_ctx* ctx, int n, const int* rptrs, const int* cols, bo
       mask[i] |= 1ull << cols[p];
       pattern[(size_t)i * n + cols[p]] = 1.0;  // the sparse estimators use the pattern only
     }
-  return mc_run(ctx, mask, &pattern, n, scaling, trials, y, z, seed, tv, out);
+  return mc_run(ctx, mask, &pattern, n, scaling, trials, y, z, seed, tv, out, trial0);
 }
 
 // Grid-graph input (util.h:403-520): dense 0/1 matrix of an m x n board.
@@ -2082,6 +2082,20 @@ extern "C" int perm_approx_scaling_sparse(perm_ctx* ctx, int n, const int* rptrs
   (void)cptrs;
   (void)rows;
   return mc_sparse(ctx, n, rptrs, cols, true, trials, y, z, seed, tv, out);
+}
+extern "C" int perm_approx_rasmussen_sparse_range(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
+                                                  int64_t trial0, int64_t trials, uint64_t seed, double* tv,
+                                                  perm_estimate* out) {
+  if (!ctx) return PERM_EINVAL;
+  if (trial0 < 0) return fail(ctx, PERM_EINVAL, "first trial must be >= 0 (got %lld)", (long long)trial0);
+  return mc_sparse(ctx, n, rptrs, cols, false, trials, 1, 0, seed, tv, out, (uint64_t)trial0);
+}
+extern "C" int perm_approx_scaling_sparse_range(perm_ctx* ctx, int n, const int* rptrs, const int* cols,
+                                                int64_t trial0, int64_t trials, int y, int z, uint64_t seed,
+                                                double* tv, perm_estimate* out) {
+  if (!ctx) return PERM_EINVAL;
+  if (trial0 < 0) return fail(ctx, PERM_EINVAL, "first trial must be >= 0 (got %lld)", (long long)trial0);
+  return mc_sparse(ctx, n, rptrs, cols, true, trials, y, z, seed, tv, out, (uint64_t)trial0);
 }
 
 // ---------------------------------------------------------------------------

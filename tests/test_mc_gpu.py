@@ -67,7 +67,7 @@ def test_streams_independent_of_trial_count(engine):
     np.testing.assert_array_equal(a, b[:1000])
 
 
-def test_trial_ranges_are_the_whole_runs_trials(engine):
+def test_trial_ranges_are_the_whole_runs_trials(engine, pb):
     """perm_approx_*_range: trials [t0, t0 + k) of the same streams give the
     whole run's weights bit for bit, and ranges' sums add up to its sums
     (the multi-GPU split by trial id)."""
@@ -81,6 +81,18 @@ def test_trial_ranges_are_the_whole_runs_trials(engine):
     s_whole = engine.scaling(A, 600, 4, 5, seed=6, keep_trials=True)
     s_hi = engine.scaling(A, 250, 4, 5, seed=6, keep_trials=True, trial0=350)
     np.testing.assert_array_equal(s_hi.trial_values, s_whole.trial_values[350:])
+    # the sparse forms: below and above order 64 (bitset kernel)
+    for n in (30, 100):
+        B = bernoulli(rng, n, 0.3 if n == 30 else 0.05)
+        c = pb.compress(0, B)
+        w = engine.rasmussen_sparse(n, c["rptrs"], c["cols"], 900, seed=2, keep_trials=True)
+        h = engine.rasmussen_sparse(n, c["rptrs"], c["cols"], 400, seed=2, keep_trials=True, trial0=500)
+        np.testing.assert_array_equal(h.trial_values, w.trial_values[500:])
+        sw = engine.scaling_sparse(n, c["rptrs"], c["cols"], c["cptrs"], c["rows"], 300, 4, 5, seed=3,
+                                   keep_trials=True)
+        sh = engine.scaling_sparse(n, c["rptrs"], c["cols"], c["cptrs"], c["rows"], 100, 4, 5, seed=3,
+                                   keep_trials=True, trial0=200)
+        np.testing.assert_array_equal(sh.trial_values, sw.trial_values[200:])
 
 
 def test_sparse_equals_dense_pattern(engine, pb):

@@ -186,7 +186,7 @@ def run_reference_arm(args):
 # a recorded ncu count is only valid for the same template instance compiled
 # from the same text.
 KERNEL_SOURCES = {
-    "int32x": ["ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
+    "int32x": ["ryser_dense_int_sparse.cuh", "ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
     "fp64x": ["ryser_dense.cuh", "perman_common.cuh"],
     "int32x_dd": ["ryser_dense_intc.cuh", "ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
 }
@@ -202,23 +202,11 @@ def source_sha16(kname: str) -> str | None:
     return h.hexdigest()[:16]
 
 
-def int_group_size(A: np.ndarray) -> int:
-    """The int32-X kernels' product-group size for an integer matrix: the
-    largest G in {6,5,4,3} with prod(row absolute sums) < 2^31 over every run
-    of G consecutive rows (the engine's own rule, restated to name the
-    template instance that runs)."""
-    n = A.shape[0]
-    rows = np.maximum(np.abs(A).sum(axis=1).astype(float), 1.0)
-    for g in (6, 5, 4, 3):
-        if all(np.prod(rows[j:j + g]) < 2.0 ** 31 for j in range(0, n, g)):
-            return g
-    return 0
-
-
 def kernel_template(kname: str, A: np.ndarray) -> str:
     n = A.shape[0]
     if kname == "int32x":
-        return f"ryser_dense_int_kernel<{n}, {int_group_size(A)}>"
+        g, ngo = (sys.modules.get("perman_b200") or load_pkg()).int_layout(A)
+        return f"ryser_dense_int_sparse_kernel<{n}, {g}, {ngo}>" if ngo else f"ryser_dense_int_kernel<{n}, {g}>"
     if kname == "int32x_dd":
         # product groups and pairing as the engine lays them out; last template
         # argument: CTAs per SM compiled for (3 up to order 36, 2 above)
@@ -500,6 +488,8 @@ def main():
     line["config"]["kernel"] = {1: "FP64-X register kernel", 3: "int32-X register kernel",
                                 5: "tensor-core row sums (tcgen05 kind::i8) + int32 products",
                                 7: "int32-X register kernel, double-double products and sum"}.get(r.kernel, r.kernel)
+    if r.kernel == pb.PERM_KERNEL_DENSE_INT:
+        line["config"]["kernel_instance"] = kernel_template("int32x", A)
     if rank == 0 and not args.no_secondary:
         line["secondary"] = secondary(pb, eng)
         # the same n=40 matrix through the int32-X and tensor-core kernels

@@ -219,6 +219,16 @@ int perm_ctx_inject_wait_timeout(perm_ctx* ctx, int launches);
  * No counterpart in the reference. */
 int perm_sdd_layout(const double* mat, int n);
 
+/* Host only (no device): the layout PERM_KERNEL_DENSE_INT (the int32-X walk)
+ * uses for the row-major n x n matrix `mat`: returns the product-group size
+ * G (3..6, every group's product fits int32) and sets *ngo to the number of
+ * outer groups of the two-level row layout (orders 20..48: the three
+ * columns whose nonzeros lie in the fewest rows go first, and *ngo groups of
+ * the rows they never touch keep their product for seven of every eight Gray
+ * steps), 0 for the one-level walk.  PERM_EUNSUPPORTED where int32 X does not
+ * apply, PERM_EINVAL for bad arguments.  No counterpart in the reference. */
+int perm_int_layout(const double* mat, int n, int* ngo);
+
 /* Host only (no device): the layout PERM_KERNEL_DENSE_INT_DD uses for the
  * row-major n x n matrix `mat`: returns the product-group size G (3..6:
  * every run of G rows has prod(sum_k |a_jk|) < 2^31, so group values are

@@ -39,6 +39,7 @@
 #include "ryser_dense_tc.cuh"
 #include "ryser_dense_int.cuh"
 #include "ryser_dense_intc.cuh"
+#include "ryser_dense_int_sparse.cuh"
 #include "ryser_dense_sdd.cuh"
 #include "skipper.h"
 
@@ -61,6 +62,9 @@ const void* dense_intc_kernel_g3(int n);
 const void* dense_intc_kernel_g4(int n);
 const void* dense_intc_kernel_g5(int n);
 const void* dense_intc_kernel_g6(int n);
+const void* dense_int_sparse_kernel_g4(int n, int ngo);
+const void* dense_int_sparse_kernel_g5(int n, int ngo);
+const void* dense_int_sparse_kernel_g6(int n, int ngo);
 const void* dense_intc_pair_kernel_g4(int n);
 const void* dense_intc_pair_kernel_g5(int n);
 const void* dense_intc_pair_kernel_g6(int n);
@@ -92,6 +96,18 @@ static const void* dense_int_kernel(int n, int g) {
     case 4: return dense_int_kernel_g4(n);
     case 5: return dense_int_kernel_g5(n);
     case 6: return dense_int_kernel_g6(n);
+    default: return nullptr;
+  }
+}
+
+// int32-X walk in the two-level row layout (ryser_dense_int_sparse.cuh):
+// orders 20..48, groups of 4..6 rows, 1..3 outer groups
+constexpr int kIntSparseMinN = 20, kIntSparseMaxN = 48, kIntSparseMaxOuter = 3;
+static const void* dense_int_sparse_kernel(int n, int g, int ngo) {
+  switch (g) {
+    case 4: return dense_int_sparse_kernel_g4(n, ngo);
+    case 5: return dense_int_sparse_kernel_g5(n, ngo);
+    case 6: return dense_int_sparse_kernel_g6(n, ngo);
     default: return nullptr;
   }
 }
@@ -343,8 +359,9 @@ struct perm_ctx {
   // occupancy per kernel family and order: [0] FP64-X, [G] int32-X, [7] dd,
   // [8 + G - 3] tensor core, [12] split X, [13 + G - 3] certified int32-X,
   // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows,
-  // [22 + G - 4] certified int32-X with exact pairs of groups
-  int dense_occ[25][PERM_MAX_EXACT_N + 1] = {};
+  // [22 + G - 4] certified int32-X with exact pairs of groups, [25 + 3 (G - 4)
+  // + ngo - 1] int32-X in the two-level row layout
+  int dense_occ[34][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
@@ -565,6 +582,7 @@ static int finish_and_read(perm_ctx* ctx, int nout) {
 struct DenseOperand {
   int n = 0, variant = PERM_KERNEL_DENSE, group = 0;
   int pair = 0;   // certified int32-X walk: consecutive groups multiplied in exact FP64 pairs
+  int ngo = 0;    // int32-X walk: outer product groups of the two-level row layout (0: one level)
   int inner = 0;  // split-dd: rows 0..inner-1 hold the support of columns 0..2 (0: dense layout)
   std::vector<unsigned char> image;
 };
@@ -785,6 +803,58 @@ static std::vector<double> sparse_permutation(const double* a, int n, const int*
   return p;
 }
 
+// Two-level row layout of the int32-X walk (ryser_dense_int_sparse.cuh): the
+// three columns whose nonzeros lie in the fewest rows move to positions 0..2
+// and those rows to the top (sparse_permutation); the remaining rows form
+// ngo whole product groups that columns 0..2 never touch.  Per 8 Gray steps
+// the one-level walk with groups of G costs about 8 (2n + ceil(n/G)) integer
+// and FP64 instructions, the two-level one 7 (2 RI + ceil(RI/G) + 1) +
+// 2n + ceil(n/G) + ngo with RI = n - ngo G inner rows.  Takes the cheapest
+// (G, ngo), G in 4..6 up to the one-level G, ngo in 1..3, among layouts
+// whose every group product provably fits int32 in this grouping (inner
+// groups from row 0, outer groups from row RI); *perm receives the permuted
+// matrix.  False when the one-level walk is as cheap.
+static bool int_two_level_layout(const std::vector<double>& a, int n, int g1, int* g_out, int* ngo_out,
+                                 std::vector<double>* perm) {
+  if (n < kIntSparseMinN || n > kIntSparseMaxN || g1 < 4) return false;
+  int c3[3];
+  const int support = sparsest_column_triple(a, n, c3);
+  const int outer = n - support;
+  if (outer < 4) return false;
+  std::vector<double> p = sparse_permutation(a.data(), n, c3);
+  std::vector<double> rowabs;
+  if (!int_row_abs(p, n, rowabs)) return false;
+  auto fits = [&](int g, int ngo) {
+    const int ri = n - g * ngo;
+    auto run = [&](int j0, int j1) {
+      double b = 1.0;
+      for (int j = j0; j < j1; j++) b *= std::max(rowabs[j], 1.0);
+      return b < 2147483648.0;
+    };
+    for (int j = 0; j < ri; j += g)
+      if (!run(j, std::min(j + g, ri))) return false;
+    for (int t = 0; t < ngo; t++)
+      if (!run(ri + t * g, ri + t * g + g)) return false;
+    return true;
+  };
+  const long best_one = 8L * (2 * n + (n + g1 - 1) / g1);
+  long best = best_one;
+  for (int g = std::min(g1, 6); g >= 4; g--)
+    for (int ngo = std::min(kIntSparseMaxOuter, outer / g); ngo >= 1; ngo--) {
+      const int ri = n - g * ngo;
+      if (ri < 3) continue;
+      const long cost = 7L * (2 * ri + (ri + g - 1) / g + 1) + 2 * n + (n + g - 1) / g + ngo;
+      if (cost < best && fits(g, ngo)) {
+        best = cost;
+        *g_out = g;
+        *ngo_out = ngo;
+      }
+    }
+  if (best == best_one) return false;
+  *perm = std::move(p);
+  return true;
+}
+
 static int build_sdd_operand(perm_ctx* ctx, const std::vector<double>& a, int n, DenseOperand* op) {
   if (n < 4 || n > 40) return fail(ctx, PERM_EUNSUPPORTED, "split-dd kernel covers orders 4..40 (got %d)", n);
   int c3[3] = {0, 1, 2};
@@ -826,7 +896,11 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
                                                         : PERM_KERNEL_DENSE_INT;
     op->group = G;
     op->pair = 0;
+    op->ngo = 0;
     if (op->variant == PERM_KERNEL_DENSE_INT_DD) op->group = intc_layout(a, n, &op->pair);
+    std::vector<double> two;
+    if (op->variant == PERM_KERNEL_DENSE_INT && int_two_level_layout(a, n, G, &op->group, &op->ngo, &two))
+      a.swap(two);  // walk the permuted matrix (same permanent)
     op->image.assign(sizeof(int) * (size_t)(n + 1) * np4, 0);
     int* img = reinterpret_cast<int*>(op->image.data());
     for (int k = 0; k < n; k++)
@@ -855,7 +929,8 @@ struct perm_matrix {
 };
 
 static const void* operand_kernel(const DenseOperand& op) {
-  if (op.variant == PERM_KERNEL_DENSE_INT) return dense_int_kernel(op.n, op.group);
+  if (op.variant == PERM_KERNEL_DENSE_INT)
+    return op.ngo ? dense_int_sparse_kernel(op.n, op.group, op.ngo) : dense_int_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_INT_DD) return dense_intc_kernel(op.n, op.group, op.pair);
   if (op.variant == PERM_KERNEL_DENSE_SDD) return sdd_kernel(op.n, op.inner);
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
@@ -898,6 +973,21 @@ static void shard_bounds(int n, int shard, int nshards, uint64_t* first, uint64_
   if (ms_out) *ms_out = ms;
 }
 
+extern "C" int perm_int_layout(const double* mat, int n, int* ngo) {
+  if (!mat || !ngo || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
+  std::vector<double> a(mat, mat + (size_t)n * n);
+  *ngo = 0;
+  int g = int_group_size(a, n);
+  if (!g) return PERM_EUNSUPPORTED;
+  std::vector<double> two;
+  int g2 = g, ngo2 = 0;
+  if (int_two_level_layout(a, n, g, &g2, &ngo2, &two)) {
+    g = g2;
+    *ngo = ngo2;
+  }
+  return g;
+}
+
 extern "C" int perm_intc_layout(const double* mat, int n, int* pair) {
   if (!mat || !pair || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
   std::vector<double> a(mat, mat + (size_t)n * n);
@@ -927,7 +1017,8 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
   int sparse_slot = 0;
   for (int i = 0; i < 4; i++)
     if (op.inner == kSparseInner[i]) sparse_slot = 18 + i;
-  int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? op.group
+  int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? (op.ngo ? 25 + 3 * (op.group - 4) + op.ngo - 1
+                                                                              : op.group)
                                  : op.variant == PERM_KERNEL_DENSE_DD ? 7
                                  : op.variant == PERM_KERNEL_DENSE_TC ? 8 + op.group - 3
                                  : op.variant == PERM_KERNEL_DENSE_SPLIT ? 12

@@ -75,6 +75,21 @@ def test_header_constants_match_the_binding(pb):
             assert hasattr(pb, name), name
 
 
+def test_int_layout_query(pb):
+    """Host-only layout of the int32-X walk: the order-40 bench matrix walks
+    in the two-level row layout with three outer groups of 5 rows (its three
+    sparsest columns touch 25 of 40 rows); small orders keep one level;
+    non-integer matrices are refused."""
+    import bench
+
+    assert pb.int_layout(bench.make_matrix(0)) == (5, 3)
+    rng = np.random.default_rng(4)
+    assert pb.int_layout((rng.random((16, 16)) < 0.5).astype(float))[1] == 0
+    g, ngo = pb.int_layout((rng.random((30, 30)) < 0.5) * rng.integers(1, 5, (30, 30)).astype(float))
+    assert g in (4, 5, 6) and ngo in (1, 2, 3)
+    assert pb.int_layout(rng.random((20, 20)))[0] == pb.PERM_EUNSUPPORTED
+
+
 def test_intc_layout_query(pb):
     """Host-only layout of the certified int32-X walk: the product-group size
     is the int32-X rule's, and consecutive groups are paired (exact FP64

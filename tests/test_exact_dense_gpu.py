@@ -158,6 +158,35 @@ def test_int_kernel_exact_vs_oracle(engine, orc, pb, n):
         assert rel_err(f.value, r.value) < 1e-12
 
 
+@pytest.mark.parametrize("n", [20, 23, 27])
+def test_int_kernel_two_level_layout_vs_exact(engine, orc, pb, n):
+    """The int32-X walk in the two-level row layout (the rows that the three
+    sparsest columns never touch keep their group product for seven of
+    every eight steps) against the exact multi-modular oracle, on dense
+    U{1..4}, 0/1 and signed matrices; shards and a resident matrix of the
+    same layout add up to the whole walk."""
+    rng = np.random.default_rng(600 + n)
+    cases = {"u1to4": bernoulli(rng, n, 0.5) * rng.integers(1, 5, (n, n)),
+             "binary": bernoulli(rng, n, 0.5),
+             "signed": bernoulli(rng, n, 0.5) * rng.integers(-3, 4, (n, n))}
+    for kind, A in cases.items():
+        g, ngo = pb.int_layout(A)
+        assert ngo >= 1, (kind, g, ngo)
+        exact = orc.perm_exact_int(A)[0]
+        r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
+        assert r.kernel == pb.PERM_KERNEL_DENSE_INT
+        assert abs(r.value - exact) <= 1e-12 * max(abs(exact), 1.0) + 1e-12 * r.abs_term_sum, (kind, r.value, exact)
+    A = cases["u1to4"]
+    whole = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT).value
+    parts = [engine.exact_dense_shard(A, s, 3, variant=pb.PERM_KERNEL_DENSE_INT) for s in range(3)]
+    assert rel_err(sum(p.hi + p.lo for p in parts), whole) < 1e-13
+    res = engine.upload_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
+    try:
+        assert res.run().value == whole
+    finally:
+        res.free()
+
+
 def test_int_kernel_signed_entries(engine, orc, pb):
     rng = np.random.default_rng(17)
     A = rng.integers(-4, 5, (18, 18)).astype(float)

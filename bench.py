@@ -188,7 +188,8 @@ def run_reference_arm(args):
 KERNEL_SOURCES = {
     "int32x": ["ryser_dense_int_sparse.cuh", "ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
     "fp64x": ["ryser_dense.cuh", "perman_common.cuh"],
-    "int32x_dd": ["ryser_dense_intc.cuh", "ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
+    "int32x_dd": ["ryser_dense_intc_sparse.cuh", "ryser_dense_intc.cuh", "ryser_dense_int_sparse.cuh",
+                  "ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
 }
 
 
@@ -210,8 +211,11 @@ def kernel_template(kname: str, A: np.ndarray) -> str:
     if kname == "int32x_dd":
         # product groups and pairing as the engine lays them out; last template
         # argument: CTAs per SM compiled for (3 up to order 36, 2 above)
-        g, pair = (sys.modules.get("perman_b200") or load_pkg()).intc_layout(A)
-        return f"ryser_dense_intc_kernel<{n}, {g}, {'true' if pair else 'false'}, {3 if n <= 36 else 2}>"
+        g, pair, ngo = (sys.modules.get("perman_b200") or load_pkg()).intc_layout(A)
+        pb_ = "true" if pair else "false"
+        if ngo:
+            return f"ryser_dense_intc_sparse_kernel<{n}, {g}, {pb_}, {ngo}, {3 if n <= 36 else 2}>"
+        return f"ryser_dense_intc_kernel<{n}, {g}, {pb_}, {3 if n <= 36 else 2}>"
     if kname == "fp64x":
         return f"ryser_dense_kernel<{n}>"
     return kname

@@ -121,7 +121,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_exact_dense_ex": (i, [_P, _P, i, i, i, i, i, ctypes.POINTER(PermResult)]),
         "perm_shard_range": (i, [i, i, i, ctypes.POINTER(u64), ctypes.POINTER(u64)]),
         "perm_sdd_layout": (i, [_P, i]),
-        "perm_intc_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int)]),
+        "perm_intc_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
         "perm_int_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int)]),
         "perm_exact_dense_plan": (i, [_P, _P, i, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
         "perm_matrix_create_dense_ex": (i, [_P, _P, i, i, i, ctypes.POINTER(_P)]),
@@ -627,14 +627,15 @@ def int_layout(mat) -> tuple[int, int]:
     return g, ngo.value
 
 
-def intc_layout(mat) -> tuple[int, bool]:
-    """Product-group size G and exact pairing of the certified int32-X walk
-    for this matrix (perm_intc_layout; host only); (negative status, False)
+def intc_layout(mat) -> tuple[int, bool, int]:
+    """Product-group size G, exact int64 pairing and number of outer groups
+    of the two-level row layout (0: one level) of the certified int32-X walk
+    for this matrix (perm_intc_layout; host only); (negative status, False, 0)
     where the kernel does not apply."""
     a = np.ascontiguousarray(mat, dtype=np.float64)
-    pair = ctypes.c_int(0)
-    g = int(load_library().perm_intc_layout(_ptr(a), a.shape[0], ctypes.byref(pair)))
-    return g, bool(pair.value)
+    pair, ngo = ctypes.c_int(0), ctypes.c_int(0)
+    g = int(load_library().perm_intc_layout(_ptr(a), a.shape[0], ctypes.byref(pair), ctypes.byref(ngo)))
+    return g, bool(pair.value), ngo.value
 
 
 def shard_range(n: int, shard: int, nshards: int) -> tuple[int, int]:

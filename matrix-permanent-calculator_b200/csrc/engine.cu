@@ -40,6 +40,7 @@
 #include "ryser_dense_int.cuh"
 #include "ryser_dense_intc.cuh"
 #include "ryser_dense_int_sparse.cuh"
+#include "ryser_dense_intc_sparse.cuh"
 #include "ryser_dense_sdd.cuh"
 #include "skipper.h"
 
@@ -65,6 +66,9 @@ const void* dense_intc_kernel_g6(int n);
 const void* dense_int_sparse_kernel_g4(int n, int ngo);
 const void* dense_int_sparse_kernel_g5(int n, int ngo);
 const void* dense_int_sparse_kernel_g6(int n, int ngo);
+const void* dense_intc_sparse_kernel_g4p(int n, int ngo);
+const void* dense_intc_sparse_kernel_g5(int n, int ngo);
+const void* dense_intc_sparse_kernel_g6p(int n, int ngo);
 const void* dense_intc_pair_kernel_g4(int n);
 const void* dense_intc_pair_kernel_g5(int n);
 const void* dense_intc_pair_kernel_g6(int n);
@@ -108,6 +112,20 @@ static const void* dense_int_sparse_kernel(int n, int g, int ngo) {
     case 4: return dense_int_sparse_kernel_g4(n, ngo);
     case 5: return dense_int_sparse_kernel_g5(n, ngo);
     case 6: return dense_int_sparse_kernel_g6(n, ngo);
+    default: return nullptr;
+  }
+}
+
+// certified int32-X walk in the two-level row layout: groups of 4 and 6 in
+// int64 pairs, groups of 5 alone (family index 0, 1, 2)
+static int intc_sparse_family(int g, int pair) {
+  return (g == 4 && pair) ? 0 : (g == 5 && !pair) ? 1 : (g == 6 && pair) ? 2 : -1;
+}
+static const void* dense_intc_sparse_kernel(int n, int g, int pair, int ngo) {
+  switch (intc_sparse_family(g, pair)) {
+    case 0: return dense_intc_sparse_kernel_g4p(n, ngo);
+    case 1: return dense_intc_sparse_kernel_g5(n, ngo);
+    case 2: return dense_intc_sparse_kernel_g6p(n, ngo);
     default: return nullptr;
   }
 }
@@ -360,8 +378,9 @@ struct perm_ctx {
   // [8 + G - 3] tensor core, [12] split X, [13 + G - 3] certified int32-X,
   // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows,
   // [22 + G - 4] certified int32-X with exact pairs of groups, [25 + 3 (G - 4)
-  // + ngo - 1] int32-X in the two-level row layout
-  int dense_occ[34][PERM_MAX_EXACT_N + 1] = {};
+  // + ngo - 1] int32-X in the two-level row layout, [34 + 3 family + ngo - 1]
+  // certified int32-X in the two-level layout
+  int dense_occ[43][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
@@ -632,7 +651,7 @@ static int int_group_size(const std::vector<double>& a, int n) {
 // pairs cost n - g multiplies, floor(g/2) 64-bit multiplies, f = ceil(g/2)
 // conversions and 3f - 4 operations; the layout with the fewest instructions
 // is taken.  Returns G, or 0 when int32 X does not apply.
-static int intc_layout(const std::vector<double>& a, int n, int* pair) {
+static int intc_layout(const std::vector<double>& a, int n, int* pair, int* cost_out = nullptr) {
   *pair = 0;
   if (n < 8) return 0;
   std::vector<double> rowabs;
@@ -649,6 +668,7 @@ static int intc_layout(const std::vector<double>& a, int n, int* pair) {
     }
   }
   *pair = best_pair;
+  if (cost_out) *cost_out = best_cost;
   return best_g;
 }
 
@@ -855,6 +875,70 @@ static bool int_two_level_layout(const std::vector<double>& a, int n, int g1, in
   return true;
 }
 
+// Two-level row layout of the certified int32-X walk
+// (ryser_dense_intc_sparse.cuh): the permutation of int_two_level_layout,
+// with groups of 4 or 6 rows in int64 pairs or groups of 5 alone.  Per Gray
+// step a level of r rows in g groups with f factors costs r - g int32
+// multiplies, its 64-bit pair multiplies, f conversions and 3 double-double
+// operations per factor; the inner level runs at every step, the outer one
+// and the updates of all n rows at one step in eight.  Takes the cheapest
+// layout among those whose group (< 2^31) and pair (< 2^53) products
+// provably fit, and only when it beats the one-level layout `one_cost`
+// (instructions per 8 steps).  *perm receives the permuted matrix.
+static bool intc_two_level_layout(const std::vector<double>& a, int n, long one_cost, int* g_out, int* pair_out,
+                                  int* ngo_out, std::vector<double>* perm) {
+  if (n < kIntSparseMinN || n > kIntSparseMaxN) return false;
+  int c3[3];
+  const int support = sparsest_column_triple(a, n, c3);
+  const int outer = n - support;
+  if (outer < 4) return false;
+  std::vector<double> p = sparse_permutation(a.data(), n, c3);
+  std::vector<double> rowabs;
+  if (!int_row_abs(p, n, rowabs)) return false;
+  auto prod = [&](int j0, int j1) {
+    double b = 1.0;
+    for (int j = j0; j < j1; j++) b *= std::max(rowabs[j], 1.0);
+    return b;
+  };
+  // groups of one level, rows [j0, j1) in runs of g
+  auto level_fits = [&](int j0, int j1, int g, bool pair) {
+    std::vector<std::pair<int, int>> grp;
+    for (int j = j0; j < j1; j += g) grp.push_back({j, std::min(j + g, j1)});
+    for (auto& r : grp)
+      if (!(prod(r.first, r.second) < 2147483648.0)) return false;
+    if (pair)
+      for (size_t i = 0; i + 1 < grp.size(); i += 2)
+        if (!(prod(grp[i].first, grp[i + 1].second) < 9007199254740992.0)) return false;
+    return true;
+  };
+  auto level_cost = [&](int rows, int g, bool pair) {
+    const int ng = (rows + g - 1) / g, f = pair ? (ng + 1) / 2 : ng;
+    return (long)(rows - ng) + (pair ? ng / 2 : 0) + f + 3L * f;
+  };
+  long best = one_cost;
+  const int fam_g[3] = {4, 5, 6};
+  const bool fam_pair[3] = {true, false, true};
+  for (int fam = 0; fam < 3; fam++) {
+    const int g = fam_g[fam];
+    const bool pair = fam_pair[fam];
+    for (int ngo = std::min(kIntSparseMaxOuter, outer / g); ngo >= 1; ngo--) {
+      const int ri = n - g * ngo;
+      if (ri < 3) continue;
+      const long inner = ri + level_cost(ri, g, pair);
+      const long cost = 7 * inner + n + level_cost(ri, g, pair) + level_cost(n - ri, g, pair);
+      if (cost < best && level_fits(0, ri, g, pair) && level_fits(ri, n, g, pair)) {
+        best = cost;
+        *g_out = g;
+        *pair_out = pair ? 1 : 0;
+        *ngo_out = ngo;
+      }
+    }
+  }
+  if (best == one_cost) return false;
+  *perm = std::move(p);
+  return true;
+}
+
 static int build_sdd_operand(perm_ctx* ctx, const std::vector<double>& a, int n, DenseOperand* op) {
   if (n < 4 || n > 40) return fail(ctx, PERM_EUNSUPPORTED, "split-dd kernel covers orders 4..40 (got %d)", n);
   int c3[3] = {0, 1, 2};
@@ -897,10 +981,15 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
     op->group = G;
     op->pair = 0;
     op->ngo = 0;
-    if (op->variant == PERM_KERNEL_DENSE_INT_DD) op->group = intc_layout(a, n, &op->pair);
     std::vector<double> two;
+    if (op->variant == PERM_KERNEL_DENSE_INT_DD) {
+      int cost1 = 0;
+      op->group = intc_layout(a, n, &op->pair, &cost1);
+      if (intc_two_level_layout(a, n, 8L * (n + cost1), &op->group, &op->pair, &op->ngo, &two))
+        a.swap(two);  // walk the permuted matrix (same permanent)
+    }
     if (op->variant == PERM_KERNEL_DENSE_INT && int_two_level_layout(a, n, G, &op->group, &op->ngo, &two))
-      a.swap(two);  // walk the permuted matrix (same permanent)
+      a.swap(two);
     op->image.assign(sizeof(int) * (size_t)(n + 1) * np4, 0);
     int* img = reinterpret_cast<int*>(op->image.data());
     for (int k = 0; k < n; k++)
@@ -931,7 +1020,8 @@ struct perm_matrix {
 static const void* operand_kernel(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_INT)
     return op.ngo ? dense_int_sparse_kernel(op.n, op.group, op.ngo) : dense_int_kernel(op.n, op.group);
-  if (op.variant == PERM_KERNEL_DENSE_INT_DD) return dense_intc_kernel(op.n, op.group, op.pair);
+  if (op.variant == PERM_KERNEL_DENSE_INT_DD)
+    return op.ngo ? dense_intc_sparse_kernel(op.n, op.group, op.pair, op.ngo) : dense_intc_kernel(op.n, op.group, op.pair);
   if (op.variant == PERM_KERNEL_DENSE_SDD) return sdd_kernel(op.n, op.inner);
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
@@ -988,11 +1078,21 @@ extern "C" int perm_int_layout(const double* mat, int n, int* ngo) {
   return g;
 }
 
-extern "C" int perm_intc_layout(const double* mat, int n, int* pair) {
-  if (!mat || !pair || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
+extern "C" int perm_intc_layout(const double* mat, int n, int* pair, int* ngo) {
+  if (!mat || !pair || !ngo || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
   std::vector<double> a(mat, mat + (size_t)n * n);
-  const int g = intc_layout(a, n, pair);
-  return g ? g : PERM_EUNSUPPORTED;
+  int cost1 = 0;
+  int g = intc_layout(a, n, pair, &cost1);
+  *ngo = 0;
+  if (!g) return PERM_EUNSUPPORTED;
+  std::vector<double> two;
+  int g2 = g, p2 = *pair, ngo2 = 0;
+  if (intc_two_level_layout(a, n, 8L * (n + cost1), &g2, &p2, &ngo2, &two)) {
+    g = g2;
+    *pair = p2;
+    *ngo = ngo2;
+  }
+  return g;
 }
 
 extern "C" int perm_sdd_layout(const double* mat, int n) {
@@ -1022,7 +1122,9 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
                                  : op.variant == PERM_KERNEL_DENSE_DD ? 7
                                  : op.variant == PERM_KERNEL_DENSE_TC ? 8 + op.group - 3
                                  : op.variant == PERM_KERNEL_DENSE_SPLIT ? 12
-                                 : op.variant == PERM_KERNEL_DENSE_INT_DD ? (op.pair ? 22 + op.group - 4 : 13 + op.group - 3)
+                                 : op.variant == PERM_KERNEL_DENSE_INT_DD
+                                     ? (op.ngo ? 34 + 3 * intc_sparse_family(op.group, op.pair) + op.ngo - 1
+                                               : op.pair ? 22 + op.group - 4 : 13 + op.group - 3)
                                  : op.variant == PERM_KERNEL_DENSE_SDD ? (op.inner ? sparse_slot : 17) : 0][n];
   if (!occ_slot) {
     int rc = allow_smem(ctx, fn, operand_smem(op));

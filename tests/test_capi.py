@@ -91,18 +91,20 @@ def test_int_layout_query(pb):
 
 
 def test_intc_layout_query(pb):
-    """Host-only layout of the certified int32-X walk: the product-group size
-    is the int32-X rule's, and consecutive groups are paired (exact FP64
-    products) from order 16 when every run of 2G rows stays below 2^53 --
-    the layout with the fewest FP64 operations per Gray step."""
+    """Host-only layout of the certified int32-X walk: product groups that
+    fit int32, consecutive groups paired (exact int64 products) from order 16
+    when every run of 2G rows stays below 2^53, and from order 20 the
+    two-level row layout where it is cheaper -- the layout with the fewest
+    instructions per Gray step."""
     rng = np.random.default_rng(3)
     A = ((rng.random((40, 40)) < 0.5) * rng.integers(1, 5, (40, 40))).astype(float)
-    assert pb.intc_layout(A) == (4, True)  # groups of 5 fit int32, pairs of 5 would not fit 2^53
+    g, pair, ngo = pb.intc_layout(A)
+    assert (g, pair) in ((4, True), (5, False)) and ngo in (1, 2, 3)  # two levels at order 40
     B = (rng.random((40, 40)) < 0.5).astype(float)
-    assert pb.intc_layout(B) == (6, True)
-    assert pb.intc_layout(B[:12, :12])[1] is False  # pairs from order 16
+    assert pb.intc_layout(B)[0] in (4, 5, 6)
+    assert pb.intc_layout(B[:12, :12])[1:] == (False, 0)  # pairs from order 16, two levels from 20
     C = rng.integers(0, 60, (24, 24)).astype(float)
-    assert pb.intc_layout(C) == (3, False)  # large entries: groups of 3, no pairs
+    assert pb.intc_layout(C) == (3, False, 0)  # large entries: groups of 3, no pairs
     assert pb.intc_layout(rng.random((20, 20)))[0] == pb.PERM_EUNSUPPORTED
     assert pb.intc_layout(np.ones((7, 7)))[0] == pb.PERM_EUNSUPPORTED
 

@@ -28,9 +28,11 @@ def test_int_dd_vs_exact(engine, orc, pb, n):
         "binary": bernoulli(rng, n, 0.5),
         "large": rng.integers(0, 60, (n, n)).astype(float),  # small product groups
     }
-    layouts = set()
+    layouts, levels = set(), set()
     for kind, A in cases.items():
-        layouts.add(pb.intc_layout(A))
+        g, pair, ngo = pb.intc_layout(A)
+        layouts.add((g, pair))
+        levels.add(ngo > 0)
         exact = orc.perm_exact_int(A)[0]
         r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT_DD)
         assert r.kernel == pb.PERM_KERNEL_DENSE_INT_DD
@@ -41,8 +43,29 @@ def test_int_dd_vs_exact(engine, orc, pb, n):
         assert ok, (kind, info)
         assert r.rel_error_estimate < 1e-20, (kind, r.rel_error_estimate)  # u^2-level bound
         assert rel_err(r.value, exact) <= 1.2e-16  # value is the pair rounded once (<= 2^-53)
-    if n >= 16:  # both product layouts ran: exact FP64 pairs of groups and the plain chain
+    if n >= 16:  # both product layouts ran: exact int64 pairs of groups and the plain chain
         assert {p for _, p in layouts} == {True, False}, layouts
+    if n >= 20:  # and the two-level row layout beside the one-level walk
+        assert True in levels, levels
+
+
+@pytest.mark.parametrize("n,d,seed", [(24, 0.3, 1), (26, 0.3, 0), (27, 0.4, 2)])
+def test_int_dd_two_level_groups_of_6_vs_exact(engine, orc, pb, n, d, seed):
+    """Sparse 0/1 matrices whose certified walk takes the two-level row
+    layout with groups of 6 in int64 pairs: exact against the multi-modular
+    oracle within the walk's own bound."""
+    rng = np.random.default_rng(seed)
+    A = bernoulli(rng, n, d)
+    g, pair, ngo = pb.intc_layout(A)
+    assert g == 6 and pair and ngo >= 2
+    exact = orc.perm_exact_int(A)[0]
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT_DD)
+    if exact == 0:
+        assert abs(r.value) <= r.rel_error_estimate * max(r.abs_term_sum, 1.0)
+    else:
+        ok, info = _covers(r, exact)
+        assert ok, info
+        assert rel_err(r.value, exact) <= 1.2e-16
 
 
 def test_int_dd_golden_n32(engine, golden, pb):

@@ -162,7 +162,7 @@ int perm_exact_dense_ex(perm_ctx* ctx, const void* mat, int n, int dtype, int va
  * policy; < 0 also skips the estimate):
  *  - a zero pattern without a perfect matching returns exactly 0;
  *  - whole walks of integer matrices whose group products fit in int32 run
- *    PERM_KERNEL_DENSE_INT_DD at once (about 1.3 int32-X walks), and real
+ *    PERM_KERNEL_DENSE_INT_DD at once (about 1.4 int32-X walks), and real
  *    matrices of order 12..40 whose three sparsest columns touch so few rows
  *    R that the sparse layout's (7 (6R + 9) + 6n + 5) / 8 FP64 operations
  *    per Gray step are at most FP64 X's 2n run PERM_KERNEL_DENSE_SDD in

@@ -1572,7 +1572,7 @@ static int refine_result(perm_ctx* ctx, const void* mat, int n, int dtype, const
 
 // With the accuracy policy on, the kernel a whole-walk call starts with
 // when a certified walk is cheap enough to go first: int32 X with
-// double-double products for integer matrices (about 1.3 int32-X walks, its
+// double-double products for integer matrices (about 1.4 int32-X walks, its
 // bound needs no sample), split-dd in the sparse layout for real matrices
 // whose three sparsest columns touch so few rows R that its
 // (7 (6R + 9) + 6n + 5) / 8 FP64 operations per Gray step are no more than

@@ -212,8 +212,10 @@ int perm_ctx_inject_wait_timeout(perm_ctx* ctx, int launches);
 
 /* Host only (no device): the layout PERM_KERNEL_DENSE_SDD uses for the
  * row-major n x n matrix `mat`: the number of inner rows R of the sparse
- * layout (6, 8, 12 or 16: columns 0..2 after its permutation touch rows
- * 0..R-1 only, so 7 of 8 Gray steps walk R rows), 0 for the dense layout,
+ * layout (6, 8, 12, 16, or 20, 24, 28 with a rolled step loop for dense
+ * matrices whose three sparsest columns still miss a quarter or more of the
+ * rows: columns 0..2 after its permutation touch rows 0..R-1 only, so 7 of
+ * 8 Gray steps walk R rows), 0 for the dense layout,
  * PERM_EUNSUPPORTED where the kernel does not apply (orders outside 4..40,
  * row absolute sums at or above 2^1020), PERM_EINVAL for bad arguments.
  * No counterpart in the reference. */

@@ -78,6 +78,9 @@ const void* sparse_sdd_kernel_r6(int n);
 const void* sparse_sdd_kernel_r8(int n);
 const void* sparse_sdd_kernel_r12(int n);
 const void* sparse_sdd_kernel_r16(int n);
+const void* sparse_sdd_kernel_r20(int n);
+const void* sparse_sdd_kernel_r24(int n);
+const void* sparse_sdd_kernel_r28(int n);
 
 const void* dense_tc_kernel_g3(int n);
 const void* dense_tc_kernel_g4(int n);
@@ -149,7 +152,8 @@ static const void* dense_intc_kernel(int n, int g, int pair) {
 }
 
 // Inner-row counts of the sparse split-dd layout (ryser_sparse_sdd_kernel<N, R>).
-constexpr int kSparseInner[4] = {6, 8, 12, 16};
+// 20..28: the rolled step loop (two-level rows of dense matrices)
+constexpr int kSparseInner[7] = {6, 8, 12, 16, 20, 24, 28};
 
 static const void* sdd_kernel(int n, int inner) {
   switch (inner) {
@@ -158,6 +162,9 @@ static const void* sdd_kernel(int n, int inner) {
     case 8: return sparse_sdd_kernel_r8(n);
     case 12: return sparse_sdd_kernel_r12(n);
     case 16: return sparse_sdd_kernel_r16(n);
+    case 20: return sparse_sdd_kernel_r20(n);
+    case 24: return sparse_sdd_kernel_r24(n);
+    case 28: return sparse_sdd_kernel_r28(n);
     default: return nullptr;
   }
 }
@@ -376,11 +383,12 @@ struct perm_ctx {
   size_t d_trials_cap = 0;
   // occupancy per kernel family and order: [0] FP64-X, [G] int32-X, [7] dd,
   // [8 + G - 3] tensor core, [12] split X, [13 + G - 3] certified int32-X,
-  // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows,
+  // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows
+  // (i < 4; [43 + i - 4] for the others),
   // [22 + G - 4] certified int32-X with exact pairs of groups, [25 + 3 (G - 4)
   // + ngo - 1] int32-X in the two-level row layout, [34 + 3 family + ngo - 1]
   // certified int32-X in the two-level layout
-  int dense_occ[43][PERM_MAX_EXACT_N + 1] = {};
+  int dense_occ[46][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
@@ -787,12 +795,19 @@ static int sparsest_column_triple(const std::vector<double>& a, int n, int* c3) 
 
 // Inner-row count of the sparse split-dd layout for this matrix (0: dense
 // layout): the smallest kSparseInner entry that holds the rows of the three
-// sparsest columns, for orders 12..40.
+// sparsest columns, for orders 12..40.  Inner-row counts of 20 and more
+// (the rolled two-level walk of dense matrices) are taken when their
+// (7 (6R + 13) + 12n - 6R + 20) / 8 FP64 operations per step are at most
+// 0.85 of the dense layout's 6n + 10 (measured: n = 32 with 20 inner rows
+// 27.2 against 38.0 ms, n = 34 with 24 inner rows 123 against 156 ms).
 static int sdd_inner_rows(const std::vector<double>& a, int n, int* c3) {
   if (n < 12 || n > 40) return 0;
   const int u = sparsest_column_triple(a, n, c3);
   for (int r : kSparseInner)
-    if (u <= r && r + 4 <= n) return r;
+    if (u <= r && r + 4 <= n) {
+      if (r >= 20 && 7 * (6 * r + 13) + 12 * n - 6 * r + 20 > 0.85 * 8 * (6 * n + 10)) return 0;
+      return r;
+    }
   return 0;
 }
 
@@ -1115,8 +1130,8 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
   const void* fn = operand_kernel(op);
   if (!fn) return fail(ctx, PERM_EUNSUPPORTED, "dense exact order %d outside [1, %d]", n, PERM_MAX_EXACT_N);
   int sparse_slot = 0;
-  for (int i = 0; i < 4; i++)
-    if (op.inner == kSparseInner[i]) sparse_slot = 18 + i;
+  for (int i = 0; i < 7; i++)
+    if (op.inner == kSparseInner[i]) sparse_slot = i < 4 ? 18 + i : 43 + i - 4;
   int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? (op.ngo ? 25 + 3 * (op.group - 4) + op.ngo - 1
                                                                               : op.group)
                                  : op.variant == PERM_KERNEL_DENSE_DD ? 7

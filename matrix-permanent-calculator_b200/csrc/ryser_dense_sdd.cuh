@@ -226,7 +226,11 @@ __host__ __device__ inline size_t sparse_sdd_smem_bytes(int n, int r, int thread
   return dense_sdd_smem_bytes(n) + 16 * (size_t)(n - r) * threads;
 }
 
-template <int N, int R, int kMinBlocks = 2>
+// kRolled: the step loop is rolled (a runtime column at every step, the
+// outer rows updated and P_out recomputed when it is >= 3), which keeps the
+// register file to the inner rows for inner-row counts of 20 and more,
+// where the unrolled eight-step group spills.
+template <int N, int R, int kMinBlocks = 2, bool kRolled = false>
 __global__ void __launch_bounds__(128, kMinBlocks) ryser_sparse_sdd_kernel(DenseSddArgs args) {
   static_assert(R >= 2 && R + 2 <= N && (R & 1) == 0, "inner rows: even, and outer rows must remain");
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -315,6 +319,28 @@ __global__ void __launch_bounds__(128, kMinBlocks) ryser_sparse_sdd_kernel(Dense
       L = t0.lo;
       m1 = fabs(t0.hi);
     }
+    if constexpr (kRolled) {
+#pragma unroll 1
+      for (uint64_t base = s0; base < e0; base += 8) {
+        const uint64_t top = base + 8 < e0 ? base + 8 : e0 - 1;
+        double gs = 0.0, gc = 0.0, ma = 0.0;
+#pragma unroll 1
+        for (uint64_t i = base + 1; i <= top; i++) {
+          const int k = __ffsll((long long)i) - 1;
+          const double sg = ((i >> (k + 1)) & 1) ? -1.0 : 1.0;
+          pair_update<0, R, 0, R>(xh, xl, sH + k * np, sL + k * np, sg);
+          if (k >= 3) pout = outer(true, k, sg);  // the eighth step of a group: every row may change
+          const dd t = inner_term();
+          if (i & 1)
+            sum2_add(gs, gc, -t.hi, -t.lo);
+          else
+            sum2_add(gs, gc, t.hi, t.lo);
+          ma += fabs(t.hi);
+        }
+        sum2_add(H, L, gs, gc);
+        m1 += ma;
+      }
+    } else {
     const double *h0 = sH, *h1 = sH + np, *h2 = sH + 2 * np;
     const double *l0 = sL, *l1 = sL + np, *l2 = sL + 2 * np;
     const uint64_t groups = (e0 - s0) >> 3;
@@ -365,6 +391,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) ryser_sparse_sdd_kernel(Dense
 #pragma unroll 1
     for (uint64_t gi = 0; gi + 1 < groups; gi++, base += 8) group8(false);
     group8(true);
+    }
   }
   sdd_finish(H, L, m1, args, red, (N & 1) ? 2.0 : -2.0);
 }

@@ -1,0 +1,17 @@
+// ryser_sparse_sdd_r28.cu -- sparse-layout split-dd Ryser kernels whose
+// columns 0..2 touch rows 0..27 only, orders 32..40: the rolled step loop,
+// 2 CTAs per SM (inner rows in registers, the others in shared memory).
+#include "ryser_dense_sdd.cuh"
+
+namespace perm {
+#define PERM_SPSDD_CASE(n) \
+  case n: return reinterpret_cast<const void*>(&ryser_sparse_sdd_kernel<n, 28, 2, true>);
+const void* sparse_sdd_kernel_r28(int n) {
+  switch (n) {
+    PERM_SPSDD_CASE(32) PERM_SPSDD_CASE(33) PERM_SPSDD_CASE(34) PERM_SPSDD_CASE(35) PERM_SPSDD_CASE(36)
+    PERM_SPSDD_CASE(37) PERM_SPSDD_CASE(38) PERM_SPSDD_CASE(39) PERM_SPSDD_CASE(40)
+    default: return nullptr;
+  }
+}
+#undef PERM_SPSDD_CASE
+}  // namespace perm

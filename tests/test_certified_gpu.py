@@ -159,6 +159,27 @@ def test_sdd_sparse_layout_vs_oracle_dd(engine, orc, pb, n, d):
     assert rel_err(s.value, want) < TOL
 
 
+@pytest.mark.parametrize("n,seed", [(27, 1), (28, 3)])
+def test_sdd_two_level_rolled_vs_oracle_dd(engine, orc, pb, n, seed):
+    """Dense real matrices (density 1/2): the three sparsest columns still
+    miss a third of the rows, so split-dd walks 20 inner rows at seven of
+    eight steps (the rolled two-level loop); against the CPU double-double
+    Ryser, and the automatic path certifies 1e-10."""
+    rng = np.random.default_rng(seed)
+    A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+    inner = pb.sdd_layout(A)
+    assert inner in (20, 24, 28), inner
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SDD)
+    hi, lo = orc.perm_dd(A)
+    want = hi + lo
+    slack = (4 * n + 32) * 2.0 ** -106 * r.abs_term_sum
+    ok, info = _covers(r, want, slack)
+    assert ok, info
+    assert r.rel_error_estimate <= TOL
+    a = engine.exact_dense(A)
+    assert a.rel_error_estimate <= TOL and rel_err(a.value, want) <= TOL
+
+
 def test_cfg2_full_size_against_golden(engine, golden, pb, orc):
     """The sparse exact configuration at its stated size (n=36, density 0.20,
     values U(0,1]) against the CPU double-double oracle's value recorded in

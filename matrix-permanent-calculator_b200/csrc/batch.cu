@@ -454,6 +454,10 @@ __device__ __forceinline__ void walk_dispatch_sparse(int n, int r, const double*
     PERM_BATCH_SCASE(24, 16) PERM_BATCH_SCASE(25, 16) PERM_BATCH_SCASE(26, 16) PERM_BATCH_SCASE(27, 16)
     PERM_BATCH_SCASE(28, 16) PERM_BATCH_SCASE(29, 16) PERM_BATCH_SCASE(30, 16) PERM_BATCH_SCASE(31, 16)
     PERM_BATCH_SCASE(32, 16)
+    PERM_BATCH_SCASE(24, 20) PERM_BATCH_SCASE(25, 20) PERM_BATCH_SCASE(26, 20) PERM_BATCH_SCASE(27, 20)
+    PERM_BATCH_SCASE(28, 20) PERM_BATCH_SCASE(29, 20) PERM_BATCH_SCASE(30, 20) PERM_BATCH_SCASE(31, 20)
+    PERM_BATCH_SCASE(32, 20)
+    PERM_BATCH_SCASE(29, 24) PERM_BATCH_SCASE(30, 24) PERM_BATCH_SCASE(31, 24) PERM_BATCH_SCASE(32, 24)
 #undef PERM_BATCH_SCASE
     default: break;
   }
@@ -476,6 +480,10 @@ __device__ __forceinline__ void walk_dispatch_int_sparse(int n, int r, const int
     PERM_BATCH_ISCASE(24, 12) PERM_BATCH_ISCASE(25, 12) PERM_BATCH_ISCASE(26, 12) PERM_BATCH_ISCASE(27, 12)
     PERM_BATCH_ISCASE(28, 12) PERM_BATCH_ISCASE(29, 12) PERM_BATCH_ISCASE(30, 12) PERM_BATCH_ISCASE(31, 12)
     PERM_BATCH_ISCASE(32, 12)
+    PERM_BATCH_ISCASE(22, 18) PERM_BATCH_ISCASE(23, 18) PERM_BATCH_ISCASE(24, 18) PERM_BATCH_ISCASE(25, 18)
+    PERM_BATCH_ISCASE(26, 18) PERM_BATCH_ISCASE(27, 18) PERM_BATCH_ISCASE(28, 18) PERM_BATCH_ISCASE(29, 18)
+    PERM_BATCH_ISCASE(30, 18) PERM_BATCH_ISCASE(31, 18) PERM_BATCH_ISCASE(32, 18)
+    PERM_BATCH_ISCASE(29, 24) PERM_BATCH_ISCASE(30, 24) PERM_BATCH_ISCASE(31, 24) PERM_BATCH_ISCASE(32, 24)
 #undef PERM_BATCH_ISCASE
     default: break;
   }

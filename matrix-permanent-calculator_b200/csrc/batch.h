@@ -22,8 +22,8 @@ struct BatchMatrix {
                         // with product groups of g rows (doubled int columns, stride
                         // np4 = n rounded up to 4, then y0) -- orders >= 9 only
   int r;                // 0: dense walk; > 0: sparse layout, columns 0..2 nonzero in
-                        // rows 0..r-1 only (FP64: r in {8, 16}; int32, g = 6: r in {6, 12}),
-                        // orders 12..32
+                        // rows 0..r-1 only (FP64: r in {8, 16, 20, 24}; int32, g = 6: r in
+                        // {6, 12, 18, 24}), orders 12..32
 };
 
 struct BatchArgs {

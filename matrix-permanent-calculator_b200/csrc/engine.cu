@@ -2376,17 +2376,21 @@ static int batch_create_locked(perm_ctx* ctx, int count, const int* orders, cons
       std::vector<double> a(values + src_off[i], values + src_off[i] + (size_t)n * n);
       const int G = int_group_size(a, n);
       if (G >= 5) M.g = G;
-      // sparse layout (orders 12..32) when three columns have their nonzeros
-      // in few rows: FP64 X with 8 or 16 inner rows, int32 X (groups of 6)
-      // with 6 or 12
+      // two-level (sparse) layout (orders 12..32) when three columns have
+      // their nonzeros in few rows: FP64 X with 8, 16, 20 or 24 inner rows,
+      // int32 X (groups of 6) with 6, 12, 18 or 24; taken while the inner
+      // steps' 2R + 1 operations keep the 8-step cost 7 (2R + 1) + 2n within
+      // 0.85 of the one-level walk's 16n (dense matrices of density up to
+      // about 0.55 at these orders)
       if (n >= 12 && n <= 32) {
         int c3[3];
         const int u = sparsest_column_triple(a, n, c3);
         int r = 0;
         if (M.g)
-          r = u <= 6 ? 6 : u <= 12 ? 12 : 0;
+          r = u <= 6 ? 6 : u <= 12 ? 12 : u <= 18 ? 18 : u <= 24 ? 24 : 0;
         else
-          r = u <= 8 ? 8 : u <= 16 ? 16 : 0;
+          r = u <= 8 ? 8 : u <= 16 ? 16 : u <= 20 ? 20 : u <= 24 ? 24 : 0;
+        if (r > 16 && 7 * (2 * r + 1) + 2 * n > 0.85 * 16 * n) r = 0;
         if (r && r + 4 <= n) {
           std::vector<double> p = sparse_permutation(a.data(), n, c3);
           if (!M.g || int_group_size(p, n) == 6) {

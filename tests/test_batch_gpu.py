@@ -165,6 +165,30 @@ def test_sparse_layout_in_the_batch(engine, orc, pb):
         assert rel_err(v, want) < 1e-11, (m.shape, v, want)
 
 
+def test_dense_two_level_layout_in_the_batch(engine, orc, pb):
+    """Dense matrices (density 1/2) whose three sparsest columns still miss a
+    quarter or more of the rows walk the two-level layout with 18..24 inner
+    rows inside the batch: against the oracle at orders 25..28 and against
+    single-matrix walks at 30..32."""
+    rng = np.random.default_rng(92)
+    small, large = [], []
+    for n in (25, 27, 28, 30, 31, 32):
+        P = (rng.random((n, n)) < 0.5) | (np.eye(n)[rng.permutation(n)] > 0)
+        trio = [P.astype(np.float64), P * rng.integers(1, 4, (n, n)).astype(float), P * (1.0 - rng.random((n, n)))]
+        (small if n <= 28 else large).extend(trio)
+    vals, _ = engine.batch_exact(small + large)
+    for m, v in zip(small, vals[:len(small)]):
+        if np.all(m == np.round(m)):
+            want = orc.perm_exact_int(m)[0]
+        else:
+            hi, lo = orc.perm_dd(m)
+            want = hi + lo
+        assert rel_err(v, want) < 1e-11, (m.shape, v, want)
+    for m, v in zip(large, vals[len(small):]):
+        one = engine.exact_dense(m, variant=pb.PERM_KERNEL_DENSE)
+        assert rel_err(v, one.value) < 1e-10 + 2 * one.rel_error_estimate, (m.shape, v, one.value)
+
+
 def test_every_batch_variant_agrees(pb, orc):
     """Each compiled batch kernel variant (threads per block, register budget,
     shared-memory X) returns the same permanents, to rounding, on a batch of

@@ -221,6 +221,15 @@ int perm_ctx_inject_wait_timeout(perm_ctx* ctx, int launches);
  * No counterpart in the reference. */
 int perm_sdd_layout(const double* mat, int n);
 
+/* Host only (no device): the number of inner rows R (16, 20, 24 or 28) of
+ * the two-level row layout that PERM_KERNEL_DENSE (the FP64-X walk) uses for
+ * the row-major n x n matrix `mat` (orders 20..48: the three columns whose
+ * nonzeros lie in the fewest rows go first, their rows to the top, and at
+ * seven of every eight Gray steps only those R rows are updated and
+ * multiplied), 0 for the one-level walk; PERM_EINVAL for bad arguments.  No
+ * counterpart in the reference. */
+int perm_fp64_layout(const double* mat, int n);
+
 /* Host only (no device): the layout PERM_KERNEL_DENSE_INT (the int32-X walk)
  * uses for the row-major n x n matrix `mat`: returns the product-group size
  * G (3..6, every group's product fits int32) and sets *ngo to the number of

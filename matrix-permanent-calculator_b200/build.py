@@ -31,7 +31,7 @@ HOST_CXX = os.environ.get("PERM_HOST_CXX", "/usr/bin/g++")
 LIB_SOURCES = [
     "engine.cu", "ryser_skipper.cu", "mc.cu", "mc_sparse.cu", "batch.cu", "serve.cu", "noalloc.cu",
     "ryser_dense_inst_0.cu", "ryser_dense_inst_1.cu", "ryser_dense_inst_2.cu",
-    "ryser_dense_inst_3.cu", "ryser_dense_inst_4.cu", "ryser_dense_int_g3.cu", "ryser_dense_int_g4.cu",
+    "ryser_dense_inst_3.cu", "ryser_dense_inst_4.cu", "ryser_dense_2l_inst_0.cu", "ryser_dense_2l_inst_1.cu", "ryser_dense_int_g3.cu", "ryser_dense_int_g4.cu",
     "ryser_dense_int_g5.cu", "ryser_dense_int_g6.cu", "ryser_dense_int_sparse_g4.cu", "ryser_dense_int_sparse_g5.cu",
     "ryser_dense_int_sparse_g6.cu", "ryser_dense_intc_sparse_g4p.cu", "ryser_dense_intc_sparse_g5.cu",
     "ryser_dense_intc_sparse_g6p.cu", "ryser_dense_dd_inst.cu", "matrix_io.cpp",

@@ -41,6 +41,7 @@
 #include "ryser_dense_intc.cuh"
 #include "ryser_dense_int_sparse.cuh"
 #include "ryser_dense_intc_sparse.cuh"
+#include "ryser_dense_2l.cuh"
 #include "ryser_dense_sdd.cuh"
 #include "skipper.h"
 
@@ -57,6 +58,23 @@ const void* dense_int_kernel_g5(int n);
 const void* dense_int_kernel_g6(int n);
 
 const void* dense_dd_kernel(int n);
+const void* dense_2l_kernel_r16(int n);
+const void* dense_2l_kernel_r20(int n);
+const void* dense_2l_kernel_r24(int n);
+const void* dense_2l_kernel_r28(int n);
+
+// FP64-X walk in the two-level row layout (ryser_dense_2l.cuh): orders
+// 20..48, 16..28 inner rows
+constexpr int k2lInner[4] = {16, 20, 24, 28};
+static const void* dense_2l_kernel(int n, int inner) {
+  switch (inner) {
+    case 16: return dense_2l_kernel_r16(n);
+    case 20: return dense_2l_kernel_r20(n);
+    case 24: return dense_2l_kernel_r24(n);
+    case 28: return dense_2l_kernel_r28(n);
+    default: return nullptr;
+  }
+}
 const void* dense_split_kernel(int n);
 
 const void* dense_intc_kernel_g3(int n);
@@ -384,11 +402,12 @@ struct perm_ctx {
   // occupancy per kernel family and order: [0] FP64-X, [G] int32-X, [7] dd,
   // [8 + G - 3] tensor core, [12] split X, [13 + G - 3] certified int32-X,
   // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows
-  // (i < 4; [43 + i - 4] for the others),
+  // (i < 4; [43 + i - 4] for the others), [46 + i] FP64-X in the two-level
+  // layout with k2lInner[i] inner rows,
   // [22 + G - 4] certified int32-X with exact pairs of groups, [25 + 3 (G - 4)
   // + ngo - 1] int32-X in the two-level row layout, [34 + 3 family + ngo - 1]
   // certified int32-X in the two-level layout
-  int dense_occ[46][PERM_MAX_EXACT_N + 1] = {};
+  int dense_occ[50][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
@@ -610,7 +629,7 @@ struct DenseOperand {
   int n = 0, variant = PERM_KERNEL_DENSE, group = 0;
   int pair = 0;   // certified int32-X walk: consecutive groups multiplied in exact FP64 pairs
   int ngo = 0;    // int32-X walk: outer product groups of the two-level row layout (0: one level)
-  int inner = 0;  // split-dd: rows 0..inner-1 hold the support of columns 0..2 (0: dense layout)
+  int inner = 0;  // split-dd and FP64 X: rows 0..inner-1 hold the support of columns 0..2 (0: one level)
   std::vector<unsigned char> image;
 };
 
@@ -890,6 +909,20 @@ static bool int_two_level_layout(const std::vector<double>& a, int n, int g1, in
   return true;
 }
 
+// Inner-row count of the FP64-X walk's two-level layout (ryser_dense_2l.cuh;
+// 0: one level): the smallest of 16, 20, 24, 28 that holds the rows of the
+// three sparsest columns, orders 20..48, when the seven inner steps' 2R + 1
+// operations keep the 8-step cost 7 (2R + 1) + 2n within 0.85 of the
+// one-level walk's 16n (measured: n = 34 with 24 inner rows 29.6 against
+// 37.6 ms, n = 40 with 28, 2120 against 2773 ms).
+static int fp64_two_level_rows(const std::vector<double>& a, int n, int* c3) {
+  if (n < 20 || n > 48) return 0;
+  const int u = sparsest_column_triple(a, n, c3);
+  for (int r : k2lInner)
+    if (u <= r && r + 4 <= n) return 7 * (2 * r + 1) + 2 * n <= 0.85 * 16 * n ? r : 0;
+  return 0;
+}
+
 // Two-level row layout of the certified int32-X walk
 // (ryser_dense_intc_sparse.cuh): the permutation of int_two_level_layout,
 // with groups of 4 or 6 rows in int64 pairs or groups of 5 alone.  Per Gray
@@ -1019,6 +1052,15 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
     const int np = (n + 1) & ~1;
     op->variant = variant == PERM_KERNEL_DENSE_DD ? PERM_KERNEL_DENSE_DD : PERM_KERNEL_DENSE;
     op->group = 0;
+    op->inner = 0;
+    if (op->variant == PERM_KERNEL_DENSE) {
+      int c3[3];
+      const int r = fp64_two_level_rows(a, n, c3);
+      if (r) {
+        a = sparse_permutation(a.data(), n, c3);  // walk the permuted matrix (same permanent)
+        op->inner = r;
+      }
+    }
     op->image.assign(sizeof(double) * (size_t)n * np, 0);
     double* img = reinterpret_cast<double*>(op->image.data());
     for (int k = 0; k < n; k++)
@@ -1041,7 +1083,7 @@ static const void* operand_kernel(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
   if (op.variant == PERM_KERNEL_DENSE_SPLIT) return dense_split_kernel(op.n);
-  return dense_kernel(op.n);
+  return op.inner ? dense_2l_kernel(op.n, op.inner) : dense_kernel(op.n);
 }
 static int operand_threads(const DenseOperand& op) { return op.variant == PERM_KERNEL_DENSE_TC ? kTcThreads : 128; }
 static size_t operand_smem(const DenseOperand& op) {
@@ -1076,6 +1118,13 @@ static void shard_bounds(int n, int shard, int nshards, uint64_t* first, uint64_
   *first = (units * (uint64_t)shard / (uint64_t)nshards) << ms;
   *last = (units * (uint64_t)(shard + 1) / (uint64_t)nshards) << ms;
   if (ms_out) *ms_out = ms;
+}
+
+extern "C" int perm_fp64_layout(const double* mat, int n) {
+  if (!mat || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
+  std::vector<double> a(mat, mat + (size_t)n * n);
+  int c3[3];
+  return fp64_two_level_rows(a, n, c3);
 }
 
 extern "C" int perm_int_layout(const double* mat, int n, int* ngo) {
@@ -1132,6 +1181,9 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
   int sparse_slot = 0;
   for (int i = 0; i < 7; i++)
     if (op.inner == kSparseInner[i]) sparse_slot = i < 4 ? 18 + i : 43 + i - 4;
+  int fp_slot = 0;
+  for (int i = 0; i < 4; i++)
+    if (op.inner == k2lInner[i]) fp_slot = 46 + i;
   int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? (op.ngo ? 25 + 3 * (op.group - 4) + op.ngo - 1
                                                                               : op.group)
                                  : op.variant == PERM_KERNEL_DENSE_DD ? 7
@@ -1140,7 +1192,8 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
                                  : op.variant == PERM_KERNEL_DENSE_INT_DD
                                      ? (op.ngo ? 34 + 3 * intc_sparse_family(op.group, op.pair) + op.ngo - 1
                                                : op.pair ? 22 + op.group - 4 : 13 + op.group - 3)
-                                 : op.variant == PERM_KERNEL_DENSE_SDD ? (op.inner ? sparse_slot : 17) : 0][n];
+                                 : op.variant == PERM_KERNEL_DENSE_SDD ? (op.inner ? sparse_slot : 17)
+                                 : op.inner ? fp_slot : 0][n];
   if (!occ_slot) {
     int rc = allow_smem(ctx, fn, operand_smem(op));
     if (rc) return rc;

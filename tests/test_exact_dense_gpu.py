@@ -187,6 +187,28 @@ def test_int_kernel_two_level_layout_vs_exact(engine, orc, pb, n):
         res.free()
 
 
+@pytest.mark.parametrize("n", [22, 25, 28])
+def test_fp64_two_level_layout_vs_oracle(engine, orc, pb, n):
+    """The FP64-X walk in the two-level row layout on real density-1/2
+    matrices: against the CPU double-double Ryser within the walk's own
+    bound, and shards and a resident matrix of that layout add up to it."""
+    rng = np.random.default_rng(700 + n)
+    A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+    assert pb.fp64_layout(A) in (16, 20, 24, 28)
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE)
+    hi, lo = orc.perm_dd(A)
+    want = hi + lo
+    assert abs(r.value - want) <= r.rel_error_estimate * abs(want), (r.value, want, r.rel_error_estimate)
+    assert rel_err(r.value, want) < 1e-10
+    parts = [engine.exact_dense_shard(A, s, 3, variant=pb.PERM_KERNEL_DENSE) for s in range(3)]
+    assert rel_err(sum(p.hi + p.lo for p in parts), r.value) < 1e-12
+    res = engine.upload_dense(A, variant=pb.PERM_KERNEL_DENSE)
+    try:
+        assert res.run().value == r.value
+    finally:
+        res.free()
+
+
 def test_int_kernel_signed_entries(engine, orc, pb):
     rng = np.random.default_rng(17)
     A = rng.integers(-4, 5, (18, 18)).astype(float)

@@ -200,8 +200,9 @@ def test_fp64_two_level_layout_vs_oracle(engine, orc, pb, n):
     want = hi + lo
     assert abs(r.value - want) <= r.rel_error_estimate * abs(want), (r.value, want, r.rel_error_estimate)
     assert rel_err(r.value, want) < 1e-10
+    # shards re-anchor X at other indices: same bound, different roundings
     parts = [engine.exact_dense_shard(A, s, 3, variant=pb.PERM_KERNEL_DENSE) for s in range(3)]
-    assert rel_err(sum(p.hi + p.lo for p in parts), r.value) < 1e-12
+    assert abs(sum(p.hi + p.lo for p in parts) - r.value) <= 2 * r.rel_error_estimate * abs(r.value)
     res = engine.upload_dense(A, variant=pb.PERM_KERNEL_DENSE)
     try:
         assert res.run().value == r.value

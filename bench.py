@@ -206,7 +206,9 @@ def source_sha16(kname: str) -> str | None:
 def kernel_template(kname: str, A: np.ndarray) -> str:
     n = A.shape[0]
     if kname == "int32x":
-        g, ngo = (sys.modules.get("perman_b200") or load_pkg()).int_layout(A)
+        g, ngo, ng1, ng2 = (sys.modules.get("perman_b200") or load_pkg()).int_layout(A)
+        if ng1:
+            return f"ryser_dense_int_3l_kernel<{n}, {g}, {ng1}, {ng2}>"
         return f"ryser_dense_int_sparse_kernel<{n}, {g}, {ngo}>" if ngo else f"ryser_dense_int_kernel<{n}, {g}>"
     if kname == "int32x_dd":
         # product groups and pairing as the engine lays them out; last template

@@ -232,13 +232,19 @@ int perm_fp64_layout(const double* mat, int n);
 
 /* Host only (no device): the layout PERM_KERNEL_DENSE_INT (the int32-X walk)
  * uses for the row-major n x n matrix `mat`: returns the product-group size
- * G (3..6, every group's product fits int32) and sets *ngo to the number of
- * outer groups of the two-level row layout (orders 20..48: the three
- * columns whose nonzeros lie in the fewest rows go first, and *ngo groups of
- * the rows they never touch keep their product for seven of every eight Gray
- * steps), 0 for the one-level walk.  PERM_EUNSUPPORTED where int32 X does not
+ * G (3..6, every group's product fits int32) and fills levels[3]:
+ *  - levels[0] > 0: the two-level row layout (orders 20..48): the three
+ *    columns whose nonzeros lie in the fewest rows go first, and levels[0]
+ *    groups of the rows they never touch keep their product for seven of
+ *    every eight Gray steps;
+ *  - levels[1], levels[2] > 0: the three-level layout (orders 28..48): the
+ *    rows of column 0 (flipped at every other step) form levels[1] groups,
+ *    the further rows of columns 1 and 2 levels[2] groups, and each level's
+ *    product is recomputed only when a column that touches it flips;
+ *  - all 0: the one-level walk.
+ * The cheapest layout is taken.  PERM_EUNSUPPORTED where int32 X does not
  * apply, PERM_EINVAL for bad arguments.  No counterpart in the reference. */
-int perm_int_layout(const double* mat, int n, int* ngo);
+int perm_int_layout(const double* mat, int n, int* levels);
 
 /* Host only (no device): the layout PERM_KERNEL_DENSE_INT_DD uses for the
  * row-major n x n matrix `mat`: returns the product-group size G (3..6:

@@ -122,7 +122,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_shard_range": (i, [i, i, i, ctypes.POINTER(u64), ctypes.POINTER(u64)]),
         "perm_sdd_layout": (i, [_P, i]),
         "perm_intc_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
-        "perm_int_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int)]),
+        "perm_int_layout": (i, [_P, i, _P]),
         "perm_fp64_layout": (i, [_P, i]),
         "perm_exact_dense_plan": (i, [_P, _P, i, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
         "perm_matrix_create_dense_ex": (i, [_P, _P, i, i, i, ctypes.POINTER(_P)]),
@@ -624,15 +624,15 @@ def fp64_layout(mat) -> int:
     return int(load_library().perm_fp64_layout(_ptr(a), a.shape[0]))
 
 
-def int_layout(mat) -> tuple[int, int]:
-    """Product-group size G and number of outer groups of the two-level row
-    layout (0: one level) of the int32-X walk for this matrix
-    (perm_int_layout; host only); (negative status, 0) where int32 X does
-    not apply."""
+def int_layout(mat) -> tuple[int, int, int, int]:
+    """(G, outer groups of the two-level layout, first- and second-level
+    groups of the three-level layout) of the int32-X walk for this matrix
+    (perm_int_layout; host only): all zero beside G for the one-level walk;
+    (negative status, 0, 0, 0) where int32 X does not apply."""
     a = np.ascontiguousarray(mat, dtype=np.float64)
-    ngo = ctypes.c_int(0)
-    g = int(load_library().perm_int_layout(_ptr(a), a.shape[0], ctypes.byref(ngo)))
-    return g, ngo.value
+    lv = np.zeros(3, dtype=np.int32)
+    g = int(load_library().perm_int_layout(_ptr(a), a.shape[0], _ptr(lv)))
+    return g, int(lv[0]), int(lv[1]), int(lv[2])
 
 
 def intc_layout(mat) -> tuple[int, bool, int]:

@@ -81,6 +81,9 @@ const void* dense_intc_kernel_g3(int n);
 const void* dense_intc_kernel_g4(int n);
 const void* dense_intc_kernel_g5(int n);
 const void* dense_intc_kernel_g6(int n);
+const void* dense_int_3l_kernel_g4(int n, int ng1, int ng2);
+const void* dense_int_3l_kernel_g5(int n, int ng1, int ng2);
+const void* dense_int_3l_kernel_g6(int n, int ng1, int ng2);
 const void* dense_int_sparse_kernel_g4(int n, int ngo);
 const void* dense_int_sparse_kernel_g5(int n, int ngo);
 const void* dense_int_sparse_kernel_g6(int n, int ngo);
@@ -147,6 +150,18 @@ static const void* dense_intc_sparse_kernel(int n, int g, int pair, int ngo) {
     case 0: return dense_intc_sparse_kernel_g4p(n, ngo);
     case 1: return dense_intc_sparse_kernel_g5(n, ngo);
     case 2: return dense_intc_sparse_kernel_g6p(n, ngo);
+    default: return nullptr;
+  }
+}
+
+// int32-X walk in the three-level row layout: orders 28..48, groups of 4..6,
+// 2..4 groups on the first level (column 0), 1..2 on the second (columns 1, 2)
+constexpr int kInt3lMinN = 28;
+static const void* dense_int_3l_kernel(int n, int g, int ng1, int ng2) {
+  switch (g) {
+    case 4: return dense_int_3l_kernel_g4(n, ng1, ng2);
+    case 5: return dense_int_3l_kernel_g5(n, ng1, ng2);
+    case 6: return dense_int_3l_kernel_g6(n, ng1, ng2);
     default: return nullptr;
   }
 }
@@ -403,11 +418,12 @@ struct perm_ctx {
   // [8 + G - 3] tensor core, [12] split X, [13 + G - 3] certified int32-X,
   // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows
   // (i < 4; [43 + i - 4] for the others), [46 + i] FP64-X in the two-level
-  // layout with k2lInner[i] inner rows,
+  // layout with k2lInner[i] inner rows, [50 + 6 (G - 4) + 2 (ng1 - 2) + ng2 - 1]
+  // int32-X in the three-level layout,
   // [22 + G - 4] certified int32-X with exact pairs of groups, [25 + 3 (G - 4)
   // + ngo - 1] int32-X in the two-level row layout, [34 + 3 family + ngo - 1]
   // certified int32-X in the two-level layout
-  int dense_occ[50][PERM_MAX_EXACT_N + 1] = {};
+  int dense_occ[68][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
@@ -629,6 +645,7 @@ struct DenseOperand {
   int n = 0, variant = PERM_KERNEL_DENSE, group = 0;
   int pair = 0;   // certified int32-X walk: consecutive groups multiplied in exact FP64 pairs
   int ngo = 0;    // int32-X walk: outer product groups of the two-level row layout (0: one level)
+  int ng1 = 0, ng2 = 0;  // int32-X walk: groups of the three-level layout's first and second level (0: not)
   int inner = 0;  // split-dd and FP64 X: rows 0..inner-1 hold the support of columns 0..2 (0: one level)
   std::vector<unsigned char> image;
 };
@@ -909,6 +926,111 @@ static bool int_two_level_layout(const std::vector<double>& a, int n, int g1, in
   return true;
 }
 
+// Three-level row layout of the int32-X walk (ryser_dense_int_3l_kernel):
+// column 0 (flipped at every other Gray step) touches rows [0, R1) only,
+// columns 1 and 2 (three steps in eight) rows [0, R2) only, with
+// R1 = ng1 G and R2 = R1 + ng2 G; rows of a later level may fill an earlier
+// one (their zero entries there make the extra updates no-ops).  Per 8 steps
+// about 4 (2 R1 + 2 ng1) + 3 (2 R2 + 2 (ng1 + ng2) + 1) + 2n + 2 ceil(n/G)
+// instructions.  Searches every column for level 1 and every pair for
+// level 2 (orders 28..48, G in 4..6 up to the one-level G, ng1 in 2..4,
+// ng2 in 1..2) and returns the cheapest layout below `best_cost` whose
+// groups provably fit int32, with the permuted matrix in *perm.
+static bool int_three_level_layout(const std::vector<double>& a, int n, int g1, long best_cost, int* g_out,
+                                   int* ng1_out, int* ng2_out, std::vector<double>* perm) {
+  if (n < kInt3lMinN || n > kIntSparseMaxN || g1 < 4) return false;
+  std::vector<uint64_t> sup(n, 0);
+  for (int j = 0; j < n; j++)
+    for (int k = 0; k < n; k++)
+      if (a[(size_t)j * n + k] != 0.0) sup[k] |= 1ull << j;
+  long best = best_cost;
+  int bc[3] = {0, 0, 0}, bg = 0, b1 = 0, b2 = 0;
+  for (int g = std::min(g1, 6); g >= 4; g--) {
+    for (int c0 = 0; c0 < n; c0++) {
+      const int ng1 = std::max(2, (__builtin_popcountll(sup[c0]) + g - 1) / g);
+      if (ng1 > 4) continue;
+      for (int c1 = 0; c1 < n; c1++) {
+        if (c1 == c0) continue;
+        for (int c2 = c1 + 1; c2 < n; c2++) {
+          if (c2 == c0) continue;
+          const int u = __builtin_popcountll(sup[c0] | sup[c1] | sup[c2]);
+          const int ng2 = std::max(1, (u - ng1 * g + g - 1) / g);
+          if (ng2 > 2 || (ng1 + ng2) * g + 2 > n) continue;
+          const int r1 = ng1 * g, r2 = r1 + ng2 * g;
+          const long cost = 4L * (2 * r1 + 2 * ng1) + 3L * (2 * r2 + 2 * (ng1 + ng2) + 1) + 2 * n + 2 * ((n + g - 1) / g);
+          if (cost < best) {
+            best = cost;
+            bc[0] = c0, bc[1] = c1, bc[2] = c2, bg = g, b1 = ng1, b2 = ng2;
+          }
+        }
+      }
+    }
+  }
+  if (best == best_cost) return false;
+  // rows: level 1 = support of column c0, filled up to R1 with rows of the
+  // other two columns' support, then of the rest; level 2 likewise to R2
+  const int r1 = b1 * bg, r2 = r1 + b2 * bg;
+  const uint64_t s0 = sup[bc[0]], s12 = sup[bc[1]] | sup[bc[2]];
+  std::vector<int> rows, pool;
+  for (int j = 0; j < n; j++)
+    if ((s0 >> j) & 1) rows.push_back(j);
+  for (int j = 0; j < n; j++)
+    if (!((s0 >> j) & 1) && ((s12 >> j) & 1)) pool.push_back(j);
+  for (int j = 0; j < n; j++)
+    if (!(((s0 | s12) >> j) & 1)) pool.push_back(j);
+  size_t pi = 0;
+  while ((int)rows.size() < r1) rows.push_back(pool[pi++]);
+  while ((int)rows.size() < r2) rows.push_back(pool[pi++]);
+  while (pi < pool.size()) rows.push_back(pool[pi++]);
+  // every row of columns 1, 2 must be in [0, R2): guaranteed when the
+  // support of columns 0..2 fits R2 rows
+  if (__builtin_popcountll(s0 | s12) > r2) return false;
+  std::vector<int> cols = {bc[0], bc[1], bc[2]};
+  for (int k = 0; k < n; k++)
+    if (k != bc[0] && k != bc[1] && k != bc[2]) cols.push_back(k);
+  std::vector<double> p((size_t)n * n);
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < n; k++) p[(size_t)i * n + k] = a[(size_t)rows[i] * n + cols[k]];
+  std::vector<double> rowabs;
+  if (!int_row_abs(p, n, rowabs)) return false;
+  for (int j0 = 0; j0 < n; j0 += bg) {  // every group of bg rows (levels are multiples of bg)
+    double b = 1.0;
+    for (int j = j0; j < std::min(j0 + bg, n); j++) b *= std::max(rowabs[j], 1.0);
+    if (!(b < 2147483648.0)) return false;
+  }
+  *g_out = bg;
+  *ng1_out = b1;
+  *ng2_out = b2;
+  *perm = std::move(p);
+  return true;
+}
+
+// Layout of the int32-X walk with product groups of G (int_group_size): one
+// level, two levels (int_two_level_layout) or three (int_three_level_layout),
+// whichever costs least; *perm receives the permuted matrix of the two- and
+// three-level layouts.
+struct IntLayout {
+  int g, ngo, ng1, ng2;
+};
+static IntLayout choose_int_layout(const std::vector<double>& a, int n, int G, std::vector<double>* perm) {
+  IntLayout l = {G, 0, 0, 0};
+  long cost = 8L * (2 * n + (n + G - 1) / G);
+  int g2 = G, ngo2 = 0, g3 = G, a1 = 0, a2 = 0;
+  std::vector<double> two, three;
+  if (int_two_level_layout(a, n, G, &g2, &ngo2, &two)) {
+    const int ri = n - g2 * ngo2;
+    cost = 7L * (2 * ri + (ri + g2 - 1) / g2 + 1) + 2 * n + (n + g2 - 1) / g2 + ngo2;
+  }
+  if (int_three_level_layout(a, n, G, cost, &g3, &a1, &a2, &three)) {
+    l = {g3, 0, a1, a2};
+    *perm = std::move(three);
+  } else if (ngo2) {
+    l = {g2, ngo2, 0, 0};
+    *perm = std::move(two);
+  }
+  return l;
+}
+
 // Inner-row count of the FP64-X walk's two-level layout (ryser_dense_2l.cuh;
 // 0: one level): the smallest of 16, 20, 24, 28 that holds the rows of the
 // three sparsest columns, orders 20..48, when the seven inner steps' 2R + 1
@@ -1029,6 +1151,7 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
     op->group = G;
     op->pair = 0;
     op->ngo = 0;
+    op->ng1 = op->ng2 = 0;
     std::vector<double> two;
     if (op->variant == PERM_KERNEL_DENSE_INT_DD) {
       int cost1 = 0;
@@ -1036,8 +1159,14 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
       if (intc_two_level_layout(a, n, 8L * (n + cost1), &op->group, &op->pair, &op->ngo, &two))
         a.swap(two);  // walk the permuted matrix (same permanent)
     }
-    if (op->variant == PERM_KERNEL_DENSE_INT && int_two_level_layout(a, n, G, &op->group, &op->ngo, &two))
-      a.swap(two);
+    if (op->variant == PERM_KERNEL_DENSE_INT) {
+      const IntLayout l = choose_int_layout(a, n, G, &two);
+      op->group = l.g;
+      op->ngo = l.ngo;
+      op->ng1 = l.ng1;
+      op->ng2 = l.ng2;
+      if (l.ngo || l.ng1) a.swap(two);  // walk the permuted matrix (same permanent)
+    }
     op->image.assign(sizeof(int) * (size_t)(n + 1) * np4, 0);
     int* img = reinterpret_cast<int*>(op->image.data());
     for (int k = 0; k < n; k++)
@@ -1076,7 +1205,9 @@ struct perm_matrix {
 
 static const void* operand_kernel(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_INT)
-    return op.ngo ? dense_int_sparse_kernel(op.n, op.group, op.ngo) : dense_int_kernel(op.n, op.group);
+    return op.ng1 ? dense_int_3l_kernel(op.n, op.group, op.ng1, op.ng2)
+           : op.ngo ? dense_int_sparse_kernel(op.n, op.group, op.ngo)
+                    : dense_int_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_INT_DD)
     return op.ngo ? dense_intc_sparse_kernel(op.n, op.group, op.pair, op.ngo) : dense_intc_kernel(op.n, op.group, op.pair);
   if (op.variant == PERM_KERNEL_DENSE_SDD) return sdd_kernel(op.n, op.inner);
@@ -1127,19 +1258,18 @@ extern "C" int perm_fp64_layout(const double* mat, int n) {
   return fp64_two_level_rows(a, n, c3);
 }
 
-extern "C" int perm_int_layout(const double* mat, int n, int* ngo) {
-  if (!mat || !ngo || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
+extern "C" int perm_int_layout(const double* mat, int n, int* levels) {
+  if (!mat || !levels || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
   std::vector<double> a(mat, mat + (size_t)n * n);
-  *ngo = 0;
-  int g = int_group_size(a, n);
+  levels[0] = levels[1] = levels[2] = 0;
+  const int g = int_group_size(a, n);
   if (!g) return PERM_EUNSUPPORTED;
-  std::vector<double> two;
-  int g2 = g, ngo2 = 0;
-  if (int_two_level_layout(a, n, g, &g2, &ngo2, &two)) {
-    g = g2;
-    *ngo = ngo2;
-  }
-  return g;
+  std::vector<double> perm;
+  const IntLayout l = choose_int_layout(a, n, g, &perm);
+  levels[0] = l.ngo;
+  levels[1] = l.ng1;
+  levels[2] = l.ng2;
+  return l.g;
 }
 
 extern "C" int perm_intc_layout(const double* mat, int n, int* pair, int* ngo) {
@@ -1184,8 +1314,10 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
   int fp_slot = 0;
   for (int i = 0; i < 4; i++)
     if (op.inner == k2lInner[i]) fp_slot = 46 + i;
-  int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT ? (op.ngo ? 25 + 3 * (op.group - 4) + op.ngo - 1
-                                                                              : op.group)
+  int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT
+                                     ? (op.ng1 ? 50 + 6 * (op.group - 4) + 2 * (op.ng1 - 2) + op.ng2 - 1
+                                        : op.ngo ? 25 + 3 * (op.group - 4) + op.ngo - 1
+                                                 : op.group)
                                  : op.variant == PERM_KERNEL_DENSE_DD ? 7
                                  : op.variant == PERM_KERNEL_DENSE_TC ? 8 + op.group - 3
                                  : op.variant == PERM_KERNEL_DENSE_SPLIT ? 12

@@ -189,4 +189,125 @@ __global__ void __launch_bounds__(128) ryser_dense_int_sparse_kernel(DenseIntArg
   grid_finish_dd(bt, args.partials, args.ticket, args.out, factor, red);
 }
 
+// Three-level row layout: column 0 (flipped at every other Gray step)
+// touches rows [0, R1) only, columns 1 and 2 (three steps in eight) rows
+// [0, R2) only, R1 = NG1 G and R2 = R1 + NG2 G; the host permutes the matrix
+// accordingly (rows of a later level may sit in an earlier one: their zero
+// entries make the extra updates no-ops).  Column-0 steps update R1 rows and
+// multiply their NG1 groups by P23 = P2 P_out; column-1/2 steps update R2
+// rows and recompute P1, P2 and P23; the other step of each eight updates
+// every row and recomputes P_out too.  Terms keep ceil(N/G) FP64 factors
+// combined by ceil(N/G) - 1 multiplies.
+template <int N, int J0, int J1, int G>
+__device__ __forceinline__ double level_product(const int (&y)[N]) {
+  constexpr int NG = (J1 - J0 + G - 1) / G;
+  double p = 1.0;
+#pragma unroll
+  for (int g = 0; g < NG; g++) {
+    const int a = J0 + g * G;
+    uint32_t pr = (uint32_t)y[a];
+#pragma unroll
+    for (int t = 1; t < G; t++)
+      if (a + t < J1) pr = pr * (uint32_t)y[a + t];
+    const double d = __int2double_rn((int)pr);
+    p = g == 0 ? d : p * d;
+  }
+  return p;
+}
+
+template <int N, int G, int NG1, int NG2>
+__global__ void __launch_bounds__(128) ryser_dense_int_3l_kernel(DenseIntArgs args) {
+  constexpr int R1 = NG1 * G, R2 = R1 + NG2 * G;
+  static_assert(NG1 >= 1 && NG2 >= 1 && R2 + 2 <= N, "levels must leave outer rows");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int np4 = args.np4;
+  int* sC = reinterpret_cast<int*>(smem_raw);  // [N][np4] columns, then y0
+  dd* red = reinterpret_cast<dd*>(sC + (size_t)(N + 1) * np4);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(red + 32);
+  const bool staged = stage_to_smem(sC, args.colI, (uint32_t)(sizeof(int) * (N + 1) * np4), bar, args.err);
+  const int* sY0 = sC + (size_t)N * np4;
+
+  Acc acc;
+  const uint64_t TT = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t q = args.nblocks / TT, r = args.nblocks % TT;
+  const uint64_t b0 = q * tid + (r * tid) / TT;
+  const uint64_t b1 = q * (tid + 1) + (r * (tid + 1)) / TT;
+
+  if (staged && b1 > b0) {
+    const uint64_t s0 = (args.block0 + b0) << args.m, e0 = (args.block0 + b1) << args.m;
+    int y[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) y[j] = sY0[j];
+    const uint64_t g = s0 ^ (s0 >> 1);
+#pragma unroll 1
+    for (int k = 0; k < N - 1; k++) {
+      if ((g >> k) & 1) {
+#pragma unroll
+        for (int j = 0; j < N; j++) y[j] += sC[k * np4 + j];
+      }
+    }
+    double pout = level_product<N, R2, N, G>(y);
+    double p23 = level_product<N, R1, R2, G>(y) * pout;
+    acc.add(level_product<N, 0, R1, G>(y) * p23);
+
+    const int* c0 = sC;
+    const int* c1 = sC + np4;
+    const int* c2 = sC + 2 * np4;
+    const uint64_t groups = (e0 - s0) >> 3;
+    uint64_t base = s0;
+    // column-0 step: level 1 only; column-1/2 step: levels 1 and 2
+    auto step0 = [&](int sg) {
+      if (sg > 0)
+        iupdate_rows<N, R1, +1>(y, c0, 0);
+      else
+        iupdate_rows<N, R1, -1>(y, c0, 0);
+      return level_product<N, 0, R1, G>(y) * p23;
+    };
+    auto step12 = [&](const int* c, int sg, bool known, int ks) {
+      if (known && ks > 0)
+        iupdate_rows<N, R2, +1>(y, c, 0);
+      else if (known)
+        iupdate_rows<N, R2, -1>(y, c, 0);
+      else
+        iupdate_rows<N, R2, 0>(y, c, sg);
+      p23 = level_product<N, R1, R2, G>(y) * pout;
+      return level_product<N, 0, R1, G>(y) * p23;
+    };
+    auto seven = [&](int s4, double (&t)[7]) {
+      t[0] = step0(+1);
+      t[1] = step12(c1, 1, true, +1);
+      t[2] = step0(-1);
+      t[3] = step12(c2, s4, false, 0);
+      t[4] = step0(+1);
+      t[5] = step12(c1, -1, true, -1);
+      t[6] = step0(-1);
+    };
+#pragma unroll 1
+    for (uint64_t gi = 0; gi + 1 < groups; gi++, base += 8) {
+      const int s4 = ((base >> 3) & 1) ? -1 : 1;
+      const uint64_t i8 = base + 8;
+      const int k8 = __ffsll((long long)i8) - 1;
+      const int s8 = ((i8 >> (k8 + 1)) & 1) ? -1 : 1;
+      double t[7];
+      seven(s4, t);
+      iupdate_rows<N, N, 0>(y, sC + k8 * np4, s8);
+      pout = level_product<N, R2, N, G>(y);
+      p23 = level_product<N, R1, R2, G>(y) * pout;
+      const double t8 = level_product<N, 0, R1, G>(y) * p23;
+      acc.add(((t[1] - t[0]) + (t[3] - t[2])) + ((t[5] - t[4]) + (t8 - t[6])));
+    }
+    {
+      const int s4 = ((base >> 3) & 1) ? -1 : 1;
+      double t[7];
+      seven(s4, t);
+      acc.add(((t[1] - t[0]) + (t[3] - t[2])) + ((t[5] - t[4]) - t[6]));
+    }
+  }
+
+  dd bt = block_reduce_dd(acc.value(), red);
+  const double factor = ((N & 1) ? 2.0 : -2.0) * ldexp(1.0, -N);
+  grid_finish_dd(bt, args.partials, args.ticket, args.out, factor, red);
+}
+
 }  // namespace perm

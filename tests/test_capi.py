@@ -77,16 +77,16 @@ def test_header_constants_match_the_binding(pb):
 
 def test_int_layout_query(pb):
     """Host-only layout of the int32-X walk: the order-40 bench matrix walks
-    in the two-level row layout with three outer groups of 5 rows (its three
-    sparsest columns touch 25 of 40 rows); small orders keep one level;
-    non-integer matrices are refused."""
+    in the three-level row layout (column 0's rows in 3 groups of 5, the
+    further rows of columns 1 and 2 in 2 more); order 24 takes two levels;
+    small orders keep one level; non-integer matrices are refused."""
     import bench
 
-    assert pb.int_layout(bench.make_matrix(0)) == (5, 3)
+    assert pb.int_layout(bench.make_matrix(0)) == (5, 0, 3, 2)
     rng = np.random.default_rng(4)
-    assert pb.int_layout((rng.random((16, 16)) < 0.5).astype(float))[1] == 0
-    g, ngo = pb.int_layout((rng.random((30, 30)) < 0.5) * rng.integers(1, 5, (30, 30)).astype(float))
-    assert g in (4, 5, 6) and ngo in (1, 2, 3)
+    assert pb.int_layout((rng.random((16, 16)) < 0.5).astype(float))[1:] == (0, 0, 0)
+    g, ngo, ng1, ng2 = pb.int_layout((rng.random((24, 24)) < 0.5) * rng.integers(1, 5, (24, 24)).astype(float))
+    assert g in (4, 5, 6) and ngo in (1, 2, 3) and ng1 == ng2 == 0
     assert pb.int_layout(rng.random((20, 20)))[0] == pb.PERM_EUNSUPPORTED
 
 

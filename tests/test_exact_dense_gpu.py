@@ -170,7 +170,7 @@ def test_int_kernel_two_level_layout_vs_exact(engine, orc, pb, n):
              "binary": bernoulli(rng, n, 0.5),
              "signed": bernoulli(rng, n, 0.5) * rng.integers(-3, 4, (n, n))}
     for kind, A in cases.items():
-        g, ngo = pb.int_layout(A)
+        g, ngo, _, _ = pb.int_layout(A)
         assert ngo >= 1, (kind, g, ngo)
         exact = orc.perm_exact_int(A)[0]
         r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
@@ -208,6 +208,20 @@ def test_fp64_two_level_layout_vs_oracle(engine, orc, pb, n):
         assert res.run().value == r.value
     finally:
         res.free()
+
+
+@pytest.mark.parametrize("n", [28, 30])
+def test_int_kernel_three_level_layout_vs_exact(engine, orc, pb, n):
+    """The int32-X walk in the three-level row layout (column 0's rows, the
+    further rows of columns 1 and 2, the rest) against the exact
+    multi-modular oracle on dense U{1..4} and 0/1 matrices."""
+    rng = np.random.default_rng(650 + n)
+    for kind, A in (("u1to4", bernoulli(rng, n, 0.5) * rng.integers(1, 5, (n, n))), ("binary", bernoulli(rng, n, 0.5))):
+        g, ngo, ng1, ng2 = pb.int_layout(A)
+        assert ng1 >= 2 and ng2 >= 1, (kind, g, ngo, ng1, ng2)
+        exact = orc.perm_exact_int(A)[0]
+        r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT)
+        assert rel_err(r.value, exact) < 1e-12, (kind, r.value, exact)
 
 
 def test_int_kernel_signed_entries(engine, orc, pb):

@@ -926,51 +926,48 @@ static bool int_two_level_layout(const std::vector<double>& a, int n, int g1, in
   return true;
 }
 
-// Three-level row layout of the int32-X walk (ryser_dense_int_3l_kernel):
-// column 0 (flipped at every other Gray step) touches rows [0, R1) only,
-// columns 1 and 2 (three steps in eight) rows [0, R2) only, with
-// R1 = ng1 G and R2 = R1 + ng2 G; rows of a later level may fill an earlier
-// one (their zero entries there make the extra updates no-ops).  Per 8 steps
-// about 4 (2 R1 + 2 ng1) + 3 (2 R2 + 2 (ng1 + ng2) + 1) + 2n + 2 ceil(n/G)
-// instructions.  Searches every column for level 1 and every pair for
-// level 2 (orders 28..48, G in 4..6 up to the one-level G, ng1 in 2..4,
-// ng2 in 1..2) and returns the cheapest layout below `best_cost` whose
-// groups provably fit int32, with the permuted matrix in *perm.
-static bool int_three_level_layout(const std::vector<double>& a, int n, int g1, long best_cost, int* g_out,
-                                   int* ng1_out, int* ng2_out, std::vector<double>* perm) {
-  if (n < kInt3lMinN || n > kIntSparseMaxN || g1 < 4) return false;
+// Three-level row layout (ryser_dense_int_3l_kernel,
+// ryser_dense_intc_3l_kernel): column 0 (flipped at every other Gray step)
+// touches rows [0, R1) only, columns 1 and 2 (three steps in eight) rows
+// [0, R2) only, with R1 = ng1 g and R2 = R1 + ng2 g; rows of a later level
+// may fill an earlier one (their zero entries there make the extra updates
+// no-ops).  For product groups of g rows, searches every column for column
+// 0 and every pair for columns 1, 2 (orders 28..48, ng1 in 2..4, ng2 in
+// 1..2) for the fewest rows updated per 8 steps, 4 R1 + 3 R2, and returns
+// the permuted matrix; false when no layout fits.
+static bool three_level_permutation(const std::vector<double>& a, int n, int g, int* ng1_out, int* ng2_out,
+                                    std::vector<double>* perm) {
+  if (n < kInt3lMinN || n > kIntSparseMaxN) return false;
   std::vector<uint64_t> sup(n, 0);
   for (int j = 0; j < n; j++)
     for (int k = 0; k < n; k++)
       if (a[(size_t)j * n + k] != 0.0) sup[k] |= 1ull << j;
-  long best = best_cost;
-  int bc[3] = {0, 0, 0}, bg = 0, b1 = 0, b2 = 0;
-  for (int g = std::min(g1, 6); g >= 4; g--) {
-    for (int c0 = 0; c0 < n; c0++) {
-      const int ng1 = std::max(2, (__builtin_popcountll(sup[c0]) + g - 1) / g);
-      if (ng1 > 4) continue;
-      for (int c1 = 0; c1 < n; c1++) {
-        if (c1 == c0) continue;
-        for (int c2 = c1 + 1; c2 < n; c2++) {
-          if (c2 == c0) continue;
-          const int u = __builtin_popcountll(sup[c0] | sup[c1] | sup[c2]);
-          const int ng2 = std::max(1, (u - ng1 * g + g - 1) / g);
-          if (ng2 > 2 || (ng1 + ng2) * g + 2 > n) continue;
-          const int r1 = ng1 * g, r2 = r1 + ng2 * g;
-          const long cost = 4L * (2 * r1 + 2 * ng1) + 3L * (2 * r2 + 2 * (ng1 + ng2) + 1) + 2 * n + 2 * ((n + g - 1) / g);
-          if (cost < best) {
-            best = cost;
-            bc[0] = c0, bc[1] = c1, bc[2] = c2, bg = g, b1 = ng1, b2 = ng2;
-          }
+  long best = -1;
+  int bc[3] = {0, 0, 0}, b1 = 0, b2 = 0;
+  for (int c0 = 0; c0 < n; c0++) {
+    const int ng1 = std::max(2, (__builtin_popcountll(sup[c0]) + g - 1) / g);
+    if (ng1 > 4) continue;
+    for (int c1 = 0; c1 < n; c1++) {
+      if (c1 == c0) continue;
+      for (int c2 = c1 + 1; c2 < n; c2++) {
+        if (c2 == c0) continue;
+        const int u = __builtin_popcountll(sup[c0] | sup[c1] | sup[c2]);
+        const int ng2 = std::max(1, (u - ng1 * g + g - 1) / g);
+        if (ng2 > 2 || (ng1 + ng2) * g + 2 > n) continue;
+        const long rows = 4L * ng1 * g + 3L * (ng1 + ng2) * g;
+        if (best < 0 || rows < best) {
+          best = rows;
+          bc[0] = c0, bc[1] = c1, bc[2] = c2, b1 = ng1, b2 = ng2;
         }
       }
     }
   }
-  if (best == best_cost) return false;
+  if (best < 0) return false;
+  const int r1 = b1 * g, r2 = r1 + b2 * g;
+  const uint64_t s0 = sup[bc[0]], s12 = sup[bc[1]] | sup[bc[2]];
+  if (__builtin_popcountll(s0 | s12) > r2) return false;
   // rows: level 1 = support of column c0, filled up to R1 with rows of the
   // other two columns' support, then of the rest; level 2 likewise to R2
-  const int r1 = b1 * bg, r2 = r1 + b2 * bg;
-  const uint64_t s0 = sup[bc[0]], s12 = sup[bc[1]] | sup[bc[2]];
   std::vector<int> rows, pool;
   for (int j = 0; j < n; j++)
     if ((s0 >> j) & 1) rows.push_back(j);
@@ -979,30 +976,44 @@ static bool int_three_level_layout(const std::vector<double>& a, int n, int g1, 
   for (int j = 0; j < n; j++)
     if (!(((s0 | s12) >> j) & 1)) pool.push_back(j);
   size_t pi = 0;
-  while ((int)rows.size() < r1) rows.push_back(pool[pi++]);
   while ((int)rows.size() < r2) rows.push_back(pool[pi++]);
   while (pi < pool.size()) rows.push_back(pool[pi++]);
-  // every row of columns 1, 2 must be in [0, R2): guaranteed when the
-  // support of columns 0..2 fits R2 rows
-  if (__builtin_popcountll(s0 | s12) > r2) return false;
   std::vector<int> cols = {bc[0], bc[1], bc[2]};
   for (int k = 0; k < n; k++)
     if (k != bc[0] && k != bc[1] && k != bc[2]) cols.push_back(k);
   std::vector<double> p((size_t)n * n);
   for (int i = 0; i < n; i++)
     for (int k = 0; k < n; k++) p[(size_t)i * n + k] = a[(size_t)rows[i] * n + cols[k]];
-  std::vector<double> rowabs;
-  if (!int_row_abs(p, n, rowabs)) return false;
-  for (int j0 = 0; j0 < n; j0 += bg) {  // every group of bg rows (levels are multiples of bg)
-    double b = 1.0;
-    for (int j = j0; j < std::min(j0 + bg, n); j++) b *= std::max(rowabs[j], 1.0);
-    if (!(b < 2147483648.0)) return false;
-  }
-  *g_out = bg;
   *ng1_out = b1;
   *ng2_out = b2;
   *perm = std::move(p);
   return true;
+}
+
+// Three-level layout of the int32-X walk: per 8 steps about
+// 4 (2 R1 + 2 ng1) + 3 (2 R2 + 2 (ng1 + ng2) + 1) + 2n + 2 ceil(n/G)
+// instructions; G in 4..6 up to the one-level G; the cheapest layout below
+// `best_cost` whose groups provably fit int32.
+static bool int_three_level_layout(const std::vector<double>& a, int n, int g1, long best_cost, int* g_out,
+                                   int* ng1_out, int* ng2_out, std::vector<double>* perm) {
+  if (g1 < 4) return false;
+  long best = best_cost;
+  for (int g = std::min(g1, 6); g >= 4; g--) {
+    int ng1 = 0, ng2 = 0;
+    std::vector<double> p;
+    if (!three_level_permutation(a, n, g, &ng1, &ng2, &p)) continue;
+    const int r1 = ng1 * g, r2 = r1 + ng2 * g;
+    const long cost = 4L * (2 * r1 + 2 * ng1) + 3L * (2 * r2 + 2 * (ng1 + ng2) + 1) + 2 * n + 2 * ((n + g - 1) / g);
+    if (cost >= best) continue;
+    std::vector<double> rowabs;
+    if (!int_row_abs(p, n, rowabs) || !runs_fit(rowabs, n, g, 2147483648.0)) continue;
+    best = cost;
+    *g_out = g;
+    *ng1_out = ng1;
+    *ng2_out = ng2;
+    *perm = std::move(p);
+  }
+  return best != best_cost;
 }
 
 // Layout of the int32-X walk with product groups of G (int_group_size): one

@@ -213,8 +213,10 @@ def kernel_template(kname: str, A: np.ndarray) -> str:
     if kname == "int32x_dd":
         # product groups and pairing as the engine lays them out; last template
         # argument: CTAs per SM compiled for (3 up to order 36, 2 above)
-        g, pair, ngo = (sys.modules.get("perman_b200") or load_pkg()).intc_layout(A)
+        g, pair, ngo, ng1, ng2 = (sys.modules.get("perman_b200") or load_pkg()).intc_layout(A)
         pb_ = "true" if pair else "false"
+        if ng1:
+            return f"ryser_dense_intc_3l_kernel<{n}, {g}, {pb_}, {ng1}, {ng2}, {3 if n <= 40 else 2}>"
         if ngo:
             return f"ryser_dense_intc_sparse_kernel<{n}, {g}, {pb_}, {ngo}, {3 if n <= 36 else 2}>"
         return f"ryser_dense_intc_kernel<{n}, {g}, {pb_}, {3 if n <= 36 else 2}>"

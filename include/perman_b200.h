@@ -252,13 +252,14 @@ int perm_int_layout(const double* mat, int n, int* levels);
  * exact int32 products) and sets *pair to 1 when consecutive group values
  * are multiplied in int64 first (every run of 2G rows below 2^53, so those
  * products are exact; orders >= 16), 0 otherwise; the layout with the
- * fewest instructions per Gray step is taken.  *ngo receives the number of
- * outer groups of the two-level row layout (orders 20..48, as
- * perm_int_layout: groups of 4 or 6 in pairs, or 5 alone), 0 for one level.
- * PERM_EUNSUPPORTED for non-integer matrices, |a| >= 2^24, orders below 8
- * or no fitting G; PERM_EINVAL for bad arguments.  No counterpart in the
- * reference. */
-int perm_intc_layout(const double* mat, int n, int* pair, int* ngo);
+ * fewest instructions per Gray step is taken.  levels[0] receives the
+ * number of outer groups of the two-level row layout (orders 20..48, as
+ * perm_int_layout: groups of 4 or 6 in pairs, or 5 alone), levels[1] and
+ * levels[2] the first- and second-level groups of the three-level layout
+ * (orders 28..48); all three 0 for one level.  PERM_EUNSUPPORTED for
+ * non-integer matrices, |a| >= 2^24, orders below 8 or no fitting G;
+ * PERM_EINVAL for bad arguments.  No counterpart in the reference. */
+int perm_intc_layout(const double* mat, int n, int* pair, int* levels);
 
 /* Measures, for orders n_lo..n_hi (within 8..40), which of the int32-X, the
  * FP64-X and (n >= 16) the tensor-core kernel is fastest on this device for

@@ -121,7 +121,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_exact_dense_ex": (i, [_P, _P, i, i, i, i, i, ctypes.POINTER(PermResult)]),
         "perm_shard_range": (i, [i, i, i, ctypes.POINTER(u64), ctypes.POINTER(u64)]),
         "perm_sdd_layout": (i, [_P, i]),
-        "perm_intc_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+        "perm_intc_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int), _P]),
         "perm_int_layout": (i, [_P, i, _P]),
         "perm_fp64_layout": (i, [_P, i]),
         "perm_exact_dense_plan": (i, [_P, _P, i, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
@@ -635,15 +635,17 @@ def int_layout(mat) -> tuple[int, int, int, int]:
     return g, int(lv[0]), int(lv[1]), int(lv[2])
 
 
-def intc_layout(mat) -> tuple[int, bool, int]:
-    """Product-group size G, exact int64 pairing and number of outer groups
-    of the two-level row layout (0: one level) of the certified int32-X walk
-    for this matrix (perm_intc_layout; host only); (negative status, False, 0)
+def intc_layout(mat) -> tuple[int, bool, int, int, int]:
+    """(G, exact int64 pairing, outer groups of the two-level layout, first-
+    and second-level groups of the three-level layout) of the certified
+    int32-X walk for this matrix (perm_intc_layout; host only): the last
+    three zero for the one-level walk; (negative status, False, 0, 0, 0)
     where the kernel does not apply."""
     a = np.ascontiguousarray(mat, dtype=np.float64)
-    pair, ngo = ctypes.c_int(0), ctypes.c_int(0)
-    g = int(load_library().perm_intc_layout(_ptr(a), a.shape[0], ctypes.byref(pair), ctypes.byref(ngo)))
-    return g, bool(pair.value), ngo.value
+    pair = ctypes.c_int(0)
+    lv = np.zeros(3, dtype=np.int32)
+    g = int(load_library().perm_intc_layout(_ptr(a), a.shape[0], ctypes.byref(pair), _ptr(lv)))
+    return g, bool(pair.value), int(lv[0]), int(lv[1]), int(lv[2])
 
 
 def shard_range(n: int, shard: int, nshards: int) -> tuple[int, int]:

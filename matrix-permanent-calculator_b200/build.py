@@ -34,7 +34,8 @@ LIB_SOURCES = [
     "ryser_dense_inst_3.cu", "ryser_dense_inst_4.cu", "ryser_dense_2l_inst_0.cu", "ryser_dense_2l_inst_1.cu", "ryser_dense_int_g3.cu", "ryser_dense_int_g4.cu",
     "ryser_dense_int_g5.cu", "ryser_dense_int_g6.cu", "ryser_dense_int_sparse_g4.cu", "ryser_dense_int_sparse_g5.cu",
     "ryser_dense_int_sparse_g6.cu", "ryser_dense_int_3l_g4.cu", "ryser_dense_int_3l_g5.cu", "ryser_dense_int_3l_g6.cu", "ryser_dense_intc_sparse_g4p.cu", "ryser_dense_intc_sparse_g5.cu",
-    "ryser_dense_intc_sparse_g6p.cu", "ryser_dense_dd_inst.cu", "matrix_io.cpp",
+    "ryser_dense_intc_sparse_g6p.cu", "ryser_dense_intc_3l_g4p.cu", "ryser_dense_intc_3l_g5.cu",
+    "ryser_dense_intc_3l_g6p.cu", "ryser_dense_dd_inst.cu", "matrix_io.cpp",
     "ryser_dense_tc_g3.cu", "ryser_dense_tc_g4.cu", "ryser_dense_tc_g5.cu", "ryser_dense_tc_g6.cu",
     "ryser_dense_split_inst.cu", "ryser_dense_intc_g3.cu", "ryser_dense_intc_g4.cu", "ryser_dense_intc_g5.cu",
     "ryser_dense_intc_g6.cu", "ryser_dense_intc_p4.cu", "ryser_dense_intc_p5.cu", "ryser_dense_intc_p6.cu",

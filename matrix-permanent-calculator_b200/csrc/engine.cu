@@ -87,6 +87,9 @@ const void* dense_int_3l_kernel_g6(int n, int ng1, int ng2);
 const void* dense_int_sparse_kernel_g4(int n, int ngo);
 const void* dense_int_sparse_kernel_g5(int n, int ngo);
 const void* dense_int_sparse_kernel_g6(int n, int ngo);
+const void* dense_intc_3l_kernel_g4p(int n, int ng1, int ng2);
+const void* dense_intc_3l_kernel_g5(int n, int ng1, int ng2);
+const void* dense_intc_3l_kernel_g6p(int n, int ng1, int ng2);
 const void* dense_intc_sparse_kernel_g4p(int n, int ngo);
 const void* dense_intc_sparse_kernel_g5(int n, int ngo);
 const void* dense_intc_sparse_kernel_g6p(int n, int ngo);
@@ -162,6 +165,15 @@ static const void* dense_int_3l_kernel(int n, int g, int ng1, int ng2) {
     case 4: return dense_int_3l_kernel_g4(n, ng1, ng2);
     case 5: return dense_int_3l_kernel_g5(n, ng1, ng2);
     case 6: return dense_int_3l_kernel_g6(n, ng1, ng2);
+    default: return nullptr;
+  }
+}
+
+static const void* dense_intc_3l_kernel(int n, int g, int pair, int ng1, int ng2) {
+  switch (intc_sparse_family(g, pair)) {
+    case 0: return dense_intc_3l_kernel_g4p(n, ng1, ng2);
+    case 1: return dense_intc_3l_kernel_g5(n, ng1, ng2);
+    case 2: return dense_intc_3l_kernel_g6p(n, ng1, ng2);
     default: return nullptr;
   }
 }
@@ -419,11 +431,12 @@ struct perm_ctx {
   // [17] split-dd dense, [18 + i] split-dd sparse with kSparseInner[i] inner rows
   // (i < 4; [43 + i - 4] for the others), [46 + i] FP64-X in the two-level
   // layout with k2lInner[i] inner rows, [50 + 6 (G - 4) + 2 (ng1 - 2) + ng2 - 1]
-  // int32-X in the three-level layout,
+  // int32-X in the three-level layout, [68 + 6 family + 2 (ng1 - 2) + ng2 - 1]
+  // certified int32-X in the three-level layout,
   // [22 + G - 4] certified int32-X with exact pairs of groups, [25 + 3 (G - 4)
   // + ngo - 1] int32-X in the two-level row layout, [34 + 3 family + ngo - 1]
   // certified int32-X in the two-level layout
-  int dense_occ[68][PERM_MAX_EXACT_N + 1] = {};
+  int dense_occ[86][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
@@ -1067,7 +1080,7 @@ static int fp64_two_level_rows(const std::vector<double>& a, int n, int* c3) {
 // provably fit, and only when it beats the one-level layout `one_cost`
 // (instructions per 8 steps).  *perm receives the permuted matrix.
 static bool intc_two_level_layout(const std::vector<double>& a, int n, long one_cost, int* g_out, int* pair_out,
-                                  int* ngo_out, std::vector<double>* perm) {
+                                  int* ngo_out, std::vector<double>* perm, long* cost_out = nullptr) {
   if (n < kIntSparseMinN || n > kIntSparseMaxN) return false;
   int c3[3];
   const int support = sparsest_column_triple(a, n, c3);
@@ -1117,7 +1130,60 @@ static bool intc_two_level_layout(const std::vector<double>& a, int n, long one_
   }
   if (best == one_cost) return false;
   *perm = std::move(p);
+  if (cost_out) *cost_out = best;
   return true;
+}
+
+// Three-level layout of the certified int32-X walk
+// (ryser_dense_intc_3l_kernel): the rows of three_level_permutation, with
+// the families of the two-level kernel (groups of 4 or 6 in int64 pairs, 5
+// alone); per 8 steps 4 (R1 + c1) + 3 (R2 + c1 + c2) + n + c1 + c2 + c3,
+// c the level costs of intc_two_level_layout; the cheapest below
+// `best_cost` whose groups (< 2^31) and pairs (< 2^53) provably fit.
+static bool intc_three_level_layout(const std::vector<double>& a, int n, long best_cost, int* g_out, int* pair_out,
+                                    int* ng1_out, int* ng2_out, std::vector<double>* perm) {
+  long best = best_cost;
+  const int fam_g[3] = {4, 5, 6};
+  const bool fam_pair[3] = {true, false, true};
+  for (int fam = 0; fam < 3; fam++) {
+    const int g = fam_g[fam];
+    const bool pair = fam_pair[fam];
+    int ng1 = 0, ng2 = 0;
+    std::vector<double> p;
+    if (!three_level_permutation(a, n, g, &ng1, &ng2, &p)) continue;
+    std::vector<double> rowabs;
+    if (!int_row_abs(p, n, rowabs)) continue;
+    auto prod = [&](int j0, int j1) {
+      double b = 1.0;
+      for (int j = j0; j < j1; j++) b *= std::max(rowabs[j], 1.0);
+      return b;
+    };
+    auto level_fits = [&](int j0, int j1) {
+      std::vector<std::pair<int, int>> grp;
+      for (int j = j0; j < j1; j += g) grp.push_back({j, std::min(j + g, j1)});
+      for (auto& r : grp)
+        if (!(prod(r.first, r.second) < 2147483648.0)) return false;
+      if (pair)
+        for (size_t i = 0; i + 1 < grp.size(); i += 2)
+          if (!(prod(grp[i].first, grp[i + 1].second) < 9007199254740992.0)) return false;
+      return true;
+    };
+    auto lc = [&](int rows) {
+      const int ng = (rows + g - 1) / g, f = pair ? (ng + 1) / 2 : ng;
+      return (long)(rows - ng) + (pair ? ng / 2 : 0) + f + 3L * f;
+    };
+    const int r1 = ng1 * g, r2 = r1 + ng2 * g;
+    const long c1 = lc(r1), c2 = lc(r2 - r1), c3 = lc(n - r2);
+    const long cost = 4 * (r1 + c1) + 3 * (r2 + c1 + c2) + n + c1 + c2 + c3;
+    if (cost >= best || !level_fits(0, r1) || !level_fits(r1, r2) || !level_fits(r2, n)) continue;
+    best = cost;
+    *g_out = g;
+    *pair_out = pair ? 1 : 0;
+    *ng1_out = ng1;
+    *ng2_out = ng2;
+    *perm = std::move(p);
+  }
+  return best != best_cost;
 }
 
 static int build_sdd_operand(perm_ctx* ctx, const std::vector<double>& a, int n, DenseOperand* op) {
@@ -1167,8 +1233,25 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
     if (op->variant == PERM_KERNEL_DENSE_INT_DD) {
       int cost1 = 0;
       op->group = intc_layout(a, n, &op->pair, &cost1);
-      if (intc_two_level_layout(a, n, 8L * (n + cost1), &op->group, &op->pair, &op->ngo, &two))
-        a.swap(two);  // walk the permuted matrix (same permanent)
+      long cost = 8L * (n + cost1);
+      int g2 = op->group, p2 = op->pair, ngo2 = 0;
+      std::vector<double> three;
+      if (intc_two_level_layout(a, n, cost, &g2, &p2, &ngo2, &two, &cost)) {
+        op->group = g2;
+        op->pair = p2;
+        op->ngo = ngo2;
+      }
+      int g3 = 0, p3 = 0, a1 = 0, a2 = 0;
+      if (intc_three_level_layout(a, n, cost, &g3, &p3, &a1, &a2, &three)) {
+        op->group = g3;
+        op->pair = p3;
+        op->ngo = 0;
+        op->ng1 = a1;
+        op->ng2 = a2;
+        a.swap(three);  // walk the permuted matrix (same permanent)
+      } else if (op->ngo) {
+        a.swap(two);
+      }
     }
     if (op->variant == PERM_KERNEL_DENSE_INT) {
       const IntLayout l = choose_int_layout(a, n, G, &two);
@@ -1220,7 +1303,9 @@ static const void* operand_kernel(const DenseOperand& op) {
            : op.ngo ? dense_int_sparse_kernel(op.n, op.group, op.ngo)
                     : dense_int_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_INT_DD)
-    return op.ngo ? dense_intc_sparse_kernel(op.n, op.group, op.pair, op.ngo) : dense_intc_kernel(op.n, op.group, op.pair);
+    return op.ng1   ? dense_intc_3l_kernel(op.n, op.group, op.pair, op.ng1, op.ng2)
+           : op.ngo ? dense_intc_sparse_kernel(op.n, op.group, op.pair, op.ngo)
+                    : dense_intc_kernel(op.n, op.group, op.pair);
   if (op.variant == PERM_KERNEL_DENSE_SDD) return sdd_kernel(op.n, op.inner);
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
@@ -1283,19 +1368,28 @@ extern "C" int perm_int_layout(const double* mat, int n, int* levels) {
   return l.g;
 }
 
-extern "C" int perm_intc_layout(const double* mat, int n, int* pair, int* ngo) {
-  if (!mat || !pair || !ngo || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
+extern "C" int perm_intc_layout(const double* mat, int n, int* pair, int* levels) {
+  if (!mat || !pair || !levels || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
   std::vector<double> a(mat, mat + (size_t)n * n);
+  levels[0] = levels[1] = levels[2] = 0;
   int cost1 = 0;
   int g = intc_layout(a, n, pair, &cost1);
-  *ngo = 0;
   if (!g) return PERM_EUNSUPPORTED;
-  std::vector<double> two;
+  long cost = 8L * (n + cost1);
+  std::vector<double> two, three;
   int g2 = g, p2 = *pair, ngo2 = 0;
-  if (intc_two_level_layout(a, n, 8L * (n + cost1), &g2, &p2, &ngo2, &two)) {
+  if (intc_two_level_layout(a, n, cost, &g2, &p2, &ngo2, &two, &cost)) {
     g = g2;
     *pair = p2;
-    *ngo = ngo2;
+    levels[0] = ngo2;
+  }
+  int g3 = 0, p3 = 0, a1 = 0, a2 = 0;
+  if (intc_three_level_layout(a, n, cost, &g3, &p3, &a1, &a2, &three)) {
+    g = g3;
+    *pair = p3;
+    levels[0] = 0;
+    levels[1] = a1;
+    levels[2] = a2;
   }
   return g;
 }
@@ -1333,8 +1427,11 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
                                  : op.variant == PERM_KERNEL_DENSE_TC ? 8 + op.group - 3
                                  : op.variant == PERM_KERNEL_DENSE_SPLIT ? 12
                                  : op.variant == PERM_KERNEL_DENSE_INT_DD
-                                     ? (op.ngo ? 34 + 3 * intc_sparse_family(op.group, op.pair) + op.ngo - 1
-                                               : op.pair ? 22 + op.group - 4 : 13 + op.group - 3)
+                                     ? (op.ng1 ? 68 + 6 * intc_sparse_family(op.group, op.pair) + 2 * (op.ng1 - 2) +
+                                                     op.ng2 - 1
+                                        : op.ngo ? 34 + 3 * intc_sparse_family(op.group, op.pair) + op.ngo - 1
+                                        : op.pair ? 22 + op.group - 4
+                                                  : 13 + op.group - 3)
                                  : op.variant == PERM_KERNEL_DENSE_SDD ? (op.inner ? sparse_slot : 17)
                                  : op.inner ? fp_slot : 0][n];
   if (!occ_slot) {

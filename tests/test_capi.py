@@ -94,17 +94,21 @@ def test_intc_layout_query(pb):
     """Host-only layout of the certified int32-X walk: product groups that
     fit int32, consecutive groups paired (exact int64 products) from order 16
     when every run of 2G rows stays below 2^53, and from order 20 the
-    two-level row layout where it is cheaper -- the layout with the fewest
-    instructions per Gray step."""
+    two-level row layout and from order 28 the three-level one where they
+    are cheaper -- the layout with the fewest instructions per Gray step."""
     rng = np.random.default_rng(3)
     A = ((rng.random((40, 40)) < 0.5) * rng.integers(1, 5, (40, 40))).astype(float)
-    g, pair, ngo = pb.intc_layout(A)
-    assert (g, pair) in ((4, True), (5, False)) and ngo in (1, 2, 3)  # two levels at order 40
+    g, pair, ngo, ng1, ng2 = pb.intc_layout(A)
+    # several levels at order 40: two (outer groups) or three (first, second level)
+    assert (g, pair) in ((4, True), (5, False), (6, True))
+    assert (ngo in (1, 2, 3) and ng1 == ng2 == 0) or (ngo == 0 and ng1 in (2, 3, 4) and ng2 in (1, 2))
     B = (rng.random((40, 40)) < 0.5).astype(float)
     assert pb.intc_layout(B)[0] in (4, 5, 6)
-    assert pb.intc_layout(B[:12, :12])[1:] == (False, 0)  # pairs from order 16, two levels from 20
+    assert pb.intc_layout(B[:12, :12])[1:] == (False, 0, 0, 0)  # pairs from order 16, levels from 20
+    Bs = B[:24, :24]
+    assert pb.intc_layout(Bs)[3:] == (0, 0)  # three levels from order 28
     C = rng.integers(0, 60, (24, 24)).astype(float)
-    assert pb.intc_layout(C) == (3, False, 0)  # large entries: groups of 3, no pairs
+    assert pb.intc_layout(C) == (3, False, 0, 0, 0)  # large entries: groups of 3, no pairs
     assert pb.intc_layout(rng.random((20, 20)))[0] == pb.PERM_EUNSUPPORTED
     assert pb.intc_layout(np.ones((7, 7)))[0] == pb.PERM_EUNSUPPORTED
 

@@ -30,7 +30,7 @@ def test_int_dd_vs_exact(engine, orc, pb, n):
     }
     layouts, levels = set(), set()
     for kind, A in cases.items():
-        g, pair, ngo = pb.intc_layout(A)
+        g, pair, ngo, _, _ = pb.intc_layout(A)
         layouts.add((g, pair))
         levels.add(ngo > 0)
         exact = orc.perm_exact_int(A)[0]
@@ -56,7 +56,7 @@ def test_int_dd_two_level_groups_of_6_vs_exact(engine, orc, pb, n, d, seed):
     oracle within the walk's own bound."""
     rng = np.random.default_rng(seed)
     A = bernoulli(rng, n, d)
-    g, pair, ngo = pb.intc_layout(A)
+    g, pair, ngo, _, _ = pb.intc_layout(A)
     assert g == 6 and pair and ngo >= 2
     exact = orc.perm_exact_int(A)[0]
     r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT_DD)
@@ -66,6 +66,25 @@ def test_int_dd_two_level_groups_of_6_vs_exact(engine, orc, pb, n, d, seed):
         ok, info = _covers(r, exact)
         assert ok, info
         assert rel_err(r.value, exact) <= 1.2e-16
+
+
+@pytest.mark.parametrize("n", [28, 30])
+def test_int_dd_three_level_vs_exact(engine, orc, pb, n):
+    """The certified walk in the three-level row layout (column 0's rows,
+    the further rows of columns 1 and 2, the rest) on dense U{1..4} and 0/1
+    matrices: the exact permanent inside the walk's bound, the value the
+    exact one rounded once."""
+    rng = np.random.default_rng(650 + n)
+    for kind, A in (("u1to4", bernoulli(rng, n, 0.5) * rng.integers(1, 5, (n, n))), ("binary", bernoulli(rng, n, 0.5))):
+        g, pair, ngo, ng1, ng2 = pb.intc_layout(A)
+        assert ngo == 0 and ng1 >= 2 and ng2 >= 1, (kind, g, pair, ngo, ng1, ng2)
+        exact = orc.perm_exact_int(A)[0]
+        r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_INT_DD)
+        ok, info = _covers(r, exact)
+        assert ok, (kind, info)
+        # u^2-level: dominated by K^2 u^2 S1 / |perm|, K ~ 2^n / threads terms per thread
+        assert r.rel_error_estimate < 1e-18, (kind, r.rel_error_estimate)
+        assert rel_err(r.value, exact) <= 1.2e-16, kind
 
 
 def test_int_dd_golden_n32(engine, golden, pb):

@@ -905,6 +905,7 @@ def secondary(pb, eng):
         pol[f"n{n}"] = {"planned_kernel": kern, "predicted_fp64_bound": predicted,
                         "fp64_walk_bound": f.rel_error_estimate, "fp64_walk_ms": f.kernel_ms,
                         "policy_kernel": r.kernel, "policy_ms": r.kernel_ms,
+                        "split_dd_levels": list(pb.sdd_levels(A)),
                         "policy_in_fp64_walks": r.kernel_ms / f.kernel_ms,
                         "policy_rel_error_estimate": r.rel_error_estimate}
     out["policy_real_dense_d050"] = pol

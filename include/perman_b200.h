@@ -215,11 +215,20 @@ int perm_ctx_inject_wait_timeout(perm_ctx* ctx, int launches);
  * layout (6, 8, 12, 16, or 20, 24, 28 with a rolled step loop for dense
  * matrices whose three sparsest columns still miss a quarter or more of the
  * rows: columns 0..2 after its permutation touch rows 0..R-1 only, so 7 of
- * 8 Gray steps walk R rows), 0 for the dense layout,
+ * 8 Gray steps walk R rows) or of the three-level layout's second level
+ * (16..28, perm_sdd_levels), 0 for the dense layout,
  * PERM_EUNSUPPORTED where the kernel does not apply (orders outside 4..40,
  * row absolute sums at or above 2^1020), PERM_EINVAL for bad arguments.
  * No counterpart in the reference. */
 int perm_sdd_layout(const double* mat, int n);
+
+/* Host only: both levels of that layout.  levels[1] = the perm_sdd_layout
+ * value; levels[0] = the first level R1 of the three-level layout (orders
+ * 24..40: column 0 touches rows 0..R1-1 only, columns 1 and 2 rows
+ * 0..levels[1]-1, so half of the Gray steps walk R1 rows and three in eight
+ * levels[1]; R1 in 8..20), 0 for the other layouts.  PERM_OK, or the
+ * statuses of perm_sdd_layout.  No counterpart in the reference. */
+int perm_sdd_levels(const double* mat, int n, int* levels);
 
 /* Host only (no device): the number of inner rows R (16, 20, 24 or 28) of
  * the two-level row layout that PERM_KERNEL_DENSE (the FP64-X walk) uses for

@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
-    "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_fp64_layout", "perm_int_layout", "perm_intc_layout", "perm_exact_dense_plan", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
+    "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_sdd_levels", "perm_fp64_layout", "perm_int_layout", "perm_intc_layout", "perm_exact_dense_plan", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
     "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune", "perm_batch_variant", "perm_batch_use_variant",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_range", "perm_approx_scaling_range",
@@ -121,6 +121,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_exact_dense_ex": (i, [_P, _P, i, i, i, i, i, ctypes.POINTER(PermResult)]),
         "perm_shard_range": (i, [i, i, i, ctypes.POINTER(u64), ctypes.POINTER(u64)]),
         "perm_sdd_layout": (i, [_P, i]),
+        "perm_sdd_levels": (i, [_P, i, _P]),
         "perm_intc_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int), _P]),
         "perm_int_layout": (i, [_P, i, _P]),
         "perm_fp64_layout": (i, [_P, i]),
@@ -610,11 +611,23 @@ def compress(mode: int, mat) -> dict:
 
 
 def sdd_layout(mat) -> int:
-    """Inner rows of the split-dd kernel's sparse layout for this matrix
-    (perm_sdd_layout; host only): 6, 8, 12 or 16, 0 for the dense layout,
-    negative where the kernel does not apply."""
+    """Rows the split-dd kernel keeps in registers for this matrix
+    (perm_sdd_layout; host only): the sparse layout's inner rows (6 .. 28)
+    or the three-level layout's second level (16 .. 28), 0 for the dense
+    layout, negative where the kernel does not apply."""
     a = np.ascontiguousarray(mat, dtype=np.float64)
     return int(load_library().perm_sdd_layout(_ptr(a), a.shape[0]))
+
+
+def sdd_levels(mat) -> tuple[int, int]:
+    """(first level R1 of the three-level layout, 0 for the other layouts;
+    the sdd_layout value) of the split-dd walk for this matrix
+    (perm_sdd_levels; host only); (negative status, 0) where the kernel does
+    not apply."""
+    a = np.ascontiguousarray(mat, dtype=np.float64)
+    lv = np.zeros(2, dtype=np.int32)
+    rc = int(load_library().perm_sdd_levels(_ptr(a), a.shape[0], _ptr(lv)))
+    return (rc, 0) if rc else (int(lv[0]), int(lv[1]))
 
 
 def fp64_layout(mat) -> int:

@@ -41,7 +41,8 @@ LIB_SOURCES = [
     "ryser_dense_intc_g6.cu", "ryser_dense_intc_p4.cu", "ryser_dense_intc_p5.cu", "ryser_dense_intc_p6.cu",
     "ryser_dense_sdd_inst.cu", "ryser_sparse_sdd_r6.cu", "ryser_sparse_sdd_r8.cu",
     "ryser_sparse_sdd_r12.cu", "ryser_sparse_sdd_r16.cu", "ryser_sparse_sdd_r20.cu", "ryser_sparse_sdd_r24.cu",
-    "ryser_sparse_sdd_r28.cu",
+    "ryser_sparse_sdd_r28.cu", "ryser_sdd_3l_r16.cu", "ryser_sdd_3l_r20.cu", "ryser_sdd_3l_r24.cu",
+    "ryser_sdd_3l_r28.cu",
 ]
 CLI_SOURCES = ["perman_cli.cpp"]
 

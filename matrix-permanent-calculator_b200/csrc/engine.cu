@@ -105,6 +105,10 @@ const void* sparse_sdd_kernel_r16(int n);
 const void* sparse_sdd_kernel_r20(int n);
 const void* sparse_sdd_kernel_r24(int n);
 const void* sparse_sdd_kernel_r28(int n);
+const void* sdd_3l_kernel_r16(int n, int r1);
+const void* sdd_3l_kernel_r20(int n, int r1);
+const void* sdd_3l_kernel_r24(int n, int r1);
+const void* sdd_3l_kernel_r28(int n, int r1);
 
 const void* dense_tc_kernel_g3(int n);
 const void* dense_tc_kernel_g4(int n);
@@ -200,7 +204,21 @@ static const void* dense_intc_kernel(int n, int g, int pair) {
 // 20..28: the rolled step loop (two-level rows of dense matrices)
 constexpr int kSparseInner[7] = {6, 8, 12, 16, 20, 24, 28};
 
-static const void* sdd_kernel(int n, int inner) {
+// Three-level split-dd layout (ryser_sdd_3l_kernel<N, R1, R2>): second-level
+// ends R2 and first-level ends R1 < R2 (multiples of 4).
+constexpr int kSdd3lR2[4] = {16, 20, 24, 28};
+constexpr int kSdd3lMinN = 24;
+
+static const void* sdd_kernel(int n, int inner, int inner1) {
+  if (inner1) {
+    switch (inner) {
+      case 16: return sdd_3l_kernel_r16(n, inner1);
+      case 20: return sdd_3l_kernel_r20(n, inner1);
+      case 24: return sdd_3l_kernel_r24(n, inner1);
+      case 28: return sdd_3l_kernel_r28(n, inner1);
+      default: return nullptr;
+    }
+  }
   switch (inner) {
     case 0: return dense_sdd_kernel(n);
     case 6: return sparse_sdd_kernel_r6(n);
@@ -432,11 +450,12 @@ struct perm_ctx {
   // (i < 4; [43 + i - 4] for the others), [46 + i] FP64-X in the two-level
   // layout with k2lInner[i] inner rows, [50 + 6 (G - 4) + 2 (ng1 - 2) + ng2 - 1]
   // int32-X in the three-level layout, [68 + 6 family + 2 (ng1 - 2) + ng2 - 1]
-  // certified int32-X in the three-level layout,
+  // certified int32-X in the three-level layout, [86 + 4 (R2 / 4 - 4) +
+  // R1 / 4 - 2] split-dd in the three-level layout,
   // [22 + G - 4] certified int32-X with exact pairs of groups, [25 + 3 (G - 4)
   // + ngo - 1] int32-X in the two-level row layout, [34 + 3 family + ngo - 1]
   // certified int32-X in the two-level layout
-  int dense_occ[86][PERM_MAX_EXACT_N + 1] = {};
+  int dense_occ[102][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
@@ -660,6 +679,7 @@ struct DenseOperand {
   int ngo = 0;    // int32-X walk: outer product groups of the two-level row layout (0: one level)
   int ng1 = 0, ng2 = 0;  // int32-X walk: groups of the three-level layout's first and second level (0: not)
   int inner = 0;  // split-dd and FP64 X: rows 0..inner-1 hold the support of columns 0..2 (0: one level)
+  int inner1 = 0;  // split-dd three-level layout: rows 0..inner1-1 hold column 0's support (0: not)
   std::vector<unsigned char> image;
 };
 
@@ -944,13 +964,20 @@ static bool int_two_level_layout(const std::vector<double>& a, int n, int g1, in
 // touches rows [0, R1) only, columns 1 and 2 (three steps in eight) rows
 // [0, R2) only, with R1 = ng1 g and R2 = R1 + ng2 g; rows of a later level
 // may fill an earlier one (their zero entries there make the extra updates
-// no-ops).  For product groups of g rows, searches every column for column
-// 0 and every pair for columns 1, 2 (orders 28..48, ng1 in 2..4, ng2 in
-// 1..2) for the fewest rows updated per 8 steps, 4 R1 + 3 R2, and returns
-// the permuted matrix; false when no layout fits.
+// no-ops).  For levels of g rows, searches every column for column 0 and
+// every pair for columns 1, 2 (within `lim`; the int32-X walks: orders
+// 28..48, ng1 in 2..4, ng2 in 1..2) for the fewest rows updated per 8
+// steps, 4 R1 + 3 R2, and returns the permuted matrix; false when no layout
+// fits.
+struct LevelLimits {
+  int n_lo, n_hi;                              // orders
+  int ng1_lo, ng1_hi, ng2_hi, tot_lo, tot_hi;  // first-level and second-level groups, their sum
+};
+constexpr LevelLimits kIntLevels = {kInt3lMinN, kIntSparseMaxN, 2, 4, 2, 0, 1 << 20};
+
 static bool three_level_permutation(const std::vector<double>& a, int n, int g, int* ng1_out, int* ng2_out,
-                                    std::vector<double>* perm) {
-  if (n < kInt3lMinN || n > kIntSparseMaxN) return false;
+                                    std::vector<double>* perm, const LevelLimits& lim = kIntLevels) {
+  if (n < lim.n_lo || n > lim.n_hi) return false;
   std::vector<uint64_t> sup(n, 0);
   for (int j = 0; j < n; j++)
     for (int k = 0; k < n; k++)
@@ -958,15 +985,15 @@ static bool three_level_permutation(const std::vector<double>& a, int n, int g, 
   long best = -1;
   int bc[3] = {0, 0, 0}, b1 = 0, b2 = 0;
   for (int c0 = 0; c0 < n; c0++) {
-    const int ng1 = std::max(2, (__builtin_popcountll(sup[c0]) + g - 1) / g);
-    if (ng1 > 4) continue;
+    const int ng1 = std::max(lim.ng1_lo, (__builtin_popcountll(sup[c0]) + g - 1) / g);
+    if (ng1 > lim.ng1_hi) continue;
     for (int c1 = 0; c1 < n; c1++) {
       if (c1 == c0) continue;
       for (int c2 = c1 + 1; c2 < n; c2++) {
         if (c2 == c0) continue;
         const int u = __builtin_popcountll(sup[c0] | sup[c1] | sup[c2]);
-        const int ng2 = std::max(1, (u - ng1 * g + g - 1) / g);
-        if (ng2 > 2 || (ng1 + ng2) * g + 2 > n) continue;
+        const int ng2 = std::max({1, lim.tot_lo - ng1, (u - ng1 * g + g - 1) / g});
+        if (ng2 > lim.ng2_hi || ng1 + ng2 > lim.tot_hi || (ng1 + ng2) * g + 2 > n) continue;
         const long rows = 4L * ng1 * g + 3L * (ng1 + ng2) * g;
         if (best < 0 || rows < best) {
           best = rows;
@@ -1001,6 +1028,41 @@ static bool three_level_permutation(const std::vector<double>& a, int n, int g, 
   *ng2_out = b2;
   *perm = std::move(p);
   return true;
+}
+
+// FP64 operations per 8 Gray steps of the split-dd layouts: dense, sparse
+// (inner rows r; unrolled below 20, rolled from 20) and three-level
+// (ryser_sdd_3l_kernel, levels ending at r1 and r2).
+static long sdd_cost(int n, int r, int r1 = 0, int r2 = 0) {
+  if (r1) return 24L * r1 + 18L * r2 + 6L * n + 116;
+  if (!r) return 8L * (6 * n + 10);
+  if (r < 20) return 7L * (6 * r + 9) + 6L * n + 5;
+  return 7L * (6 * r + 13) + 12L * n - 6L * r + 20;
+}
+
+// Three-level layout of the split-dd walk, levels of 4 rows: first level
+// 8..20 rows, second level ending at 16..28, orders 24..40.
+constexpr LevelLimits kSddLevels = {kSdd3lMinN, 40, 2, 5, 5, 4, 7};
+
+// Layout of the split-dd walk for this matrix: the sparse layout's inner
+// rows (sdd_inner_rows), or the three-level layout when its cost per 8
+// steps is lower; *inner = rows in registers (0: dense layout), *inner1 =
+// the three-level layout's first level (0: not), *perm = the permuted
+// matrix for the sparse and three-level layouts.
+static void sdd_choose(const std::vector<double>& a, int n, int* inner, int* inner1, std::vector<double>* perm) {
+  int c3[3] = {0, 1, 2};
+  *inner = sdd_inner_rows(a, n, c3);
+  *inner1 = 0;
+  int ng1 = 0, ng2 = 0;
+  std::vector<double> three;
+  if (three_level_permutation(a, n, 4, &ng1, &ng2, &three, kSddLevels) &&
+      sdd_cost(n, 0, 4 * ng1, 4 * (ng1 + ng2)) < sdd_cost(n, *inner)) {
+    *inner = 4 * (ng1 + ng2);
+    *inner1 = 4 * ng1;
+    *perm = std::move(three);
+    return;
+  }
+  if (*inner) *perm = sparse_permutation(a.data(), n, c3);
 }
 
 // Three-level layout of the int32-X walk: per 8 steps about
@@ -1188,17 +1250,14 @@ static bool intc_three_level_layout(const std::vector<double>& a, int n, long be
 
 static int build_sdd_operand(perm_ctx* ctx, const std::vector<double>& a, int n, DenseOperand* op) {
   if (n < 4 || n > 40) return fail(ctx, PERM_EUNSUPPORTED, "split-dd kernel covers orders 4..40 (got %d)", n);
-  int c3[3] = {0, 1, 2};
-  const int inner = sdd_inner_rows(a, n, c3);
-  int rc;
-  if (inner) {
-    rc = build_split_operand(ctx, sparse_permutation(a.data(), n, c3), n, op);
-  } else {
-    rc = build_split_operand(ctx, a, n, op);
-  }
+  int inner = 0, inner1 = 0;
+  std::vector<double> perm;
+  sdd_choose(a, n, &inner, &inner1, &perm);
+  const int rc = build_split_operand(ctx, inner ? perm : a, n, op);
   if (rc) return rc;
   op->variant = PERM_KERNEL_DENSE_SDD;
   op->inner = inner;
+  op->inner1 = inner1;
   return PERM_OK;
 }
 
@@ -1306,7 +1365,7 @@ static const void* operand_kernel(const DenseOperand& op) {
     return op.ng1   ? dense_intc_3l_kernel(op.n, op.group, op.pair, op.ng1, op.ng2)
            : op.ngo ? dense_intc_sparse_kernel(op.n, op.group, op.pair, op.ngo)
                     : dense_intc_kernel(op.n, op.group, op.pair);
-  if (op.variant == PERM_KERNEL_DENSE_SDD) return sdd_kernel(op.n, op.inner);
+  if (op.variant == PERM_KERNEL_DENSE_SDD) return sdd_kernel(op.n, op.inner, op.inner1);
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
   if (op.variant == PERM_KERNEL_DENSE_SPLIT) return dense_split_kernel(op.n);
@@ -1395,11 +1454,18 @@ extern "C" int perm_intc_layout(const double* mat, int n, int* pair, int* levels
 }
 
 extern "C" int perm_sdd_layout(const double* mat, int n) {
-  if (!mat || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
+  int levels[2];
+  const int rc = perm_sdd_levels(mat, n, levels);
+  return rc ? rc : levels[1];
+}
+
+extern "C" int perm_sdd_levels(const double* mat, int n, int* levels) {
+  if (!mat || !levels || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
   std::vector<double> a(mat, mat + (size_t)n * n);
   if (n < 4 || n > 40 || !split_rows_ok(a, n)) return PERM_EUNSUPPORTED;
-  int c3[3];
-  return sdd_inner_rows(a, n, c3);
+  std::vector<double> perm;
+  sdd_choose(a, n, &levels[1], &levels[0], &perm);
+  return PERM_OK;
 }
 
 extern "C" int perm_shard_range(int n, int shard, int nshards, uint64_t* first, uint64_t* last) {
@@ -1417,8 +1483,10 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
   for (int i = 0; i < 7; i++)
     if (op.inner == kSparseInner[i]) sparse_slot = i < 4 ? 18 + i : 43 + i - 4;
   int fp_slot = 0;
-  for (int i = 0; i < 4; i++)
+  for (int i = 0; i < 4; i++) {
     if (op.inner == k2lInner[i]) fp_slot = 46 + i;
+    if (op.inner1 && op.inner == kSdd3lR2[i]) sparse_slot = 86 + 4 * i + op.inner1 / 4 - 2;
+  }
   int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT
                                      ? (op.ng1 ? 50 + 6 * (op.group - 4) + 2 * (op.ng1 - 2) + op.ng2 - 1
                                         : op.ngo ? 25 + 3 * (op.group - 4) + op.ngo - 1

@@ -123,3 +123,19 @@ def test_sdd_layout_query(pb):
     assert pb.sdd_layout(P) == 6
     assert pb.sdd_layout(np.ones((41, 41))) == pb.PERM_EUNSUPPORTED
     assert pb.sdd_layout(np.ones((3, 3))) == pb.PERM_EUNSUPPORTED
+    assert pb.sdd_levels(P) == (0, 6)
+
+
+def test_sdd_levels_query(pb):
+    """Density-1/2 real matrices of orders 24..40 take the split-dd walk's
+    three-level layout (first level 8..20 rows, second ending at 16..28);
+    below order 24 they do not."""
+    for n in (24, 30, 34, 40):
+        rng = np.random.default_rng(n)
+        A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+        r1, r2 = pb.sdd_levels(A)
+        assert r1 in (8, 12, 16, 20) and r2 in (16, 20, 24, 28) and r1 < r2, (n, r1, r2)
+        assert pb.sdd_layout(A) == r2
+    rng = np.random.default_rng(5)
+    assert pb.sdd_levels((rng.random((22, 22)) < 0.5) * 1.0)[0] == 0
+    assert pb.sdd_levels(np.ones((41, 41)))[0] == pb.PERM_EUNSUPPORTED

@@ -178,16 +178,66 @@ def test_sdd_sparse_layout_vs_oracle_dd(engine, orc, pb, n, d):
     assert rel_err(s.value, want) < TOL
 
 
-@pytest.mark.parametrize("n,seed", [(27, 1), (28, 3)])
-def test_sdd_two_level_rolled_vs_oracle_dd(engine, orc, pb, n, seed):
-    """Dense real matrices (density 1/2): the three sparsest columns still
-    miss a third of the rows, so split-dd walks 20 inner rows at seven of
-    eight steps (the rolled two-level loop); against the CPU double-double
-    Ryser, and the automatic path certifies 1e-10."""
+def _sdd_vs_oracle(engine, orc, pb, A):
+    n = A.shape[0]
+    r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SDD)
+    hi, lo = orc.perm_dd(A)
+    want = hi + lo
+    slack = (4 * n + 32) * 2.0 ** -106 * r.abs_term_sum
+    ok, info = _covers(r, want, slack)
+    assert ok, info
+    assert r.rel_error_estimate <= TOL
+    a = engine.exact_dense(A)
+    assert a.rel_error_estimate <= TOL and rel_err(a.value, want) <= TOL
+
+
+@pytest.mark.parametrize("n,seed,levels", [(24, 1, (12, 16)), (26, 0, (8, 20)), (27, 2, (12, 20)), (28, 10, (8, 16)),
+                                           (30, 11, (12, 24))])
+def test_sdd_three_level_vs_oracle_dd(engine, orc, pb, n, seed, levels):
+    """Dense real matrices (density 1/2): split-dd walks column 0's rows
+    (R1) at half of the steps and those of columns 0..2 (R2) at three in
+    eight -- the three-level layout; against the CPU double-double Ryser,
+    and the automatic path certifies 1e-10."""
     rng = np.random.default_rng(seed)
     A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+    assert pb.sdd_levels(A) == levels
+    _sdd_vs_oracle(engine, orc, pb, A)
+
+
+@pytest.mark.parametrize("seed", [0, 2])
+def test_sdd_three_level_second_level_28_vs_oracle_dd(engine, orc, pb, seed):
+    """Order 30, column 0 on rows 0..15, columns 1 and 2 on rows 0..27, the
+    rest dense: the three-level layout with 28 rows in registers (2 CTAs per
+    SM)."""
+    rng = np.random.default_rng(seed)
+    n = 30
+    mask = rng.random((n, n)) < 0.9
+    mask[16:, 0] = False
+    mask[:16, 0] = True
+    mask[:, 1:3] = False
+    mask[16:28, 1:3] = rng.random((12, 2)) < 0.7
+    mask[16:28, 1] |= ~mask[16:28, 2]
+    mask[:16, 1:3] = rng.random((16, 2)) < 0.25
+    A = mask * (1.0 - rng.random((n, n)))
+    r1, r2 = pb.sdd_levels(A)
+    assert r1 in (8, 12, 16) and r2 == 28, (r1, r2)
+    _sdd_vs_oracle(engine, orc, pb, A)
+
+
+@pytest.mark.parametrize("n,seed", [(27, 1), (28, 2)])
+def test_sdd_two_level_rolled_vs_oracle_dd(engine, orc, pb, n, seed):
+    """Three columns on the same 20 rows and every other column on 21 or
+    more (no cheaper three-level layout): split-dd walks 20 inner rows at
+    seven of eight steps (the rolled two-level loop); against the CPU
+    double-double Ryser, and the automatic path certifies 1e-10."""
+    rng = np.random.default_rng(seed)
+    mask = rng.random((n, n)) < 0.9
+    mask[20:, :3] = False
+    mask[:20, :3] |= rng.random((20, 3)) < 0.5
+    A = mask * (1.0 - rng.random((n, n)))
+    assert pb.sdd_levels(A) == (0, 20)
     inner = pb.sdd_layout(A)
-    assert inner in (20, 24, 28), inner
+    assert inner == 20, inner
     r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE_SDD)
     hi, lo = orc.perm_dd(A)
     want = hi + lo

@@ -187,7 +187,7 @@ def run_reference_arm(args):
 # from the same text.
 KERNEL_SOURCES = {
     "int32x": ["ryser_dense_int_sparse.cuh", "ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
-    "fp64x": ["ryser_dense.cuh", "perman_common.cuh"],
+    "fp64x": ["ryser_dense_2l.cuh", "ryser_dense.cuh", "perman_common.cuh"],
     "int32x_dd": ["ryser_dense_intc_sparse.cuh", "ryser_dense_intc.cuh", "ryser_dense_int_sparse.cuh",
                   "ryser_dense_int.cuh", "ryser_dense.cuh", "perman_common.cuh"],
 }
@@ -221,7 +221,10 @@ def kernel_template(kname: str, A: np.ndarray) -> str:
             return f"ryser_dense_intc_sparse_kernel<{n}, {g}, {pb_}, {ngo}, {3 if n <= 36 else 2}>"
         return f"ryser_dense_intc_kernel<{n}, {g}, {pb_}, {3 if n <= 36 else 2}>"
     if kname == "fp64x":
-        return f"ryser_dense_kernel<{n}>"
+        r1, r = (sys.modules.get("perman_b200") or load_pkg()).fp64_levels(A)
+        if r1:
+            return f"ryser_dense_3l_kernel<{n}, {r1}, {r}>"
+        return f"ryser_dense_2l_kernel<{n}, {r}>" if r else f"ryser_dense_kernel<{n}>"
     return kname
 
 
@@ -516,12 +519,16 @@ def main():
         f64.free()
         # FP64 operations the walk executes per Gray step: n updates and n - 1
         # multiplies (one level); in the two-level layout R inner rows at
-        # seven of eight steps (R updates, R - 1 multiplies, times P_out)
-        r2l = pb.fp64_layout(A)
-        executed = (7 * 2 * r2l + 2 * n - 1) / 8 if r2l else 2 * n - 1
+        # seven of eight steps (R updates, R - 1 multiplies, times P_out); in
+        # the three-level layout 2 R1 at four steps in eight, 2 R2 at three
+        r1, r2l = pb.fp64_levels(A)
+        if r1:
+            executed = (4 * 2 * r1 + 3 * 2 * r2l + 2 * n - 1) / 8
+        else:
+            executed = (7 * 2 * r2l + 2 * n - 1) / 8 if r2l else 2 * n - 1
         line["secondary"]["dense_n40_fp64x_same_matrix"] = {
             "kernel_ms": fr.kernel_ms, "steps_per_s": total_steps / (fr.kernel_ms * 1e-3),
-            "two_level_inner_rows": r2l,
+            "levels": [r1, r2l],
             "fp64_equivalent_frac_of_measured_peak": total_steps * ops_per_step / (fr.kernel_ms * 1e-3) / peak_ops,
             "fp64_pipe_frac_of_measured_peak": total_steps * executed / (fr.kernel_ms * 1e-3) / peak_ops,
             "rel_diff_vs_headline": abs(fr.value - perm_value) / abs(perm_value)}

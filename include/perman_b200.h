@@ -235,9 +235,18 @@ int perm_sdd_levels(const double* mat, int n, int* levels);
  * the row-major n x n matrix `mat` (orders 20..48: the three columns whose
  * nonzeros lie in the fewest rows go first, their rows to the top, and at
  * seven of every eight Gray steps only those R rows are updated and
- * multiplied), 0 for the one-level walk; PERM_EINVAL for bad arguments.  No
- * counterpart in the reference. */
+ * multiplied), or the second level R2 (20..36) of its three-level layout
+ * (perm_fp64_levels), 0 for the one-level walk; PERM_EINVAL for bad
+ * arguments.  No counterpart in the reference. */
 int perm_fp64_layout(const double* mat, int n);
+
+/* Host only: both levels of that layout.  levels[1] = the perm_fp64_layout
+ * value; levels[0] = the first level R1 (8..20) of the three-level layout
+ * (orders 28..48: column 0 touches rows 0..R1-1 only, columns 1 and 2 rows
+ * 0..levels[1]-1, so half of the Gray steps update R1 rows and three in
+ * eight levels[1]), 0 for the other layouts.  PERM_OK or PERM_EINVAL.  No
+ * counterpart in the reference. */
+int perm_fp64_levels(const double* mat, int n, int* levels);
 
 /* Host only (no device): the layout PERM_KERNEL_DENSE_INT (the int32-X walk)
  * uses for the row-major n x n matrix `mat`: returns the product-group size

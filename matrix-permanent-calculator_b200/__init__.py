@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
     "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
-    "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_sdd_levels", "perm_fp64_layout", "perm_int_layout", "perm_intc_layout", "perm_exact_dense_plan", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
+    "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_sdd_levels", "perm_fp64_layout", "perm_fp64_levels", "perm_int_layout", "perm_intc_layout", "perm_exact_dense_plan", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
     "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune", "perm_batch_variant", "perm_batch_use_variant",
     "perm_server_create", "perm_server_submit", "perm_server_wait", "perm_server_stats", "perm_server_destroy",
     "perm_approx_rasmussen", "perm_approx_scaling", "perm_approx_rasmussen_range", "perm_approx_scaling_range",
@@ -125,6 +125,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_intc_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int), _P]),
         "perm_int_layout": (i, [_P, i, _P]),
         "perm_fp64_layout": (i, [_P, i]),
+        "perm_fp64_levels": (i, [_P, i, _P]),
         "perm_exact_dense_plan": (i, [_P, _P, i, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
         "perm_matrix_create_dense_ex": (i, [_P, _P, i, i, i, ctypes.POINTER(_P)]),
         "perm_exact_sparse": (i, [_P, i, _P, _P, _P, _P, _P, _P, ctypes.POINTER(PermResult)]),
@@ -632,9 +633,20 @@ def sdd_levels(mat) -> tuple[int, int]:
 
 def fp64_layout(mat) -> int:
     """Inner rows of the FP64-X walk's two-level row layout for this matrix
-    (perm_fp64_layout; host only): 16, 20, 24 or 28, 0 for one level."""
+    (perm_fp64_layout; host only): 16, 20, 24 or 28, or the second level
+    (20..36) of its three-level layout; 0 for one level."""
     a = np.ascontiguousarray(mat, dtype=np.float64)
     return int(load_library().perm_fp64_layout(_ptr(a), a.shape[0]))
+
+
+def fp64_levels(mat) -> tuple[int, int]:
+    """(first level R1 of the FP64-X walk's three-level layout, 0 for the
+    other layouts; the fp64_layout value) for this matrix (perm_fp64_levels;
+    host only)."""
+    a = np.ascontiguousarray(mat, dtype=np.float64)
+    lv = np.zeros(2, dtype=np.int32)
+    rc = int(load_library().perm_fp64_levels(_ptr(a), a.shape[0], _ptr(lv)))
+    return (rc, 0) if rc else (int(lv[0]), int(lv[1]))
 
 
 def int_layout(mat) -> tuple[int, int, int, int]:

@@ -42,7 +42,8 @@ LIB_SOURCES = [
     "ryser_dense_sdd_inst.cu", "ryser_sparse_sdd_r6.cu", "ryser_sparse_sdd_r8.cu",
     "ryser_sparse_sdd_r12.cu", "ryser_sparse_sdd_r16.cu", "ryser_sparse_sdd_r20.cu", "ryser_sparse_sdd_r24.cu",
     "ryser_sparse_sdd_r28.cu", "ryser_sdd_3l_r16.cu", "ryser_sdd_3l_r20.cu", "ryser_sdd_3l_r24.cu",
-    "ryser_sdd_3l_r28.cu",
+    "ryser_sdd_3l_r28.cu", "ryser_dense_3l_r20.cu", "ryser_dense_3l_r24.cu", "ryser_dense_3l_r28.cu",
+    "ryser_dense_3l_r32.cu", "ryser_dense_3l_r36.cu",
 ]
 CLI_SOURCES = ["perman_cli.cpp"]
 

@@ -62,10 +62,28 @@ const void* dense_2l_kernel_r16(int n);
 const void* dense_2l_kernel_r20(int n);
 const void* dense_2l_kernel_r24(int n);
 const void* dense_2l_kernel_r28(int n);
+const void* dense_3l_kernel_r20(int n, int r1);
+const void* dense_3l_kernel_r24(int n, int r1);
+const void* dense_3l_kernel_r28(int n, int r1);
+const void* dense_3l_kernel_r32(int n, int r1);
+const void* dense_3l_kernel_r36(int n, int r1);
 
 // FP64-X walk in the two-level row layout (ryser_dense_2l.cuh): orders
 // 20..48, 16..28 inner rows
 constexpr int k2lInner[4] = {16, 20, 24, 28};
+// FP64-X three-level layout (ryser_dense_3l_kernel<N, R1, R2>): second
+// levels ending at R2, first levels R1 in 8..20
+constexpr int kFp3lR2[5] = {20, 24, 28, 32, 36};
+static const void* dense_3l_kernel(int n, int r1, int r2) {
+  switch (r2) {
+    case 20: return dense_3l_kernel_r20(n, r1);
+    case 24: return dense_3l_kernel_r24(n, r1);
+    case 28: return dense_3l_kernel_r28(n, r1);
+    case 32: return dense_3l_kernel_r32(n, r1);
+    case 36: return dense_3l_kernel_r36(n, r1);
+    default: return nullptr;
+  }
+}
 static const void* dense_2l_kernel(int n, int inner) {
   switch (inner) {
     case 16: return dense_2l_kernel_r16(n);
@@ -451,11 +469,12 @@ struct perm_ctx {
   // layout with k2lInner[i] inner rows, [50 + 6 (G - 4) + 2 (ng1 - 2) + ng2 - 1]
   // int32-X in the three-level layout, [68 + 6 family + 2 (ng1 - 2) + ng2 - 1]
   // certified int32-X in the three-level layout, [86 + 4 (R2 / 4 - 4) +
-  // R1 / 4 - 2] split-dd in the three-level layout,
+  // R1 / 4 - 2] split-dd in the three-level layout, [102 + 4 i + R1 / 4 - 2]
+  // FP64 X in the three-level layout with kFp3lR2[i],
   // [22 + G - 4] certified int32-X with exact pairs of groups, [25 + 3 (G - 4)
   // + ngo - 1] int32-X in the two-level row layout, [34 + 3 family + ngo - 1]
   // certified int32-X in the two-level layout
-  int dense_occ[102][PERM_MAX_EXACT_N + 1] = {};
+  int dense_occ[122][PERM_MAX_EXACT_N + 1] = {};
   int batch_m[kBatchMaxOrder + 1] = {};          // autotuned lane-range exponents (0: default)
   int dense_pref[PERM_MAX_EXACT_N + 1] = {};     // autotuned kernel for integer inputs (0: built-in choice)
   double rel_target = 1e-10;                     // rerun in double-double above this estimate (<=0: never)
@@ -1131,6 +1150,34 @@ static int fp64_two_level_rows(const std::vector<double>& a, int n, int* c3) {
   return 0;
 }
 
+// Three-level layout of the FP64-X walk (ryser_dense_3l_kernel), levels of 4
+// rows: first level 8..20 rows, second ending at 20..36, orders 28..48.
+constexpr LevelLimits kFp64Levels = {28, 48, 2, 5, 7, 5, 9};
+
+// Layout of the FP64-X walk for this matrix: *inner = the two-level
+// layout's inner rows (fp64_two_level_rows) or the three-level layout's
+// second level R2, 0 for one level; *inner1 = the three-level layout's
+// first level R1 (0: not); *perm = the permuted matrix.  Per 8 steps the
+// one-level walk costs 16n operations, the two-level 7 (2R + 1) + 2n, the
+// three-level 8 R1 + 6 R2 + 2n + 13; the three-level layout is taken when
+// cheapest.
+static void fp64_choose(const std::vector<double>& a, int n, int* inner, int* inner1, std::vector<double>* perm) {
+  int c3[3] = {0, 1, 2};
+  *inner = fp64_two_level_rows(a, n, c3);
+  *inner1 = 0;
+  const long cost = *inner ? 7L * (2 * *inner + 1) + 2L * n : 16L * n;
+  int ng1 = 0, ng2 = 0;
+  std::vector<double> three;
+  if (three_level_permutation(a, n, 4, &ng1, &ng2, &three, kFp64Levels) &&
+      32L * ng1 + 24L * (ng1 + ng2) + 2L * n + 13 < cost) {
+    *inner = 4 * (ng1 + ng2);
+    *inner1 = 4 * ng1;
+    *perm = std::move(three);
+    return;
+  }
+  if (*inner) *perm = sparse_permutation(a.data(), n, c3);
+}
+
 // Two-level row layout of the certified int32-X walk
 // (ryser_dense_intc_sparse.cuh): the permutation of int_two_level_layout,
 // with groups of 4 or 6 rows in int64 pairs or groups of 5 alone.  Per Gray
@@ -1335,13 +1382,11 @@ static int build_operand(perm_ctx* ctx, const void* mat, int n, int dtype, int v
     op->variant = variant == PERM_KERNEL_DENSE_DD ? PERM_KERNEL_DENSE_DD : PERM_KERNEL_DENSE;
     op->group = 0;
     op->inner = 0;
+    op->inner1 = 0;
     if (op->variant == PERM_KERNEL_DENSE) {
-      int c3[3];
-      const int r = fp64_two_level_rows(a, n, c3);
-      if (r) {
-        a = sparse_permutation(a.data(), n, c3);  // walk the permuted matrix (same permanent)
-        op->inner = r;
-      }
+      std::vector<double> perm;
+      fp64_choose(a, n, &op->inner, &op->inner1, &perm);
+      if (op->inner) a.swap(perm);  // walk the permuted matrix (same permanent)
     }
     op->image.assign(sizeof(double) * (size_t)n * np, 0);
     double* img = reinterpret_cast<double*>(op->image.data());
@@ -1369,7 +1414,9 @@ static const void* operand_kernel(const DenseOperand& op) {
   if (op.variant == PERM_KERNEL_DENSE_TC) return dense_tc_kernel(op.n, op.group);
   if (op.variant == PERM_KERNEL_DENSE_DD) return dense_dd_kernel(op.n);
   if (op.variant == PERM_KERNEL_DENSE_SPLIT) return dense_split_kernel(op.n);
-  return op.inner ? dense_2l_kernel(op.n, op.inner) : dense_kernel(op.n);
+  return op.inner1  ? dense_3l_kernel(op.n, op.inner1, op.inner)
+         : op.inner ? dense_2l_kernel(op.n, op.inner)
+                    : dense_kernel(op.n);
 }
 static int operand_threads(const DenseOperand& op) { return op.variant == PERM_KERNEL_DENSE_TC ? kTcThreads : 128; }
 static size_t operand_smem(const DenseOperand& op) {
@@ -1407,10 +1454,17 @@ static void shard_bounds(int n, int shard, int nshards, uint64_t* first, uint64_
 }
 
 extern "C" int perm_fp64_layout(const double* mat, int n) {
-  if (!mat || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
+  int levels[2];
+  const int rc = perm_fp64_levels(mat, n, levels);
+  return rc ? rc : levels[1];
+}
+
+extern "C" int perm_fp64_levels(const double* mat, int n, int* levels) {
+  if (!mat || !levels || n < 1 || n > PERM_MAX_EXACT_N) return PERM_EINVAL;
   std::vector<double> a(mat, mat + (size_t)n * n);
-  int c3[3];
-  return fp64_two_level_rows(a, n, c3);
+  std::vector<double> perm;
+  fp64_choose(a, n, &levels[1], &levels[0], &perm);
+  return PERM_OK;
 }
 
 extern "C" int perm_int_layout(const double* mat, int n, int* levels) {
@@ -1487,6 +1541,8 @@ static int dense_plan(perm_ctx* ctx, const DenseOperand& op, int shard, int nsha
     if (op.inner == k2lInner[i]) fp_slot = 46 + i;
     if (op.inner1 && op.inner == kSdd3lR2[i]) sparse_slot = 86 + 4 * i + op.inner1 / 4 - 2;
   }
+  for (int i = 0; i < 5; i++)
+    if (op.inner1 && op.inner == kFp3lR2[i]) fp_slot = 102 + 4 * i + op.inner1 / 4 - 2;
   int& occ_slot = ctx->dense_occ[op.variant == PERM_KERNEL_DENSE_INT
                                      ? (op.ng1 ? 50 + 6 * (op.group - 4) + 2 * (op.ng1 - 2) + op.ng2 - 1
                                         : op.ngo ? 25 + 3 * (op.group - 4) + op.ngo - 1

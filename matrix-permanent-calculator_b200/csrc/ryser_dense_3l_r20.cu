@@ -1,0 +1,118 @@
+// ryser_dense_3l_r20.cu -- FP64-X dense Ryser kernels in the three-level
+// row layout whose columns 1 and 2 touch rows 0..19 only and column 0
+// rows 0..R1-1 (R1 in 8, 12, 16), orders 28..48.
+#include "ryser_dense_2l.cuh"
+
+namespace perm {
+const void* dense_3l_kernel_r20(int n, int r1) {
+  switch (n) {
+    case 28:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<28, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<28, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<28, 16, 20>);
+      return nullptr;
+    case 29:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<29, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<29, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<29, 16, 20>);
+      return nullptr;
+    case 30:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<30, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<30, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<30, 16, 20>);
+      return nullptr;
+    case 31:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<31, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<31, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<31, 16, 20>);
+      return nullptr;
+    case 32:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<32, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<32, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<32, 16, 20>);
+      return nullptr;
+    case 33:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<33, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<33, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<33, 16, 20>);
+      return nullptr;
+    case 34:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<34, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<34, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<34, 16, 20>);
+      return nullptr;
+    case 35:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<35, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<35, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<35, 16, 20>);
+      return nullptr;
+    case 36:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<36, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<36, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<36, 16, 20>);
+      return nullptr;
+    case 37:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<37, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<37, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<37, 16, 20>);
+      return nullptr;
+    case 38:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<38, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<38, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<38, 16, 20>);
+      return nullptr;
+    case 39:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<39, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<39, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<39, 16, 20>);
+      return nullptr;
+    case 40:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<40, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<40, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<40, 16, 20>);
+      return nullptr;
+    case 41:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<41, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<41, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<41, 16, 20>);
+      return nullptr;
+    case 42:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<42, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<42, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<42, 16, 20>);
+      return nullptr;
+    case 43:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<43, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<43, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<43, 16, 20>);
+      return nullptr;
+    case 44:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<44, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<44, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<44, 16, 20>);
+      return nullptr;
+    case 45:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<45, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<45, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<45, 16, 20>);
+      return nullptr;
+    case 46:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<46, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<46, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<46, 16, 20>);
+      return nullptr;
+    case 47:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<47, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<47, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<47, 16, 20>);
+      return nullptr;
+    case 48:
+      if (r1 == 8) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<48, 8, 20>);
+      if (r1 == 12) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<48, 12, 20>);
+      if (r1 == 16) return reinterpret_cast<const void*>(&ryser_dense_3l_kernel<48, 16, 20>);
+      return nullptr;
+    default:
+      return nullptr;
+  }
+}
+}  // namespace perm

@@ -126,6 +126,22 @@ def test_sdd_layout_query(pb):
     assert pb.sdd_levels(P) == (0, 6)
 
 
+def test_fp64_levels_query(pb):
+    """Density-1/2 real matrices of orders 28..48 take the FP64-X walk's
+    three-level layout (first level 8..20 rows, second ending at 20..36);
+    orders 20..27 the two-level one."""
+    for n in (28, 34, 40, 48):
+        rng = np.random.default_rng(n)
+        A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+        r1, r2 = pb.fp64_levels(A)
+        assert r1 in (8, 12, 16, 20) and r2 in (20, 24, 28, 32, 36) and r1 < r2, (n, r1, r2)
+        assert pb.fp64_layout(A) == r2
+    rng = np.random.default_rng(7)
+    A = (rng.random((24, 24)) < 0.5) * 1.0
+    assert pb.fp64_levels(A) == (0, pb.fp64_layout(A))
+    assert pb.fp64_levels(1.0 - rng.random((30, 30))) == (0, 0)  # no zeros: one level
+
+
 def test_sdd_levels_query(pb):
     """Density-1/2 real matrices of orders 24..40 take the split-dd walk's
     three-level layout (first level 8..20 rows, second ending at 16..28);

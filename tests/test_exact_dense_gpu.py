@@ -187,19 +187,13 @@ def test_int_kernel_two_level_layout_vs_exact(engine, orc, pb, n):
         res.free()
 
 
-@pytest.mark.parametrize("n", [22, 25, 28])
-def test_fp64_two_level_layout_vs_oracle(engine, orc, pb, n):
-    """The FP64-X walk in the two-level row layout on real density-1/2
-    matrices: against the CPU double-double Ryser within the walk's own
-    bound, and shards and a resident matrix of that layout add up to it."""
-    rng = np.random.default_rng(700 + n)
-    A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
-    assert pb.fp64_layout(A) in (16, 20, 24, 28)
+def _fp64_layout_case(engine, orc, pb, A, tol=1e-10):
     r = engine.exact_dense(A, variant=pb.PERM_KERNEL_DENSE)
     hi, lo = orc.perm_dd(A)
     want = hi + lo
     assert abs(r.value - want) <= r.rel_error_estimate * abs(want), (r.value, want, r.rel_error_estimate)
-    assert rel_err(r.value, want) < 1e-10
+    if tol:
+        assert rel_err(r.value, want) < tol
     # shards re-anchor X at other indices: same bound, different roundings
     parts = [engine.exact_dense_shard(A, s, 3, variant=pb.PERM_KERNEL_DENSE) for s in range(3)]
     assert abs(sum(p.hi + p.lo for p in parts) - r.value) <= 2 * r.rel_error_estimate * abs(r.value)
@@ -208,6 +202,45 @@ def test_fp64_two_level_layout_vs_oracle(engine, orc, pb, n):
         assert res.run().value == r.value
     finally:
         res.free()
+
+
+@pytest.mark.parametrize("n,seed,levels", [(28, 0, (8, 20)), (29, 1, (12, 20)), (30, 2, (12, 20))])
+def test_fp64_three_level_layout_vs_oracle(engine, orc, pb, n, seed, levels):
+    """The FP64-X walk in the three-level row layout (column 0's rows at
+    half of the steps, columns 1-2's at three in eight) on real density-1/2
+    matrices: against the CPU double-double Ryser within the walk's own
+    bound; shards and a resident matrix of that layout add up to it."""
+    rng = np.random.default_rng(seed)
+    A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+    assert pb.fp64_levels(A) == levels
+    _fp64_layout_case(engine, orc, pb, A)
+
+
+def test_fp64_three_level_layout_signed_and_wide(engine, orc, pb):
+    """Signed entries (cancellation) in the three-level layout, and a
+    second level of 24 rows at order 30 (constructed supports)."""
+    rng = np.random.default_rng(31)
+    n = 30
+    mask = rng.random((n, n)) < 0.9
+    mask[12:, 0] = False
+    mask[:12, 0] = True
+    mask[24:, 1:3] = False
+    mask[12:24, 1] = True
+    A = mask * rng.standard_normal((n, n))
+    r1, r2 = pb.fp64_levels(A)
+    assert r1 == 12 and r2 == 24, (r1, r2)
+    _fp64_layout_case(engine, orc, pb, A, tol=None)  # cancellation: the bound alone
+
+
+@pytest.mark.parametrize("n", [22, 25])
+def test_fp64_two_level_layout_vs_oracle(engine, orc, pb, n):
+    """The FP64-X walk in the two-level row layout on real density-1/2
+    matrices: against the CPU double-double Ryser within the walk's own
+    bound, and shards and a resident matrix of that layout add up to it."""
+    rng = np.random.default_rng(700 + n)
+    A = (rng.random((n, n)) < 0.5) * (1.0 - rng.random((n, n)))
+    assert pb.fp64_layout(A) in (16, 20, 24, 28) and pb.fp64_levels(A)[0] == 0
+    _fp64_layout_case(engine, orc, pb, A)
 
 
 @pytest.mark.parametrize("n", [28, 30])

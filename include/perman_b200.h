@@ -316,12 +316,15 @@ int perm_exact_dense_tc_rounds(perm_ctx* ctx, const void* mat, int n, int dtype,
  * buffer `d_out` of two doubles that receives (hi, lo); everything else lives
  * in one static device array (~96 KB per GPU that loads this library, held
  * until the process exits).  No cudaMalloc or cudaFree is called.
- *  - the computation is perm_exact_dense_ex's FP64-X kernel (PERM_KERNEL_DENSE)
- *    with the same launch decomposition and X re-anchoring, so its value
- *    equals that call's to the last bit on the same device; unlike
- *    perm_exact_dense it returns no error estimate and applies no accuracy
- *    policy (no int32-X, split-X or double-double pass), so on matrices with
- *    heavy cancellation its error is that of one FP64-X walk;
+ *  - the computation is the one-level FP64-X walk with the launch
+ *    decomposition and X re-anchoring of perm_exact_dense_ex(PERM_KERNEL_DENSE)'s
+ *    one-level walks, so its value equals that call's to the last bit on the
+ *    same device wherever that call also walks one level (orders below 20,
+ *    and matrices without a sparse enough column triple); where that call
+ *    walks a two- or three-level row layout the two agree to rounding.
+ *    Unlike perm_exact_dense it returns no error estimate and applies no
+ *    accuracy policy (no int32-X, split-dd or double-double pass), so on
+ *    matrices with heavy cancellation its error is that of one FP64-X walk;
  *  - orders 1..64; larger orders return PERM_EUNSUPPORTED (the array holds one
  *    64 x 64 operand and partials for 4096 CTAs), null pointers PERM_EINVAL;
  *  - runs asynchronously on `stream` (a cudaStream_t, NULL = default stream);

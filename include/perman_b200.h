@@ -115,6 +115,19 @@ int perm_exact_dense_shard(perm_ctx* ctx, const void* mat, int n, int dtype, int
  * covers for order n.  Host only (no device): depends on (n, shard, nshards)
  * alone, so ranks on different devices always partition [0, 2^(n-1)). */
 int perm_shard_range(int n, int shard, int nshards, uint64_t* first, uint64_t* last);
+/* One permanent sharded over devices of this process: shard s of `nshards`
+ * (1..64) runs perm_exact_dense_ex(variant) on device devices[s] (NULL:
+ * device s; a device may appear more than once) in its own host thread and
+ * context, and the shards' (hi, lo) are added in shard order in
+ * double-double, so the value does not depend on which device finishes
+ * first.  Each shard is evaluated once (no accuracy policy, no error
+ * estimate: rel_error_estimate and abs_term_sum are 0; a caller wanting the
+ * policy on the sum passes `out` to perm_exact_dense_refine); kernel_ms is
+ * the slowest shard's.  On failure the failing shard's status is returned
+ * and its message printed on stderr.  Replaces
+ * gpu_perman64_xshared_coalescing_mshared_multigpu (gpu_exact_dense.cu:702). */
+int perm_exact_dense_multi(const void* mat, int n, int dtype, int variant, int nshards, const int* devices,
+                           perm_result* out);
 /* The whole-walk value (io->hi, io->lo, io->kernel_ms) assembled from all
  * shards of perm_exact_dense_shard, given the error estimate and the
  * context's accuracy policy of perm_exact_dense (see perm_ctx_set_rel_target):
@@ -500,6 +513,14 @@ double gpu_perman64_xshared_coalescing_mshared_int(int* mat, int nov, int grid_d
 double gpu_perman64_xshared_coalescing_mshared_float(float* mat, int nov, int grid_dim, int block_dim);
 double gpu_perman64_xshared_coalescing_mshared_double(double* mat, int nov, int grid_dim,
                                                       int block_dim);
+/* gpu_exact_dense.cu:702: devices 0 .. gpu_num - 1 (clamped to the visible
+ * devices) through perm_exact_dense_multi; grid_dim and block_dim ignored. */
+double gpu_perman64_xshared_coalescing_mshared_multigpu_int(int* mat, int nov, int gpu_num, int grid_dim,
+                                                            int block_dim);
+double gpu_perman64_xshared_coalescing_mshared_multigpu_float(float* mat, int nov, int gpu_num, int grid_dim,
+                                                              int block_dim);
+double gpu_perman64_xshared_coalescing_mshared_multigpu_double(double* mat, int nov, int gpu_num, int grid_dim,
+                                                               int block_dim);
 double gpu_perman64_xshared_coalescing_mshared_skipper_int(int* mat, int* rptrs, int* cols, int* cptrs,
                                                            int* rows, int* cvals, int nov,
                                                            int grid_dim, int block_dim);

@@ -42,7 +42,8 @@ MAX_MC_SPARSE_N = 2047
 # Every extern "C" symbol declared in include/perman_b200.h.
 EXPORTED_SYMBOLS = (
     "perm_version", "perm_device_count", "perm_ctx_create", "perm_ctx_destroy", "perm_ctx_last_error",
-    "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_ex",
+    "perm_status_string", "perm_exact_dense", "perm_exact_dense_shard", "perm_shard_range", "perm_exact_dense_multi",
+    "perm_exact_dense_ex",
     "perm_exact_sparse", "perm_exact_sparse_ex", "perm_matrix_create_dense", "perm_matrix_create_dense_ex", "perm_matrix_destroy",
     "perm_exact_dense_resident", "perm_exact_dense_resident_shard", "perm_exact_dense_refine", "perm_sdd_layout", "perm_sdd_levels", "perm_fp64_layout", "perm_fp64_levels", "perm_int_layout", "perm_intc_layout", "perm_exact_dense_plan", "perm_exact_dense_tc_rounds", "perm_exact_dense_noalloc", "perm_dense_autotune", "perm_ctx_set_rel_target", "perm_ctx_inject_wait_timeout",
     "perm_batch_create", "perm_batch_run", "perm_batch_run_ex", "perm_batch_destroy", "perm_batch_exact", "perm_batch_autotune", "perm_batch_variant", "perm_batch_use_variant",
@@ -52,6 +53,8 @@ EXPORTED_SYMBOLS = (
     "perm_approx_scaling_sparse", "perm_read_matrix", "perm_compress", "perm_grid_graph", "perm_fp64_peak",
     "gpu_perman64_xshared_coalescing_mshared_int", "gpu_perman64_xshared_coalescing_mshared_float",
     "gpu_perman64_xshared_coalescing_mshared_double",
+    "gpu_perman64_xshared_coalescing_mshared_multigpu_int", "gpu_perman64_xshared_coalescing_mshared_multigpu_float",
+    "gpu_perman64_xshared_coalescing_mshared_multigpu_double",
     "gpu_perman64_xshared_coalescing_mshared_skipper_int",
     "gpu_perman64_xshared_coalescing_mshared_skipper_float",
     "gpu_perman64_xshared_coalescing_mshared_skipper_double",
@@ -120,6 +123,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "perm_exact_dense_shard": (i, [_P, _P, i, i, i, i, ctypes.POINTER(PermResult)]),
         "perm_exact_dense_ex": (i, [_P, _P, i, i, i, i, i, ctypes.POINTER(PermResult)]),
         "perm_shard_range": (i, [i, i, i, ctypes.POINTER(u64), ctypes.POINTER(u64)]),
+        "perm_exact_dense_multi": (i, [_P, i, i, i, i, _P, ctypes.POINTER(PermResult)]),
         "perm_sdd_layout": (i, [_P, i]),
         "perm_sdd_levels": (i, [_P, i, _P]),
         "perm_intc_layout": (i, [_P, i, ctypes.POINTER(ctypes.c_int), _P]),
@@ -681,6 +685,27 @@ def shard_range(n: int, shard: int, nshards: int) -> tuple[int, int]:
     if rc != PERM_OK:
         raise PermError(rc, f"bad shard request n={n} shard={shard}/{nshards}")
     return a.value, b.value
+
+
+def exact_dense_multi(mat, devices=None, nshards: int | None = None, variant: int = 0) -> ExactResult:
+    """One permanent sharded over devices of this process
+    (perm_exact_dense_multi; gpu_exact_dense.cu:702): shard s runs on
+    devices[s] (default: devices 0 .. nshards-1) in its own host thread, the
+    shards' (hi, lo) are added in shard order.  One evaluation, no error
+    estimate."""
+    a, dtype = _as_matrix(mat)
+    n = a.shape[0]
+    if devices is not None:
+        dev = np.ascontiguousarray(devices, dtype=np.int32)
+        nshards = len(dev)
+    else:
+        dev = None
+        nshards = nshards or 1
+    r = PermResult()
+    rc = load_library().perm_exact_dense_multi(_ptr(a), n, dtype, variant, nshards, _ptr(dev), ctypes.byref(r))
+    if rc != PERM_OK:
+        raise PermError(rc, f"perm_exact_dense_multi failed for n={n} over {nshards} shards (see stderr)")
+    return _exact(r)
 
 
 def dd_sum(pairs) -> tuple[float, float]:

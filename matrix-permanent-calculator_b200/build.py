@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompil
 HOST_CXX = os.environ.get("PERM_HOST_CXX", "/usr/bin/g++")
 
 LIB_SOURCES = [
-    "engine.cu", "ryser_skipper.cu", "mc.cu", "mc_sparse.cu", "batch.cu", "serve.cu", "noalloc.cu",
+    "engine.cu", "ryser_skipper.cu", "mc.cu", "mc_sparse.cu", "batch.cu", "serve.cu", "noalloc.cu", "multi_device.cpp",
     "ryser_dense_inst_0.cu", "ryser_dense_inst_1.cu", "ryser_dense_inst_2.cu",
     "ryser_dense_inst_3.cu", "ryser_dense_inst_4.cu", "ryser_dense_2l_inst_0.cu", "ryser_dense_2l_inst_1.cu", "ryser_dense_int_g3.cu", "ryser_dense_int_g4.cu",
     "ryser_dense_int_g5.cu", "ryser_dense_int_g6.cu", "ryser_dense_int_sparse_g4.cu", "ryser_dense_int_sparse_g5.cu",

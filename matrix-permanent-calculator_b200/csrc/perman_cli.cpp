@@ -26,7 +26,6 @@
 #include <cstring>
 #include <ctime>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "perman_b200.h"
@@ -77,10 +76,11 @@ int die(perm_ctx* ctx, int rc) {
   return 3;
 }
 
-// Multi-GPU exact: one host thread and context per device, shards of the
-// Gray range walked by `variant` (0: the engine's choice per shard), double-
-// double sum of the per-device results.  Evaluates once, like the
-// reference's multi-GPU ids (no error estimate on the sum).
+// Multi-GPU exact: perm_exact_dense_multi (one host thread and context per
+// device, shards of the Gray range walked by `variant` -- 0: the engine's
+// choice per shard -- and a double-double sum of the per-device results).
+// Evaluates once, like the reference's multi-GPU ids (no error estimate on
+// the sum).
 int multi_gpu_dense(const std::vector<double>& a, int n, int gpus, int variant, perm_result* total) {
   int avail = perm_device_count();
   if (avail < 1) {
@@ -88,38 +88,11 @@ int multi_gpu_dense(const std::vector<double>& a, int n, int gpus, int variant, 
     return 3;
   }
   gpus = std::max(1, std::min(gpus, avail));
-  std::vector<perm_result> parts(gpus);
-  std::vector<int> rcs(gpus, 0);
-  std::vector<std::string> errs(gpus);
-  std::vector<std::thread> th;
-  for (int g = 0; g < gpus; g++) {
-    th.emplace_back([&, g] {
-      perm_ctx* ctx = nullptr;
-      rcs[g] = perm_ctx_create(g, &ctx);
-      if (rcs[g] == PERM_OK) {
-        rcs[g] = perm_exact_dense_ex(ctx, a.data(), n, PERM_F64, variant, g, gpus, &parts[g]);
-        if (rcs[g] != PERM_OK) errs[g] = perm_ctx_last_error(ctx);
-      }
-      perm_ctx_destroy(ctx);
-    });
+  const int rc = perm_exact_dense_multi(a.data(), n, PERM_F64, variant, gpus, nullptr, total);
+  if (rc != PERM_OK) {
+    fprintf(stderr, "perman: %s\n", perm_status_string(rc));
+    return 3;
   }
-  for (auto& t : th) t.join();
-  double hi = 0, lo = 0;
-  for (int g = 0; g < gpus; g++) {
-    if (rcs[g] != PERM_OK) {
-      fprintf(stderr, "perman: device %d: %s %s\n", g, perm_status_string(rcs[g]), errs[g].c_str());
-      return 3;
-    }
-    // double-double accumulate (TwoSum on the high parts)
-    double s = hi + parts[g].hi, bb = s - hi;
-    double e = (hi - (s - bb)) + (parts[g].hi - bb);
-    hi = s;
-    lo += e + parts[g].lo;
-  }
-  *total = parts[0];
-  total->hi = hi + lo;
-  total->lo = lo - (total->hi - hi);
-  total->value = total->hi;
   return 0;
 }
 

@@ -1,6 +1,7 @@
 """The C-ABI library loads and exports every symbol include/perman_b200.h declares
 (no compute calls: runs without a GPU)."""
 import ctypes
+import math
 import re
 import subprocess
 
@@ -155,3 +156,21 @@ def test_sdd_levels_query(pb):
     rng = np.random.default_rng(5)
     assert pb.sdd_levels((rng.random((22, 22)) < 0.5) * 1.0)[0] == 0
     assert pb.sdd_levels(np.ones((41, 41)))[0] == pb.PERM_EUNSUPPORTED
+
+
+def test_multi_device_arguments_and_no_device(pb):
+    """perm_exact_dense_multi checks its arguments on the host (1..64 shards,
+    orders 1..64) and, without a GPU, fails loudly instead of computing."""
+    lib = pb.load_library()
+    A = np.ones((5, 5))
+    r = pb.PermResult()
+    p = A.ctypes.data_as(ctypes.c_void_p)
+    assert lib.perm_exact_dense_multi(p, 5, pb.PERM_F64, 0, 0, None, ctypes.byref(r)) == pb.PERM_EINVAL
+    assert lib.perm_exact_dense_multi(p, 5, pb.PERM_F64, 0, 65, None, ctypes.byref(r)) == pb.PERM_EINVAL
+    assert lib.perm_exact_dense_multi(p, 65, pb.PERM_F64, 0, 2, None, ctypes.byref(r)) == pb.PERM_EINVAL
+    assert lib.perm_exact_dense_multi(None, 5, pb.PERM_F64, 0, 2, None, ctypes.byref(r)) == pb.PERM_EINVAL
+    if lib.perm_device_count() > 0:
+        pytest.skip("a GPU is present")
+    with pytest.raises(pb.PermError):
+        pb.exact_dense_multi(A, nshards=2)
+    assert math.isnan(lib.gpu_perman64_xshared_coalescing_mshared_multigpu_double(p, 5, 2, 2048, 128))

@@ -301,6 +301,38 @@ def test_int_kernel_shards(engine, pb):
     assert rel_err(sum(p.hi + p.lo for p in parts), whole) < 1e-12
 
 
+def test_multi_device_entry_point(engine, orc, pb):
+    """perm_exact_dense_multi (gpu_exact_dense.cu:702): shards on device 0
+    listed two and three times (one host thread and context each, kernels
+    running side by side) add up to the one-walk value -- exactly for the
+    integer matrix (oracle), within 1e-12 of the FP64-X walk for the real
+    one -- and the reference-signature shim clamps gpu_num to the visible
+    devices."""
+    import ctypes
+
+    rng = np.random.default_rng(702)
+    A = bernoulli(rng, 26, 0.5) * rng.integers(1, 5, (26, 26))
+    exact = orc.perm_exact_int(A)[0]
+    for devices in ([0, 0], [0, 0, 0]):
+        r = pb.exact_dense_multi(A, devices=devices)
+        assert rel_err(r.value, exact) < 1e-13, (devices, r.value, exact)
+        assert r.total_steps == 2.0**25 and r.rel_error_estimate == 0.0
+    R = 1.0 - rng.random((23, 23))
+    want = engine.exact_dense(R, variant=pb.PERM_KERNEL_DENSE).value
+    assert rel_err(pb.exact_dense_multi(R, devices=[0, 0, 0, 0]).value, want) < 1e-12
+    lib = pb.load_library()
+    Ai = np.ascontiguousarray(A, dtype=np.int32)
+    got = lib.gpu_perman64_xshared_coalescing_mshared_multigpu_int(Ai.ctypes.data_as(ctypes.c_void_p), 26,
+                                                                    lib.perm_device_count() + 3, 2048, 256)
+    assert rel_err(got, exact) < 1e-13
+    Rd = np.ascontiguousarray(R)
+    got = lib.gpu_perman64_xshared_coalescing_mshared_multigpu_double(Rd.ctypes.data_as(ctypes.c_void_p), 23, 1,
+                                                                       2048, 128)
+    assert rel_err(got, want) < 1e-12
+    with pytest.raises(pb.PermError):
+        pb.exact_dense_multi(A, devices=[0, 10**6])  # no such device: the failing shard's status
+
+
 def test_dense_autotune_sets_the_automatic_choice(pb):
     """The autotuned kernel is the automatic choice for single evaluations
     (policy off); with the policy on, integer inputs take the certified walk."""

@@ -41,6 +41,24 @@ __device__ __forceinline__ int4 lds4i(const int* p) {
   return v;
 }
 
+// Exact int32 product of y[a .. a + len), len <= 8 (uint32 arithmetic wraps
+// to the right two's complement value: the host proved |product| < 2^31),
+// multiplied as a balanced tree -- ((y0 y1)(y2 y3)) y4 for five rows -- so
+// its dependent chain is ceil(log2 len) multiplies deep instead of len - 1.
+// Integer multiplication is associative, so the value is the chain's.
+template <int N>
+__device__ __forceinline__ uint32_t rows_product(const int (&y)[N], int a, int len) {
+  uint32_t p[8];
+#pragma unroll
+  for (int t = 0; t < 8; t++) p[t] = t < len ? (uint32_t)y[a + t] : 1u;
+#pragma unroll
+  for (int w = 1; w < 8; w *= 2)
+#pragma unroll
+    for (int t = 0; t + w < 8; t += 2 * w)
+      if (t + w < len) p[t] = p[t] * p[t + w];
+  return p[0];
+}
+
 template <int N, int G>
 __device__ __forceinline__ double group_product(const int (&y)[N]) {
   constexpr int NG = (N + G - 1) / G;

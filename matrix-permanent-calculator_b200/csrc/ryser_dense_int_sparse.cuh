@@ -205,10 +205,7 @@ __device__ __forceinline__ double level_product(const int (&y)[N]) {
 #pragma unroll
   for (int g = 0; g < NG; g++) {
     const int a = J0 + g * G;
-    uint32_t pr = (uint32_t)y[a];
-#pragma unroll
-    for (int t = 1; t < G; t++)
-      if (a + t < J1) pr = pr * (uint32_t)y[a + t];
+    const uint32_t pr = rows_product<N>(y, a, a + G <= J1 ? G : J1 - a);
     const double d = __int2double_rn((int)pr);
     p = g == 0 ? d : p * d;
   }

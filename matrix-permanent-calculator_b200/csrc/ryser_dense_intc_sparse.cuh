@@ -23,10 +23,7 @@ namespace perm {
 // int32 product of rows [j0, j1) (a group, possibly the short last inner one)
 template <int N>
 __device__ __forceinline__ int rows_int(const int (&y)[N], int j0, int j1) {
-  uint32_t pr = (uint32_t)y[j0];
-#pragma unroll
-  for (int j = j0 + 1; j < j1; j++) pr = pr * (uint32_t)y[j];
-  return (int)pr;
+  return (int)rows_product<N>(y, j0, j1 - j0);
 }
 
 // factor i of one level: rows [J0, J1) in groups of G; with kPair, groups

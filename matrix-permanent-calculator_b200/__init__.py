@@ -807,6 +807,107 @@ def distributed_exact_dense_dynamic(mat, chunks: int | None = None, group=None, 
     return dd_sum((float(table[c, 1]), float(table[c, 2])) for c in range(chunks))
 
 
+CHECKPOINT_FORMAT = "perm_b200_checkpoint_v1"
+
+
+def _fingerprint(a: np.ndarray) -> str:
+    import hashlib
+
+    h = hashlib.sha256()
+    h.update(f"{a.shape[0]}:{a.dtype.str}:".encode())
+    h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def _read_checkpoint(path, fingerprint: str, n: int, chunks: int, variant: int) -> dict[int, tuple[float, float]]:
+    import json
+
+    try:
+        with open(path) as f:
+            state = json.load(f)
+    except FileNotFoundError:
+        return {}
+    except (OSError, ValueError) as e:
+        raise PermError(PERM_EIO, f"checkpoint {path} is unreadable ({e}); remove it to start over") from e
+    want = {"format": CHECKPOINT_FORMAT, "matrix_sha256": fingerprint, "n": n, "chunks": chunks,
+            "variant": variant}
+    for k, v in want.items():
+        if state.get(k) != v:
+            raise PermError(PERM_EINVAL, f"checkpoint {path} belongs to another run ({k}: {state.get(k)!r}, "
+                                         f"this run: {v!r}); remove it or pass another path")
+    done = {}
+    for key, (h, l) in state.get("done", {}).items():
+        c = int(key)
+        if not 0 <= c < chunks:
+            raise PermError(PERM_EINVAL, f"checkpoint {path}: chunk {c} outside [0, {chunks})")
+        done[c] = (float.fromhex(h), float.fromhex(l))
+    return done
+
+
+def _write_checkpoint(path, fingerprint: str, n: int, chunks: int, variant: int,
+                      done: dict[int, tuple[float, float]]) -> None:
+    import json
+
+    state = {"format": CHECKPOINT_FORMAT, "matrix_sha256": fingerprint, "n": n, "chunks": chunks,
+             "variant": variant,
+             "done": {str(c): [h.hex(), l.hex()] for c, (h, l) in sorted(done.items())}}
+    tmp = f"{path}.tmp"
+    with open(tmp, "w") as f:
+        json.dump(state, f)
+        f.flush()
+        os.fsync(f.fileno())
+    os.replace(tmp, path)  # atomic: a crash leaves the old file or the new one, never half of one
+
+
+def checkpointed_exact_dense(mat, path, chunks: int = 64, variant: int = 0, engine: Engine | None = None,
+                             shard_fn=None, keep: bool = False) -> tuple[float, float]:
+    """Exact permanent of one long walk that survives interruption
+    (checkpoint / resume; the reference has none: a killed run starts over).
+
+    The Gray walk is cut into `chunks` device-independent shards
+    (perm_shard_range) and walked one after another with
+    perm_exact_dense_ex(variant) on `engine` (default: the process default
+    engine).  After every shard the checkpoint file `path` is rewritten
+    atomically (temporary file, fsync, rename) with the matrix fingerprint
+    (order, dtype, SHA-256 of the values), the chunk count, the variant and
+    the exact bits of every finished shard's (hi, lo).  A later call with
+    the same matrix, chunks and variant resumes: it walks only the shards the
+    file lacks.  The shards are added in chunk order in double-double, so an
+    interrupted and resumed run returns the uninterrupted run's value bit
+    for bit.  A file written for another matrix, chunk count or variant is
+    refused (PermError) instead of being mixed in.  The file is removed
+    after success unless `keep`.  One evaluation, like the shard API: pass
+    the sum to Engine.refine_dense for the accuracy policy.  `shard_fn(mat,
+    chunk, chunks) -> (hi, lo)` replaces the device call (host-logic tests
+    without a GPU)."""
+    a = np.ascontiguousarray(np.asarray(mat, dtype=np.float64))
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise PermError(PERM_EINVAL, f"need a square matrix, got shape {a.shape}")
+    n = a.shape[0]
+    if not 1 <= chunks <= (1 << 20):
+        raise PermError(PERM_EINVAL, f"chunks must be in [1, 2^20], got {chunks}")
+    fp = _fingerprint(a)
+    done = _read_checkpoint(path, fp, n, chunks, variant)
+    eng = None if shard_fn is not None else (engine or default_engine())
+    for c in range(chunks):
+        if c in done:
+            continue
+        if shard_fn is None:
+            r = eng.exact_dense_shard(a, c, chunks, variant=variant)
+            done[c] = (r.hi, r.lo)
+        else:
+            hi, lo = shard_fn(a, c, chunks)
+            done[c] = (float(hi), float(lo))
+        _write_checkpoint(path, fp, n, chunks, variant, done)
+    result = dd_sum(done[c] for c in range(chunks))
+    if not keep:
+        try:
+            os.remove(path)
+        except FileNotFoundError:
+            pass
+    return result
+
+
 def _gather_rows(row, group):
     """All-gather of one float64 row per rank (rank order), on the device for
     NCCL groups and on the host for gloo."""

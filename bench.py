@@ -689,9 +689,10 @@ def compress_for_reference(B):
 
 def batched_secondary(pb, eng, count=8192):
     """8192 matrices, n ~ U[12,28], density ~ U[0.2,0.9], half binary and half
-    U(0,1], half marked sparse (the batch kernel takes them dense): one
-    persistent launch per captured graph, lane ranges from the autotuner; the
-    comparison point is one launch per matrix of the plain kernel."""
+    U(0,1], dense or sparse layout chosen per matrix by the batch: one
+    persistent launch per captured graph, lane ranges and kernel variant from
+    the autotuner; the comparison point is one launch per matrix of the plain
+    kernel."""
     rng = np.random.default_rng(4444)
     mats = []
     for i in range(count):
@@ -713,7 +714,7 @@ def batched_secondary(pb, eng, count=8192):
     b = eng.batch(mats)
     create_ms = (time.perf_counter() - t) * 1e3  # host layout choice and images, upload, graph capture
     t = time.perf_counter()
-    eng.batch(mats).free()  # the same again: no first-use costs
+    eng.batch(mats).free()  # the same again, with the release of its device and pinned memory
     create_again_ms = (time.perf_counter() - t) * 1e3
     b.run()
     times = []

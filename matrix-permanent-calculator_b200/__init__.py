@@ -836,11 +836,14 @@ def _read_checkpoint(path, fingerprint: str, n: int, chunks: int, variant: int) 
             raise PermError(PERM_EINVAL, f"checkpoint {path} belongs to another run ({k}: {state.get(k)!r}, "
                                          f"this run: {v!r}); remove it or pass another path")
     done = {}
-    for key, (h, l) in state.get("done", {}).items():
-        c = int(key)
-        if not 0 <= c < chunks:
-            raise PermError(PERM_EINVAL, f"checkpoint {path}: chunk {c} outside [0, {chunks})")
-        done[c] = (float.fromhex(h), float.fromhex(l))
+    try:
+        for key, (h, l) in state.get("done", {}).items():
+            c = int(key)
+            if not 0 <= c < chunks:
+                raise PermError(PERM_EINVAL, f"checkpoint {path}: chunk {c} outside [0, {chunks})")
+            done[c] = (float.fromhex(h), float.fromhex(l))
+    except (AttributeError, TypeError, ValueError) as e:
+        raise PermError(PERM_EIO, f"checkpoint {path} is unreadable ({e}); remove it to start over") from e
     return done
 
 
@@ -876,7 +879,8 @@ def checkpointed_exact_dense(mat, path, chunks: int = 64, variant: int = 0, engi
     interrupted and resumed run returns the uninterrupted run's value bit
     for bit.  A file written for another matrix, chunk count or variant is
     refused (PermError) instead of being mixed in.  The file is removed
-    after success unless `keep`.  One evaluation, like the shard API: pass
+    after success unless `keep`.  One process at a time per file: two runs
+    sharing a path would overwrite each other's progress.  One evaluation, like the shard API: pass
     the sum to Engine.refine_dense for the accuracy policy.  `shard_fn(mat,
     chunk, chunks) -> (hi, lo)` replaces the device call (host-logic tests
     without a GPU)."""

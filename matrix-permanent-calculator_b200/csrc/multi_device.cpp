@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <exception>
 #include <string>
 #include <thread>
 #include <vector>
@@ -43,7 +44,7 @@ extern "C" int perm_exact_dense_multi(const void* mat, int n, int dtype, int var
   std::vector<std::thread> threads;
   threads.reserve(nshards);
   for (int s = 0; s < nshards; s++) {
-    threads.emplace_back([&, s] {
+    auto run = [&, s] {
       perm_ctx* ctx = nullptr;
       const int dev = devices ? devices[s] : s;
       rcs[s] = perm_ctx_create(dev, &ctx);
@@ -55,7 +56,16 @@ extern "C" int perm_exact_dense_multi(const void* mat, int n, int dtype, int var
       rcs[s] = perm_exact_dense_ex(ctx, mat, n, dtype, variant, s, nshards, &parts[s]);
       if (rcs[s] != PERM_OK) errs[s] = perm_ctx_last_error(ctx);
       perm_ctx_destroy(ctx);
-    });
+    };
+    try {
+      threads.emplace_back(run);
+    } catch (const std::exception& e) {  // no thread for this shard: fail it, keep the started ones
+      for (int t = s; t < nshards; t++) {
+        rcs[t] = PERM_ENOMEM;
+        errs[t] = std::string("cannot start a host thread: ") + e.what();
+      }
+      break;
+    }
   }
   for (auto& t : threads) t.join();
   for (int s = 0; s < nshards; s++) {

@@ -130,3 +130,17 @@ def test_checkpointed_walk_on_the_gpu(pb, orc, engine, tmp_path):
     assert not path.exists()
     # deterministic shard kernels: the resumed sum is the uninterrupted one
     assert (hi, lo) == pb.checkpointed_exact_dense(A, tmp_path / "again.ckpt", chunks=8, engine=engine)
+
+
+def test_checkpoint_with_bad_entries_is_refused(pb, orc, tmp_path):
+    A = np.eye(6) + 0.5
+    path = tmp_path / "walk.ckpt"
+    state = {"format": pb.CHECKPOINT_FORMAT, "matrix_sha256": pb._fingerprint(np.ascontiguousarray(A)),
+             "n": 6, "chunks": 3, "variant": 0, "done": {"0": [1.5, "0x0p+0"]}}
+    path.write_text(json.dumps(state))
+    with pytest.raises(pb.PermError, match="unreadable"):
+        pb.checkpointed_exact_dense(A, path, chunks=3, shard_fn=oracle_shard_fn(pb, orc))
+    state["done"] = {"7": ["0x1p+0", "0x0p+0"]}
+    path.write_text(json.dumps(state))
+    with pytest.raises(pb.PermError, match="outside"):
+        pb.checkpointed_exact_dense(A, path, chunks=3, shard_fn=oracle_shard_fn(pb, orc))

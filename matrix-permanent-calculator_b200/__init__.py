@@ -8,7 +8,7 @@ missing or no B200 is usable, every compute call raises ``PermError``.
 
 The reference (berkyaglioglu/matrix-permanent-calculator) exposes its GPU path
 as C++ templates taking a row-major ``T* mat`` and returning a double
-(gpu_exact_dense.cu:641, gpu_exact_sparse.cu:1124,
+(gpu_exact_dense.cu:641 and :702, gpu_exact_sparse.cu:1124,
 gpu_approximation_dense.cu:374 and :528, gpu_approximation_sparse.cu:455 and
 :608).  Functions with the same names and argument meaning are provided at the
 bottom of this module; they dispatch on the numpy dtype like the templates do
@@ -1038,6 +1038,21 @@ def gpu_perman64_xshared_coalescing_mshared(mat, nov: int | None = None, grid_di
     if nov is not None and nov != a.shape[0]:
         a = a.reshape(nov, nov)
     return default_engine().exact_dense(a).value
+
+
+def gpu_perman64_xshared_coalescing_mshared_multigpu(mat, nov: int | None = None, gpu_num: int = 2,
+                                                     grid_dim: int = 2048, block_dim: int = 256) -> float:
+    """Dense exact permanent over devices 0 .. gpu_num - 1 of this process
+    (gpu_exact_dense.cu:702; at most the visible devices): one shard per
+    device through perm_exact_dense_multi, one evaluation; grid/block are
+    ignored."""
+    a = np.asarray(mat)
+    if nov is not None and nov != a.shape[0]:
+        a = a.reshape(nov, nov)
+    avail = int(load_library().perm_device_count())
+    if avail < 1:
+        raise PermError(PERM_ECUDA, "no CUDA device")
+    return exact_dense_multi(a, nshards=max(1, min(gpu_num, avail))).value
 
 
 def gpu_perman64_xshared_coalescing_mshared_skipper(mat, rptrs, cols, cptrs, rows, cvals, nov: int,

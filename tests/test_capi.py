@@ -174,3 +174,10 @@ def test_multi_device_arguments_and_no_device(pb):
     with pytest.raises(pb.PermError):
         pb.exact_dense_multi(A, nshards=2)
     assert math.isnan(lib.gpu_perman64_xshared_coalescing_mshared_multigpu_double(p, 5, 2, 2048, 128))
+
+
+def test_multigpu_python_mirror_fails_loudly_without_gpu(pb):
+    if pb.load_library().perm_device_count() > 0:
+        pytest.skip("a GPU is present")
+    with pytest.raises(pb.PermError):
+        pb.gpu_perman64_xshared_coalescing_mshared_multigpu(np.ones((4, 4)), 4, 2)

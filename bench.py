@@ -23,7 +23,6 @@ import ctypes
 import hashlib
 import importlib.util
 import json
-import math
 import os
 import statistics
 import subprocess
